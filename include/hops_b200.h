@@ -1,0 +1,209 @@
+/*
+ * hops_b200.h -- C ABI of the B200-native HOPS trajectory hot path.
+ *
+ * Every entry point is plain C (extern "C"), takes plain pointers and sizes and
+ * returns an int status: 0 = success, > 0 = one of the HOPS_E* codes below; the
+ * text of the last error of the calling thread is available from
+ * hops_last_error().  All array pointers named *_dev are CUDA device pointers
+ * owned by the caller; the library allocates no device memory on these paths
+ * except the cuFFT plan work area inside hops_noise_filter.  `stream` is a
+ * cudaStream_t passed as void* (NULL = legacy default stream).
+ *
+ * Reference interfaces replaced (paths inside the MesoHOPS source tree
+ * src/mesohops):
+ *   hops_dsystem_dt          <- eom/hops_eom.py:196-441 (nonlinear dsystem_dt closure)
+ *                               and hops_eom.py:445-542 (LINEAR closure)
+ *   hops_rk4_propagate       <- trajectory/hops_trajectory.py:456-533 loop body:
+ *                               integrator/integrator_rk.py:78-134 (noise at
+ *                               t, t+tau/2, t+tau), integrator_rk.py:10-75 (RK4)
+ *                               and hops_trajectory.py:616-634 (normalize)
+ *   hops_resident_propagate  <- same loop, one CTA per trajectory with its own
+ *                               (possibly uneven) basis, all steps in one launch
+ *   hops_noise_filter        <- noise/hops_noise.py:630-716 (_construct_correlated_noise)
+ *                               with hops_noise.py:167-192,232-247 (alpha, complex64)
+ */
+#ifndef HOPS_B200_H
+#define HOPS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HOPS_OK 0
+#define HOPS_EINVAL 1       /* bad argument (sizes, null pointers, unsupported mode) */
+#define HOPS_ECUDA 2        /* a CUDA runtime / driver call failed */
+#define HOPS_ENOTSUP 3      /* request outside what the library implements */
+#define HOPS_ENONFINITE 5   /* a trajectory produced NaN/Inf (status word set) */
+
+#define HOPS_PREC_C128 0    /* complex128 state and arithmetic */
+#define HOPS_PREC_C64 1     /* complex64 state/SpMM, FP64 <L>, norm, z_mem */
+
+#define HOPS_EOM_NORMALIZED_NONLINEAR 0
+#define HOPS_EOM_NONLINEAR 1
+#define HOPS_EOM_LINEAR 2
+
+/*
+ * One hierarchy basis in device memory (all pointers are device pointers).
+ * Complex numbers are stored as interleaved (re, im) doubles; *_f arrays hold
+ * the same coefficients rounded to float for HOPS_PREC_C64.
+ * Aux index a, state index s; phi element (a, b, s) of a batch of B
+ * trajectories lives at ((a * B) + b) * n_state + s.
+ */
+typedef struct hops_structure {
+  int32_t n_hier, n_state, n_mode, n_lop;
+  int32_t n_first;        /* first-level aux entries used by the norm correction */
+  int32_t n_up, n_dn;     /* connection counts */
+  int32_t site_projector; /* 1: every L_j = v_j |s_j><s_j| (fast path) */
+  int32_t max_up, max_dn; /* longest connection list of any aux */
+  /* per aux */
+  const double* k_decay;  /* [n_hier] complex: -sum_m k_m w_m (K2_k diagonal) */
+  const float* k_decay_f;
+  const int32_t* up_ptr;  /* [n_hier+1] CSR over aux of the k+1 connections */
+  const int32_t* up_aux;  /* [n_up] aux index a + e_m */
+  const int32_t* up_mode; /* [n_up] relative mode m */
+  const int32_t* dn_ptr;  /* [n_hier+1] CSR over aux of the k-1 connections */
+  const int32_t* dn_aux;  /* [n_dn] aux index a - e_m */
+  const int32_t* dn_mode; /* [n_dn] relative mode m */
+  const double* dn_coef;  /* [n_dn] complex: k_m(a) * w_m */
+  const float* dn_coef_f;
+  /* per relative mode */
+  const int32_t* mode_lop; /* [n_mode] relative L index of the mode */
+  const double* mode_g;    /* [n_mode] complex g_m */
+  const double* mode_w;    /* [n_mode] complex w_m */
+  const double* mode_gw;   /* [n_mode] complex g_m / w_m */
+  const float* mode_gw_f;
+  /* first-level aux (hops_eom.py:186-194) */
+  const int32_t* first_aux;  /* [n_first] */
+  const int32_t* first_mode; /* [n_first] */
+  /* L operators in the state basis: CSR of L_j and CSR of L_j^H */
+  const int32_t* l_ptr; /* [n_lop * (n_state+1)] */
+  const int32_t* l_col;
+  const double* l_val;  /* complex */
+  const float* l_val_f;
+  const int32_t* lh_ptr;
+  const int32_t* lh_col;
+  const double* lh_val;
+  const float* lh_val_f;
+  const int32_t* lop_active; /* [n_lop] 1 if L_j has a nonzero in the basis */
+  const int32_t* lop_site;   /* [n_lop] s_j (site-projector form) */
+  const double* lop_sval;    /* [n_lop] complex v_j (site-projector form) */
+  /* -i H as CSR over states */
+  const int32_t* h_ptr; /* [n_state+1] */
+  const int32_t* h_col;
+  const double* h_val;  /* complex, already multiplied by -i */
+  const float* h_val_f;
+} hops_structure;
+
+/*
+ * A batch of B trajectories sharing one hops_structure.  Vectors phi, acc,
+ * y0, y1 have n_hier * B * n_state complex elements of the batch precision.
+ */
+typedef struct hops_batch {
+  int32_t n_traj;
+  int32_t precision; /* HOPS_PREC_* */
+  int32_t eom;       /* HOPS_EOM_* */
+  int32_t n_t1, n_t2;   /* noise time-axis lengths */
+  void* phi;   /* state; normalised lazily by `scale` (see hops_rk4_propagate) */
+  void* acc;   /* RK4 accumulator */
+  void* y0;    /* stage inputs (ping-pong) */
+  void* y1;
+  double* zmem;  /* [B][n_mode] complex noise memory */
+  double* work;  /* scalar workspace of hops_scalar_workspace_doubles() doubles */
+  const float* noise1; /* [B][n_lop][n_t1] complex64 */
+  const float* noise2; /* [B][n_lop][n_t2] complex64, or NULL for zero noise 2 */
+  int32_t* status;     /* [B] 0 ok, HOPS_ENONFINITE if a norm went NaN/Inf */
+} hops_batch;
+
+/* One trajectory of hops_resident_propagate (array in device memory). */
+typedef struct hops_task {
+  const hops_structure* st; /* device pointer to the structure */
+  void* phi;                /* [n_hier][n_state] in the task precision */
+  double* zmem;             /* [n_mode] complex */
+  const float* noise1;      /* [n_lop][n_t1] complex64 */
+  const float* noise2;      /* [n_lop][n_t2] complex64 or NULL */
+  double* psi_out;          /* [n_steps][n_state] complex128, or NULL */
+  void* scratch;            /* 3 * n_hier * n_state elements if the vectors do not fit shared memory */
+  int32_t n_t1, n_t2;
+  int32_t it0;      /* noise index of the start time */
+  int32_t di;       /* noise index step per half time step */
+  int32_t n_steps;
+  int32_t precision;
+  int32_t eom;
+  int32_t status;   /* written by the kernel: 0 ok, HOPS_ENONFINITE */
+  double tau_over_hbar;
+  double scale;     /* pending normalisation factor of phi (1 = none) */
+} hops_task;
+
+const char* hops_last_error(void);
+int hops_version(void);
+int hops_device_query(int device, int* sm_count, int* smem_optin_bytes);
+
+/* Doubles of scalar workspace hops_batch.work must hold. */
+size_t hops_scalar_workspace_doubles(int32_t n_state, int32_t n_mode, int32_t n_lop,
+                                     int32_t n_traj);
+
+/* Reset the scalar workspace (pending scale = 1, status = 0). */
+int hops_batch_reset(const hops_structure* st, hops_batch* bt, void* stream);
+
+/*
+ * dsystem_dt for the B trajectories of bt at the state bt->phi (scale applied),
+ * memory bt->zmem and one noise sample per L: z1_dev / z2_dev are [B][n_lop]
+ * complex64 (z2_dev may be NULL).  Writes dphi (layout of phi, in cm^-1, not
+ * divided by hbar) and dzmem ([B][n_mode] complex128).
+ */
+int hops_dsystem_dt(const hops_structure* st, hops_batch* bt, const float* z1_dev,
+                    const float* z2_dev, void* dphi_dev, double* dzmem_dev, void* stream);
+
+/*
+ * n_steps RK4 steps of size tau (tau_over_hbar = tau / hbar) from the noise
+ * index it0; stage noise is read at it0 + 2*n*di + {0, di, di, 2*di}.  For the
+ * normalized EOM the state is renormalised after every step; psi_out_dev
+ * (nullable) receives [n_steps][B][n_state] complex128 normalised psi_0 after
+ * each step.  On return phi holds the normalised state.
+ */
+int hops_rk4_propagate(const hops_structure* st, hops_batch* bt, int32_t it0,
+                       int32_t di, int32_t n_steps, double tau_over_hbar,
+                       double* psi_out_dev, void* stream);
+
+/*
+ * Resident propagation: one CTA per task, all n_steps steps of every task in
+ * one launch, stage vectors in shared memory when they fit (otherwise in the
+ * task's scratch).  tasks_dev is a device array of n_tasks hops_task; the
+ * kernel writes each task's status and leaves its phi normalised.
+ * max_elems: largest n_hier*n_state of any task; max_scalar_doubles: largest
+ * hops_resident_scalar_doubles() of any task; all_site_projector: 1 if every
+ * task's structure has site_projector = 1 (selects the fast path).
+ */
+int hops_resident_propagate(hops_task* tasks_dev, int32_t n_tasks, int32_t max_elems,
+                            int32_t max_scalar_doubles, int32_t precision,
+                            int32_t all_site_projector, void* stream);
+
+/* Shared-memory doubles of per-stage scalars one resident task needs. */
+int32_t hops_resident_scalar_doubles(int32_t n_state, int32_t n_mode, int32_t n_lop);
+
+/*
+ * FFT-filtered correlated noise in FP64.  For each of n_lop rows:
+ * alpha (complex128 [n_lop][n_t], already summed over the noise modes of the
+ * row) is rounded to complex64 (hops_noise.py:236), rotated so its last sample
+ * is real, embedded in a circulant of length 2(n_t-1), transformed, clipped at
+ * zero and used to filter the complex64 draws z_dev ([n_lop][2(n_t-1)]); the
+ * first n_t samples, un-rotated, are written to out_dev as complex128
+ * ([n_lop][n_t]; nullable) and, if out64_dev is not NULL, as complex64.
+ * The transforms use cuFFT (plan created and destroyed inside the call).
+ * n_negative_host (nullable) receives the number of clipped spectral values.
+ */
+int hops_noise_filter(const double* alpha_dev, const float* z_dev, int32_t n_lop,
+                      int32_t n_t, double* work_dev, double* out_dev, float* out64_dev,
+                      int64_t* n_negative_host, void* stream);
+
+/* Doubles of device work area hops_noise_filter needs (work_dev). */
+size_t hops_noise_filter_work_doubles(int32_t n_lop, int32_t n_t);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HOPS_B200_H */

@@ -1,0 +1,113 @@
+"""ctypes binding of ``libhops_b200.so`` (C ABI in ``include/hops_b200.h``).
+
+The library is built in-tree (``mesohops_b200/lib``) by ``mesohops_b200.build``.
+There is no fallback: if the shared library is missing or fails to load, every
+GPU entry point raises ``RuntimeError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from .exceptions import TrajectoryError, UnsupportedRequest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libhops_b200.so")
+
+HOPS_OK, HOPS_EINVAL, HOPS_ECUDA, HOPS_ENOTSUP, HOPS_ENONFINITE = 0, 1, 2, 3, 5
+PREC_C128, PREC_C64 = 0, 1
+EOM_CODES = {"NORMALIZED NONLINEAR": 0, "NONLINEAR": 1, "LINEAR": 2}
+
+_p = C.c_void_p
+_i = C.c_int32
+
+
+class HopsStructure(C.Structure):
+    """Mirror of ``hops_structure`` (all pointer fields are device pointers)."""
+    _fields_ = [
+        ("n_hier", _i), ("n_state", _i), ("n_mode", _i), ("n_lop", _i),
+        ("n_first", _i), ("n_up", _i), ("n_dn", _i), ("site_projector", _i),
+        ("max_up", _i), ("max_dn", _i),
+        ("k_decay", _p), ("k_decay_f", _p),
+        ("up_ptr", _p), ("up_aux", _p), ("up_mode", _p),
+        ("dn_ptr", _p), ("dn_aux", _p), ("dn_mode", _p), ("dn_coef", _p), ("dn_coef_f", _p),
+        ("mode_lop", _p), ("mode_g", _p), ("mode_w", _p), ("mode_gw", _p), ("mode_gw_f", _p),
+        ("first_aux", _p), ("first_mode", _p),
+        ("l_ptr", _p), ("l_col", _p), ("l_val", _p), ("l_val_f", _p),
+        ("lh_ptr", _p), ("lh_col", _p), ("lh_val", _p), ("lh_val_f", _p),
+        ("lop_active", _p), ("lop_site", _p), ("lop_sval", _p),
+        ("h_ptr", _p), ("h_col", _p), ("h_val", _p), ("h_val_f", _p),
+    ]
+
+
+class HopsBatch(C.Structure):
+    """Mirror of ``hops_batch``."""
+    _fields_ = [
+        ("n_traj", _i), ("precision", _i), ("eom", _i), ("n_t1", _i), ("n_t2", _i),
+        ("phi", _p), ("acc", _p), ("y0", _p), ("y1", _p),
+        ("zmem", _p), ("work", _p), ("noise1", _p), ("noise2", _p), ("status", _p),
+    ]
+
+
+class HopsTask(C.Structure):
+    """Mirror of ``hops_task``."""
+    _fields_ = [
+        ("st", _p), ("phi", _p), ("zmem", _p), ("noise1", _p), ("noise2", _p),
+        ("psi_out", _p), ("scratch", _p),
+        ("n_t1", _i), ("n_t2", _i), ("it0", _i), ("di", _i), ("n_steps", _i),
+        ("precision", _i), ("eom", _i), ("status", _i),
+        ("tau_over_hbar", C.c_double), ("scale", C.c_double),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Load (once) and return the CUDA library; raises if it is not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"mesohops_b200 CUDA library not found at {LIB_PATH}; "
+            "build it with `python -m mesohops_b200.build` (there is no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    L.hops_last_error.restype = C.c_char_p
+    L.hops_version.restype = C.c_int
+    L.hops_device_query.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.hops_scalar_workspace_doubles.restype = C.c_size_t
+    L.hops_scalar_workspace_doubles.argtypes = [_i, _i, _i, _i]
+    L.hops_batch_reset.argtypes = [C.POINTER(HopsStructure), C.POINTER(HopsBatch), _p]
+    L.hops_dsystem_dt.argtypes = [C.POINTER(HopsStructure), C.POINTER(HopsBatch), _p, _p, _p,
+                                  _p, _p]
+    L.hops_rk4_propagate.argtypes = [C.POINTER(HopsStructure), C.POINTER(HopsBatch), _i, _i,
+                                     _i, C.c_double, _p, _p]
+    L.hops_resident_propagate.argtypes = [_p, _i, _i, _i, _i, _i, _p]
+    L.hops_resident_scalar_doubles.restype = _i
+    L.hops_resident_scalar_doubles.argtypes = [_i, _i, _i]
+    L.hops_noise_filter.argtypes = [_p, _p, _i, _i, _p, _p, _p, C.POINTER(C.c_int64), _p]
+    L.hops_noise_filter_work_doubles.restype = C.c_size_t
+    L.hops_noise_filter_work_doubles.argtypes = [_i, _i]
+    _lib = L
+    return L
+
+
+def check(rc, what):
+    """Map a status code to the reference's exception types."""
+    if rc == HOPS_OK:
+        return
+    msg = lib().hops_last_error().decode(errors="replace")
+    if rc == HOPS_ENONFINITE:
+        raise TrajectoryError(f"{what}: non-finite state ({msg})")
+    if rc == HOPS_ENOTSUP:
+        raise UnsupportedRequest(f"{what}: {msg}", what, override=True)
+    raise RuntimeError(f"{what} failed with status {rc}: {msg}")
+
+
+def exported_symbols():
+    """Names declared in include/hops_b200.h that the library must export."""
+    return ["hops_last_error", "hops_version", "hops_device_query",
+            "hops_scalar_workspace_doubles", "hops_batch_reset", "hops_dsystem_dt",
+            "hops_rk4_propagate", "hops_resident_propagate", "hops_resident_scalar_doubles",
+            "hops_noise_filter", "hops_noise_filter_work_doubles"]

@@ -1,0 +1,277 @@
+// Shared device helpers of the HOPS trajectory kernels (complex arithmetic and
+// the per-stage FP64 scalars of the normalized nonlinear equation of motion).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "../../include/hops_b200.h"
+
+namespace hops {
+
+// ---------------------------------------------------------------- complex ----
+template <typename R> struct cplx;
+template <> struct cplx<double> { using T = double2; };
+template <> struct cplx<float> { using T = float2; };
+
+__device__ __forceinline__ double2 mk(double x, double y) { return make_double2(x, y); }
+__device__ __forceinline__ float2 mkf(float x, float y) { return make_float2(x, y); }
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return mk(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return mkf(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return mk(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return mkf(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cconj(double2 a) { return mk(a.x, -a.y); }
+__device__ __forceinline__ float2 cconj(float2 a) { return mkf(a.x, -a.y); }
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return mk(a.x * s, a.y * s); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return mkf(a.x * s, a.y * s); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return mk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return mkf(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * b + c
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {
+  c.x = fma(a.x, b.x, c.x);
+  c.x = fma(-a.y, b.y, c.x);
+  c.y = fma(a.x, b.y, c.y);
+  c.y = fma(a.y, b.x, c.y);
+  return c;
+}
+__device__ __forceinline__ float2 cfma(float2 a, float2 b, float2 c) {
+  c.x = fmaf(a.x, b.x, c.x);
+  c.x = fmaf(-a.y, b.y, c.x);
+  c.y = fmaf(a.x, b.y, c.y);
+  c.y = fmaf(a.y, b.x, c.y);
+  return c;
+}
+// conj(a) * b
+__device__ __forceinline__ double2 cconjmul(double2 a, double2 b) {
+  return mk(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+template <typename T> __device__ __forceinline__ T czero();
+template <> __device__ __forceinline__ double2 czero<double2>() { return mk(0.0, 0.0); }
+template <> __device__ __forceinline__ float2 czero<float2>() { return mkf(0.f, 0.f); }
+__device__ __forceinline__ double2 to_d(float2 a) { return mk((double)a.x, (double)a.y); }
+__device__ __forceinline__ double2 to_d(double2 a) { return a; }
+template <typename T> __device__ __forceinline__ T from_d(double2 a);
+template <> __device__ __forceinline__ double2 from_d<double2>(double2 a) { return a; }
+template <> __device__ __forceinline__ float2 from_d<float2>(double2 a) {
+  return mkf((float)a.x, (float)a.y);
+}
+__device__ __forceinline__ double2 ld2(const double* p, int i) {
+  return reinterpret_cast<const double2*>(p)[i];
+}
+__device__ __forceinline__ float2 ld2f(const float* p, int i) {
+  return reinterpret_cast<const float2*>(p)[i];
+}
+__device__ __forceinline__ bool finite2(double2 a) { return isfinite(a.x) && isfinite(a.y); }
+
+// ------------------------------------------------------- scalar workspace ----
+// Per-trajectory FP64 scalars of one RK stage (layout of hops_batch.work).
+struct ScalarLayout {
+  int S, M, L;
+  int stride;  // doubles per trajectory
+  __host__ __device__ ScalarLayout(int s, int m, int l) : S(s), M(m), L(l) {
+    int n = 4 + 4 * L + 7 * M + 3 * S;
+    stride = (n + 1) & ~1;
+  }
+  __host__ __device__ int scale() const { return 0; }
+  __host__ __device__ int nc() const { return 1; }
+  __host__ __device__ int n2() const { return 2; }
+  __host__ __device__ int avgL() const { return 4; }
+  __host__ __device__ int cz() const { return 4 + 2 * L; }
+  __host__ __device__ int zst() const { return 4 + 4 * L; }
+  __host__ __device__ int zacc() const { return 4 + 4 * L + 2 * M; }
+  __host__ __device__ int upc() const { return 4 + 4 * L + 4 * M; }
+  __host__ __device__ int diagD() const { return 4 + 4 * L + 6 * M; }
+  __host__ __device__ int upc_f() const { return 4 + 4 * L + 6 * M + 2 * S; }   // M float2
+  __host__ __device__ int diagD_f() const { return 4 + 4 * L + 7 * M + 2 * S; } // S float2
+};
+
+// Stage constants of classic RK4 (integrator_rk.py:29-30).
+__device__ __forceinline__ double rk_c(int i) { return i == 0 ? 0.0 : (i == 3 ? 1.0 : 0.5); }
+__device__ __forceinline__ int rk_noise_slot(int i) { return i == 0 ? 0 : (i == 3 ? 2 : 1); }
+
+// Block reduction of a double (all threads call; result valid in every thread).
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  int nw = (blockDim.x + 31) >> 5;
+  double t = 0.0;
+  if (threadIdx.x < 32) {
+    t = (l < nw) ? red[l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (l == 0) red[0] = t;
+  }
+  __syncthreads();
+  double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+struct StageIO {
+  // inputs
+  const double* zmem;   // [M] noise memory at the start of the step
+  const float2* noise1;  // [L][n_t1] of this trajectory (complex64)
+  const float2* noise2;  // [L][n_t2] or null
+  int n_t1, n_t2;
+  int it;               // noise time index of this stage
+  int stage;            // 0..3, or 4 = single derivative (no RK bookkeeping)
+  int eom;
+  double h;             // tau / hbar
+  // in/out (this trajectory's scalars)
+  double* ws;           // ScalarLayout block of this trajectory
+  double* zmem_out;     // final z_mem written at stage 3 (and dz at stage 4)
+};
+
+// Computes <L_j>, the noise coefficients cz_j = zhat_j - i z2_j, the norm
+// correction, the z_mem RK4 bookkeeping and the derived per-state / per-mode
+// coefficients for one trajectory.  Restates eom/eom_functions.py:11-213 and
+// the z_mem half of integrator/integrator_rk.py:10-75.
+//   get(a, s): stage-input element (aux a, state s) of this trajectory as double2.
+// All threads of the block must call it; red / sh are shared scratch
+// (red >= 32 doubles, sh >= 4*L + 2 doubles).
+template <class Get>
+__device__ void stage_scalars(const hops_structure& st, const StageIO& io, Get get,
+                              double* red, double* sh) {
+  const int S = st.n_state, M = st.n_mode, L = st.n_lop;
+  ScalarLayout lay(S, M, L);
+  double* ws = io.ws;
+  const bool linear = io.eom == HOPS_EOM_LINEAR;
+  const bool normalized = io.eom == HOPS_EOM_NORMALIZED_NONLINEAR;
+  double2* avgL = reinterpret_cast<double2*>(sh);       // [L]
+  double2* zhat = reinterpret_cast<double2*>(sh + 2 * L);  // [L]
+
+  // |psi_0|^2
+  double p = 0.0;
+  for (int s = threadIdx.x; s < S; s += blockDim.x) {
+    double2 v = get(0, s);
+    p += v.x * v.x + v.y * v.y;
+  }
+  const double n2 = block_sum(p, red);
+
+  // <L_j> = psi0^H L_j psi0 / psi0^H psi0 (active L only), and zhat_j.
+  for (int j = threadIdx.x; j < L; j += blockDim.x) {
+    double2 num = mk(0.0, 0.0);
+    const bool act = st.lop_active[j] != 0;
+    if (!linear && act) {
+      const int base = j * (S + 1);
+      for (int r = 0; r < S; ++r) {
+        int q0 = st.l_ptr[base + r], q1 = st.l_ptr[base + r + 1];
+        if (q0 == q1) continue;
+        double2 row = mk(0.0, 0.0);
+        for (int q = q0; q < q1; ++q) row = cfma(ld2(st.l_val, q), get(0, st.l_col[q]), row);
+        num = cadd(num, cconjmul(get(0, r), row));
+      }
+      num = mk(num.x / n2, num.y / n2);
+    }
+    avgL[j] = num;
+    // compress_zmem: sum of z_mem over the modes of L_j, then + conj(z1).
+    float2 z1 = io.noise1 ? io.noise1[(size_t)j * io.n_t1 + io.it] : mkf(0.f, 0.f);
+    double2 zs = mk(0.0, 0.0);
+    if (!linear) {
+      const double* zsrc = io.stage == 0 || io.stage == 4 ? io.zmem : ws + lay.zst();
+      for (int m = 0; m < M; ++m)
+        if (st.mode_lop[m] == j) zs = cadd(zs, ld2(zsrc, m));
+    }
+    double2 zh = cadd(mk((double)z1.x, -(double)z1.y), zs);
+    zhat[j] = zh;
+    float2 z2 = io.noise2 ? io.noise2[(size_t)j * io.n_t2 + io.it] : mkf(0.f, 0.f);
+    double2 cz = (linear || act) ? mk(zh.x + (double)z2.y, zh.y - (double)z2.x) : mk(0.0, 0.0);
+    // The LINEAR closure forms conj(z1) - 1j*z2 from complex64 samples without
+    // any complex128 term, so the reference rounds it to complex64
+    // (hops_eom.py:520,535); the float sum of two floats taken in double and
+    // rounded once is the correctly rounded float sum.
+    if (linear) cz = mk((double)(float)cz.x, (double)(float)cz.y);
+    reinterpret_cast<double2*>(ws + lay.cz())[j] = cz;
+    reinterpret_cast<double2*>(ws + lay.avgL())[j] = num;
+  }
+  __syncthreads();
+
+  // Normalisation correction (eom_functions.py:163-213).
+  double nc = 0.0;
+  if (normalized) {
+    double part_re = 0.0;
+    if (threadIdx.x == 0) {
+      double2 d = mk(0.0, 0.0);
+      for (int j = 0; j < L; ++j)
+        if (st.lop_active[j]) d = cfma(zhat[j], avgL[j], d);
+      part_re = d.x;
+    }
+    for (int f = threadIdx.x; f < st.n_first; f += blockDim.x) {
+      const int a = st.first_aux[f], m = st.first_mode[f], j = st.mode_lop[m];
+      if (!st.lop_active[j]) continue;
+      const int base = j * (S + 1);
+      double2 t1 = mk(0.0, 0.0), t2 = mk(0.0, 0.0);
+      for (int r = 0; r < S; ++r) {
+        double2 p0 = get(0, r);
+        t2 = cadd(t2, cconjmul(p0, get(a, r)));
+        int q0 = st.l_ptr[base + r], q1 = st.l_ptr[base + r + 1];
+        if (q0 == q1) continue;
+        double2 row = mk(0.0, 0.0);
+        for (int q = q0; q < q1; ++q) row = cfma(ld2(st.l_val, q), get(a, st.l_col[q]), row);
+        t1 = cadd(t1, cconjmul(p0, row));
+      }
+      double2 gw = ld2(st.mode_gw, m);
+      // -(g/w) (t1 - <L> t2)
+      double2 c = csub(t1, cmul(avgL[j], t2));
+      part_re -= (gw.x * c.x - gw.y * c.y);
+    }
+    nc = block_sum(part_re, red);
+  }
+
+  // z_mem derivative, RK4 bookkeeping of z_mem, per-mode up coefficient.
+  const double h = io.h;
+  for (int m = threadIdx.x; m < M; m += blockDim.x) {
+    const int j = st.mode_lop[m];
+    double2* zst = reinterpret_cast<double2*>(ws + lay.zst());
+    double2* zacc = reinterpret_cast<double2*>(ws + lay.zacc());
+    double2 z0 = ld2(io.zmem, m);
+    double2 zi = (io.stage == 0 || io.stage == 4) ? z0 : zst[m];
+    double2 kz = mk(0.0, 0.0);
+    double2 upc = mk(0.0, 0.0);
+    if (!linear) {
+      double2 g = ld2(st.mode_g, m), w = ld2(st.mode_w, m);
+      double2 al = st.lop_active[j] ? avgL[j] : mk(0.0, 0.0);
+      // calc_delta_zmem: conj(g) <L> - conj(w) z
+      kz = csub(cmul(cconj(g), al), cmul(cconj(w), zi));
+      upc = cmul(ld2(st.mode_gw, m), cconj(al));
+    }
+    reinterpret_cast<double2*>(ws + lay.upc())[m] = upc;
+    reinterpret_cast<float2*>(ws + lay.upc_f())[m] = mkf((float)upc.x, (float)upc.y);
+    if (io.stage == 4) {
+      reinterpret_cast<double2*>(io.zmem_out)[m] = kz;
+    } else if (io.stage == 0) {
+      zacc[m] = kz;
+      zst[m] = cadd(z0, cscale(cscale(kz, 0.5), h));
+    } else if (io.stage < 3) {
+      zacc[m] = cadd(zacc[m], cscale(kz, 2.0));
+      zst[m] = cadd(z0, cscale(cscale(kz, rk_c(io.stage + 1)), h));
+    } else {
+      double2 sum = cadd(zacc[m], kz);
+      reinterpret_cast<double2*>(io.zmem_out)[m] = cadd(z0, mk(h * sum.x / 6.0, h * sum.y / 6.0));
+    }
+  }
+
+  // Per-state diagonal: -nc + sum_j cz_j v_j [s == s_j] (site-projector form).
+  for (int s = threadIdx.x; s < S; s += blockDim.x) {
+    double2 d = mk(-nc, 0.0);
+    if (st.site_projector) {
+      const double2* cz = reinterpret_cast<const double2*>(ws + lay.cz());
+      for (int j = 0; j < L; ++j)
+        if (st.lop_site[j] == s) d = cfma(cz[j], ld2(st.lop_sval, j), d);
+    }
+    reinterpret_cast<double2*>(ws + lay.diagD())[s] = d;
+    reinterpret_cast<float2*>(ws + lay.diagD_f())[s] = mkf((float)d.x, (float)d.y);
+  }
+  if (threadIdx.x == 0) {
+    ws[lay.nc()] = nc;
+    ws[lay.n2()] = n2;
+  }
+  __syncthreads();
+}
+
+}  // namespace hops

@@ -1,0 +1,174 @@
+// FFT-filtered complex noise in FP64 (Percival circulant embedding), the GPU
+// replacement of noise/hops_noise.py:630-716.  The three length-2(n_t-1)
+// transforms are cuFFT Z2Z plans; embedding, clipping, filtering and the
+// phase (un)rotation are the kernels below.
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdio.h>
+#include <stdarg.h>
+#include "hops_common.cuh"
+
+using namespace hops;
+
+void hops_set_error_text(const char* msg);  // defined in hops_rk4.cu
+static thread_local char g_nerr[512];
+
+static int nerr(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_nerr, sizeof(g_nerr), fmt, ap);
+  va_end(ap);
+  hops_set_error_text(g_nerr);
+  return code;
+}
+
+// Rounded alpha as the reference stores it (complex64, hops_noise.py:236).
+__device__ __forceinline__ double2 alpha64(const double* alpha, size_t i) {
+  double2 a = reinterpret_cast<const double2*>(alpha)[i];
+  return mk((double)(float)a.x, (double)(float)a.y);
+}
+
+// nu_l = angle(c[l, n_t-1]) / ((n_t-1) 2 pi): rotation that makes the last sample real.
+__device__ __forceinline__ double rot_nu(const double* alpha, int l, int n_t) {
+  double2 c = alpha64(alpha, (size_t)l * n_t + (n_t - 1));
+  return atan2(c.y, c.x) / ((n_t - 1.0) * 2.0 * 3.14159265358979323846);
+}
+
+// exp(-2 pi i nu k)
+__device__ __forceinline__ double2 rot(double nu, long k) {
+  double sn, cs;
+  // reduce nu*k to [0,1) turns before the trig call
+  double x = nu * (double)k;
+  x -= floor(x);
+  sincospi(-2.0 * x, &sn, &cs);
+  return mk(cs, sn);
+}
+
+// emb[l][k], k < N = 2(n_t-1): rotated correlation function and its Hermitian mirror.
+__global__ void k_embed(const double* alpha, int n_lop, int n_t, double2* emb) {
+  const long N = 2L * (n_t - 1);
+  const long total = (long)n_lop * N;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    const int l = (int)(i / N);
+    const long k = i - (long)l * N;
+    const double nu = rot_nu(alpha, l, n_t);
+    double2 v;
+    if (k < n_t) {
+      v = cmul(alpha64(alpha, (size_t)l * n_t + k), rot(nu, k));
+    } else {
+      const long kk = N - k;  // 1 .. n_t-2
+      v = cconj(cmul(alpha64(alpha, (size_t)l * n_t + kk), rot(nu, kk)));
+    }
+    emb[i] = v;
+  }
+}
+
+// z (complex64) -> complex128 work array.
+__global__ void k_widen(const float2* z, long total, double2* zw) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x)
+    zw[i] = to_d(z[i]);
+}
+
+// zw <- zw * sqrt(max(Re(S), 0) / 2); counts clipped spectral values.
+__global__ void k_filter(const double2* spec, long total, double2* zw, unsigned long long* nneg) {
+  unsigned long long cnt = 0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    double s = spec[i].x;
+    if (s < 0.0) {
+      s = 0.0;
+      ++cnt;
+    }
+    zw[i] = cscale(zw[i], sqrt(s / 2.0));
+  }
+  if (cnt) atomicAdd(nneg, cnt);
+}
+
+// out[l][k] = ifft(...)[k] / N * conj(rot(k)), k < n_t.
+__global__ void k_unrotate(const double* alpha, const double2* y, int n_lop, int n_t,
+                           double2* out, float2* out64) {
+  const long N = 2L * (n_t - 1);
+  const long total = (long)n_lop * n_t;
+  const double invN = 1.0 / (double)N;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    const int l = (int)(i / n_t);
+    const long k = i - (long)l * n_t;
+    const double nu = rot_nu(alpha, l, n_t);
+    double2 v = cscale(y[(long)l * N + k], invN);
+    v = cmul(v, cconj(rot(nu, k)));
+    if (out) out[i] = v;
+    if (out64) out64[i] = mkf((float)v.x, (float)v.y);
+  }
+}
+
+static int grid_for(long n) {
+  long b = (n + 255) / 256;
+  if (b > 148L * 16) b = 148L * 16;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+extern "C" size_t hops_noise_filter_work_doubles(int32_t n_lop, int32_t n_t) {
+  return (size_t)4 * n_lop * 2 * (size_t)(n_t - 1) + 2;
+}
+
+extern "C" int hops_noise_filter(const double* alpha_dev, const float* z_dev, int32_t n_lop,
+                                 int32_t n_t, double* work_dev, double* out_dev, float* out64_dev,
+                                 int64_t* n_negative_host, void* stream) {
+  if (!alpha_dev || !z_dev || !work_dev || n_lop <= 0 || n_t < 3)
+    return nerr(HOPS_EINVAL, "hops_noise_filter: bad arguments (n_lop=%d n_t=%d)", n_lop, n_t);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int N = 2 * (n_t - 1);
+  const long total = (long)n_lop * N;
+  double2* emb = reinterpret_cast<double2*>(work_dev);
+  double2* zw = emb + total;
+  unsigned long long* nneg = reinterpret_cast<unsigned long long*>(zw + total);
+  cufftHandle plan;
+  if (cufftPlan1d(&plan, N, CUFFT_Z2Z, n_lop) != CUFFT_SUCCESS)
+    return nerr(HOPS_ECUDA, "cufftPlan1d(%d, batch %d) failed", N, n_lop);
+  int rc = HOPS_OK;
+  do {
+    if (cufftSetStream(plan, s) != CUFFT_SUCCESS) { rc = nerr(HOPS_ECUDA, "cufftSetStream failed"); break; }
+    if (cudaMemsetAsync(nneg, 0, sizeof(unsigned long long), s) != cudaSuccess) {
+      rc = nerr(HOPS_ECUDA, "memset failed");
+      break;
+    }
+    k_embed<<<grid_for(total), 256, 0, s>>>(alpha_dev, n_lop, n_t, emb);
+    if (cufftExecZ2Z(plan, (cufftDoubleComplex*)emb, (cufftDoubleComplex*)emb, CUFFT_FORWARD) != CUFFT_SUCCESS) {
+      rc = nerr(HOPS_ECUDA, "cufftExecZ2Z (embedding) failed");
+      break;
+    }
+    k_widen<<<grid_for(total), 256, 0, s>>>(reinterpret_cast<const float2*>(z_dev), total, zw);
+    if (cufftExecZ2Z(plan, (cufftDoubleComplex*)zw, (cufftDoubleComplex*)zw, CUFFT_FORWARD) != CUFFT_SUCCESS) {
+      rc = nerr(HOPS_ECUDA, "cufftExecZ2Z (noise) failed");
+      break;
+    }
+    k_filter<<<grid_for(total), 256, 0, s>>>(emb, total, zw, nneg);
+    if (cufftExecZ2Z(plan, (cufftDoubleComplex*)zw, (cufftDoubleComplex*)zw, CUFFT_INVERSE) != CUFFT_SUCCESS) {
+      rc = nerr(HOPS_ECUDA, "cufftExecZ2Z (inverse) failed");
+      break;
+    }
+    k_unrotate<<<grid_for((long)n_lop * n_t), 256, 0, s>>>(alpha_dev, zw, n_lop, n_t,
+                                                           reinterpret_cast<double2*>(out_dev),
+                                                           reinterpret_cast<float2*>(out64_dev));
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      rc = nerr(HOPS_ECUDA, "noise filter launch: %s", cudaGetErrorString(e));
+      break;
+    }
+    if (n_negative_host) {
+      unsigned long long h = 0;
+      if (cudaMemcpyAsync(&h, nneg, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+          cudaStreamSynchronize(s) != cudaSuccess) {
+        rc = nerr(HOPS_ECUDA, "reading the clip count failed");
+        break;
+      }
+      *n_negative_host = (int64_t)h;
+    }
+  } while (0);
+  cufftDestroy(plan);
+  return rc;
+}

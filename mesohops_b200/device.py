@@ -1,0 +1,181 @@
+"""Device-resident structure tables of one basis (system x hierarchy).
+
+``build_tables`` turns a state basis, a mode basis and an ``AuxBasis`` into the
+flat arrays of ``hops_structure`` (include/hops_b200.h); ``DeviceStructure``
+uploads them with torch and exposes the ctypes struct of device pointers.
+The arrays encode the super-operators of eom/eom_hops_ksuper.py:36-230:
+  K2_k      -> k_decay[a]            = -sum_m k_m(a) w_m
+  K2_kp1    -> up list (a, a+e_m, m)   with -(g_m/w_m) L_m applied in-kernel
+  K2_km1    -> down list (a, a-e_m, m, k_m(a) w_m) with L_m^H applied in-kernel
+  Z2_kp1    -> the same up list with (g_m/w_m) conj(<L>) applied in-kernel
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from ._lib import HopsStructure
+
+
+def _csr_of_dense(mats, n):
+    """CSR (absolute offsets) of a list of dense n x n complex matrices."""
+    ptr = np.zeros(len(mats) * (n + 1), dtype=np.int32)
+    cols, vals = [], []
+    off = 0
+    for j, A in enumerate(mats):
+        for r in range(n):
+            ptr[j * (n + 1) + r] = off
+            nz = np.nonzero(A[r])[0]
+            cols.extend(nz.tolist())
+            vals.extend(A[r, nz].tolist())
+            off += len(nz)
+        ptr[j * (n + 1) + n] = off
+    return ptr, np.array(cols, dtype=np.int32), np.array(vals, dtype=np.complex128)
+
+
+def _c2d(a):
+    """complex -> interleaved float64."""
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.complex128))
+    return a.view(np.float64).copy() if a.size else np.zeros(2, dtype=np.float64)
+
+
+def _c2f(a):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.complex64))
+    return a.view(np.float32).copy() if a.size else np.zeros(2, dtype=np.float32)
+
+
+def build_tables(system, basis, state_list=None, mode_list=None):
+    """Host arrays of one basis.
+
+    state_list: sorted absolute states of the state basis (default: all).
+    mode_list:  sorted absolute modes of the mode basis (default: basis.modes).
+    Returns a dict of numpy arrays and sizes plus index maps.
+    """
+    S_abs = system.n_state
+    states = np.arange(S_abs) if state_list is None else np.asarray(state_list, dtype=np.int64)
+    modes = basis.modes if mode_list is None else np.asarray(mode_list, dtype=np.int64)
+    S = len(states)
+    M = len(modes)
+    # relative L list: unique L of the basis modes, sorted (hops_modes.py:123-136)
+    l_abs = np.array(sorted(set(int(system.l_by_mode[m]) for m in modes)), dtype=np.int64)
+    L = len(l_abs)
+    l_rel_of_abs = {int(j): i for i, j in enumerate(l_abs)}
+    mode_lop = np.array([l_rel_of_abs[int(system.l_by_mode[m])] for m in modes], dtype=np.int32)
+    ix = np.ix_(states, states)
+    lops = [system.lops[j][ix] for j in l_abs]
+    lop_active = np.array([1 if np.any(l != 0) else 0 for l in lops], dtype=np.int32)
+    # site-projector form: exactly one diagonal nonzero
+    site = np.zeros(L, dtype=np.int32)
+    sval = np.zeros(L, dtype=np.complex128)
+    is_site = True
+    for j, l in enumerate(lops):
+        r, c = np.nonzero(l)
+        if len(r) == 1 and r[0] == c[0]:
+            site[j] = r[0]
+            sval[j] = l[r[0], c[0]]
+        elif len(r) == 0:
+            site[j] = -1
+        else:
+            is_site = False
+    l_ptr, l_col, l_val = _csr_of_dense(lops, S)
+    lh_ptr, lh_col, lh_val = _csr_of_dense([np.conj(l.T) for l in lops], S)
+    H = system.hamiltonian_dense()[ix]
+    h_ptr, h_col, h_val = _csr_of_dense([-1j * H], S)
+    G = system.G[modes]
+    W = system.W[modes]
+    counts = basis.counts
+    # K2_k diagonal (eom_hops_ksuper.py:78-87): -aux . W over the aux's own modes
+    k_decay = -(counts[:, modes].astype(np.float64) @ W) if M else np.zeros(basis.n_hier)
+    # connections are along basis.modes; remap to the relative mode list
+    rel_of_basis_mode = {int(m): i for i, m in enumerate(modes)}
+    up_m = np.array([rel_of_basis_mode[int(basis.modes[m])] for m in basis.up_m], dtype=np.int32)
+    dn_m = np.array([rel_of_basis_mode[int(basis.modes[m])] for m in basis.dn_m], dtype=np.int32)
+    dn_coef = basis.dn_k.astype(np.float64) * W[dn_m] if len(dn_m) else np.zeros(0, complex)
+    first = [(a, rel_of_basis_mode[int(basis.modes[m])]) for (a, m) in basis.first_level()]
+    first_aux = np.array([a for a, _ in first], dtype=np.int32)
+    first_mode = np.array([m for _, m in first], dtype=np.int32)
+    up_counts = np.diff(basis.up_ptr)
+    dn_counts = np.diff(basis.dn_ptr)
+    return dict(
+        n_hier=basis.n_hier, n_state=S, n_mode=M, n_lop=L,
+        states=states, modes=modes, l_abs=l_abs,
+        k_decay=k_decay, up_ptr=basis.up_ptr.astype(np.int32),
+        up_aux=basis.up_u.astype(np.int32), up_mode=up_m,
+        dn_ptr=basis.dn_ptr.astype(np.int32), dn_aux=basis.dn_d.astype(np.int32),
+        dn_mode=dn_m, dn_coef=dn_coef,
+        mode_lop=mode_lop, mode_g=G, mode_w=W, mode_gw=G / W if M else G,
+        first_aux=first_aux, first_mode=first_mode,
+        l_ptr=l_ptr, l_col=l_col, l_val=l_val, lh_ptr=lh_ptr, lh_col=lh_col, lh_val=lh_val,
+        lop_active=lop_active, lop_site=site, lop_sval=sval,
+        h_ptr=h_ptr, h_col=h_col, h_val=h_val, site_projector=int(is_site),
+        max_up=int(up_counts.max()) if len(up_counts) else 0,
+        max_dn=int(dn_counts.max()) if len(dn_counts) else 0,
+    )
+
+
+class DeviceStructure:
+    """hops_structure with its arrays resident on one CUDA device."""
+
+    def __init__(self, tables, device):
+        self.tables = tables
+        self.device = torch.device(device)
+        self._keep = []
+        t = tables
+
+        def up(arr, dtype):
+            a = np.ascontiguousarray(arr)
+            if a.size == 0:
+                a = np.zeros(2, dtype=a.dtype)
+            x = torch.from_numpy(a).to(self.device, dtype=dtype)
+            self._keep.append(x)
+            return x.data_ptr()
+
+        i32, f64, f32 = torch.int32, torch.float64, torch.float32
+        s = HopsStructure()
+        s.n_hier, s.n_state, s.n_mode, s.n_lop = t["n_hier"], t["n_state"], t["n_mode"], t["n_lop"]
+        s.n_first = len(t["first_aux"])
+        s.n_up = len(t["up_aux"])
+        s.n_dn = len(t["dn_aux"])
+        s.site_projector = t["site_projector"]
+        s.max_up, s.max_dn = t["max_up"], t["max_dn"]
+        s.k_decay = up(_c2d(t["k_decay"]), f64)
+        s.k_decay_f = up(_c2f(t["k_decay"]), f32)
+        s.up_ptr = up(t["up_ptr"], i32)
+        s.up_aux = up(t["up_aux"], i32)
+        s.up_mode = up(t["up_mode"], i32)
+        s.dn_ptr = up(t["dn_ptr"], i32)
+        s.dn_aux = up(t["dn_aux"], i32)
+        s.dn_mode = up(t["dn_mode"], i32)
+        s.dn_coef = up(_c2d(t["dn_coef"]), f64)
+        s.dn_coef_f = up(_c2f(t["dn_coef"]), f32)
+        s.mode_lop = up(t["mode_lop"], i32)
+        s.mode_g = up(_c2d(t["mode_g"]), f64)
+        s.mode_w = up(_c2d(t["mode_w"]), f64)
+        s.mode_gw = up(_c2d(t["mode_gw"]), f64)
+        s.mode_gw_f = up(_c2f(t["mode_gw"]), f32)
+        s.first_aux = up(t["first_aux"], i32)
+        s.first_mode = up(t["first_mode"], i32)
+        s.l_ptr = up(t["l_ptr"], i32)
+        s.l_col = up(t["l_col"], i32)
+        s.l_val = up(_c2d(t["l_val"]), f64)
+        s.l_val_f = up(_c2f(t["l_val"]), f32)
+        s.lh_ptr = up(t["lh_ptr"], i32)
+        s.lh_col = up(t["lh_col"], i32)
+        s.lh_val = up(_c2d(t["lh_val"]), f64)
+        s.lh_val_f = up(_c2f(t["lh_val"]), f32)
+        s.lop_active = up(t["lop_active"], i32)
+        s.lop_site = up(t["lop_site"], i32)
+        s.lop_sval = up(_c2d(t["lop_sval"]), f64)
+        s.h_ptr = up(t["h_ptr"], i32)
+        s.h_col = up(t["h_col"], i32)
+        s.h_val = up(_c2d(t["h_val"]), f64)
+        s.h_val_f = up(_c2f(t["h_val"]), f32)
+        self.cstruct = s
+        # a device copy of the struct itself (resident tasks point at it)
+        raw = np.frombuffer(bytes(s), dtype=np.uint8).copy()
+        self._dev_struct = torch.from_numpy(raw).to(self.device)
+        self.dev_ptr = self._dev_struct.data_ptr()
+
+    @property
+    def n_elem(self):
+        return self.tables["n_hier"] * self.tables["n_state"]

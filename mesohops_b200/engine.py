@@ -1,0 +1,221 @@
+"""Device state and launch wrappers around the C ABI.
+
+StreamBatch    -- B trajectories sharing one DeviceStructure, layout
+                  phi[a][b][s]; four streaming stage kernels (+ FP64 stage
+                  scalars) per RK4 step (hops_rk4_propagate).
+ResidentRunner -- any number of trajectories with their own (possibly
+                  different) structures; one CTA per trajectory runs every step
+                  of a call in one launch (hops_resident_propagate).
+Both keep all state on the device between calls; host copies happen only in
+set_state / get_state and for the stored psi trajectory.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import HopsBatch, HopsTask, PREC_C128, PREC_C64, EOM_CODES
+from .exceptions import TrajectoryError
+
+
+def precision_code(name):
+    if name in ("complex128", "c128", PREC_C128):
+        return PREC_C128
+    if name in ("complex64", "c64", PREC_C64):
+        return PREC_C64
+    raise ValueError(f"unknown precision {name}")
+
+
+def _stream(dev):
+    return torch.cuda.current_stream(dev).cuda_stream
+
+
+class StreamBatch:
+    """B trajectories sharing one structure, propagated by the streaming kernels."""
+
+    def __init__(self, dstruct, n_traj, precision="complex128", eom="NORMALIZED NONLINEAR"):
+        self.st = dstruct
+        self.dev = dstruct.device
+        t = dstruct.tables
+        self.B = int(n_traj)
+        self.S, self.N, self.M, self.L = t["n_state"], t["n_hier"], t["n_mode"], t["n_lop"]
+        self.prec = precision_code(precision)
+        self.eom = EOM_CODES[eom]
+        cdt = torch.complex128 if self.prec == PREC_C128 else torch.complex64
+        shape = (self.N, self.B, self.S)
+        self.phi = torch.zeros(shape, dtype=cdt, device=self.dev)
+        self.acc = torch.empty(shape, dtype=cdt, device=self.dev)
+        self.y0 = torch.empty(shape, dtype=cdt, device=self.dev)
+        self.y1 = torch.empty(shape, dtype=cdt, device=self.dev)
+        self.zmem = torch.zeros((self.B, max(self.M, 1)), dtype=torch.complex128, device=self.dev)
+        nws = int(_lib.lib().hops_scalar_workspace_doubles(self.S, self.M, self.L, self.B))
+        self.work = torch.zeros(nws, dtype=torch.float64, device=self.dev)
+        self.status = torch.zeros(self.B, dtype=torch.int32, device=self.dev)
+        self.noise1 = None
+        self.noise2 = None
+        b = HopsBatch()
+        b.n_traj, b.precision, b.eom = self.B, self.prec, self.eom
+        b.phi, b.acc, b.y0, b.y1 = (self.phi.data_ptr(), self.acc.data_ptr(),
+                                    self.y0.data_ptr(), self.y1.data_ptr())
+        b.zmem, b.work, b.status = self.zmem.data_ptr(), self.work.data_ptr(), self.status.data_ptr()
+        b.noise1 = b.noise2 = None
+        b.n_t1 = b.n_t2 = 0
+        self.cb = b
+        self.reset()
+
+    def reset(self):
+        rc = _lib.lib().hops_batch_reset(C.byref(self.st.cstruct), C.byref(self.cb), _stream(self.dev))
+        _lib.check(rc, "hops_batch_reset")
+
+    def set_noise(self, noise1, noise2=None):
+        """noise tensors [B, L, n_t] complex64 on the device (noise2 may be None)."""
+        self.noise1 = noise1.contiguous() if noise1 is not None else None
+        self.noise2 = noise2.contiguous() if noise2 is not None else None
+        self.cb.noise1 = self.noise1.data_ptr() if self.noise1 is not None else None
+        self.cb.n_t1 = self.noise1.shape[-1] if self.noise1 is not None else 0
+        self.cb.noise2 = self.noise2.data_ptr() if self.noise2 is not None else None
+        self.cb.n_t2 = self.noise2.shape[-1] if self.noise2 is not None else 0
+
+    def set_state(self, phi, zmem=None):
+        """phi: [B, N*S] complex (reference layout per trajectory); zmem: [B, M]."""
+        ph = torch.as_tensor(np.asarray(phi), dtype=torch.complex128).reshape(self.B, self.N, self.S)
+        self.phi.copy_(ph.permute(1, 0, 2).to(self.dev, dtype=self.phi.dtype))
+        if zmem is not None and self.M:
+            self.zmem.copy_(torch.as_tensor(np.asarray(zmem), dtype=torch.complex128).reshape(self.B, self.M))
+        self.reset()
+
+    def get_state(self):
+        ph = self.phi.permute(1, 0, 2).reshape(self.B, self.N * self.S).to(torch.complex128)
+        return ph.cpu().numpy(), self.zmem[:, :self.M].cpu().numpy()
+
+    def propagate(self, it0, di, n_steps, tau_over_hbar, psi_out=None):
+        """n_steps RK4 steps; psi_out: optional device tensor [n_steps, B, S] complex128."""
+        L = _lib.lib()
+        ptr = psi_out.data_ptr() if psi_out is not None else None
+        rc = L.hops_rk4_propagate(C.byref(self.st.cstruct), C.byref(self.cb), int(it0), int(di),
+                                  int(n_steps), float(tau_over_hbar), ptr, _stream(self.dev))
+        _lib.check(rc, "hops_rk4_propagate")
+
+    def check_status(self):
+        st = self.status.cpu().numpy()
+        if np.any(st != 0):
+            raise TrajectoryError(f"non-finite state in trajectories {np.nonzero(st)[0].tolist()}")
+
+    def dsystem_dt(self, z1, z2=None):
+        """One derivative of every trajectory at the current state.
+
+        z1, z2: [B, L] complex64 noise samples.  Returns (dphi [B, N*S] complex128
+        in cm^-1, dz [B, M] complex128).
+        """
+        z1d = torch.as_tensor(np.asarray(z1, dtype=np.complex64)).reshape(self.B, self.L).to(self.dev)
+        z2d = (torch.as_tensor(np.asarray(z2, dtype=np.complex64)).reshape(self.B, self.L).to(self.dev)
+               if z2 is not None else None)
+        dphi = torch.empty_like(self.phi)
+        dz = torch.empty((self.B, max(self.M, 1)), dtype=torch.complex128, device=self.dev)
+        rc = _lib.lib().hops_dsystem_dt(C.byref(self.st.cstruct), C.byref(self.cb), z1d.data_ptr(),
+                                        z2d.data_ptr() if z2d is not None else None,
+                                        dphi.data_ptr(), dz.data_ptr(), _stream(self.dev))
+        _lib.check(rc, "hops_dsystem_dt")
+        out = dphi.permute(1, 0, 2).reshape(self.B, self.N * self.S).to(torch.complex128)
+        return out.cpu().numpy(), dz[:, :self.M].cpu().numpy()
+
+
+class ResidentTrajectory:
+    """Device buffers of one trajectory for the resident kernel."""
+
+    def __init__(self, dstruct, precision="complex128", eom="NORMALIZED NONLINEAR"):
+        self.st = dstruct
+        self.dev = dstruct.device
+        t = dstruct.tables
+        self.S, self.N, self.M, self.L = t["n_state"], t["n_hier"], t["n_mode"], t["n_lop"]
+        self.prec = precision_code(precision)
+        self.eom = EOM_CODES[eom]
+        cdt = torch.complex128 if self.prec == PREC_C128 else torch.complex64
+        self.phi = torch.zeros(self.N * self.S, dtype=cdt, device=self.dev)
+        self.scratch = torch.empty(3 * self.N * self.S, dtype=cdt, device=self.dev)
+        self.zmem = torch.zeros(max(self.M, 1), dtype=torch.complex128, device=self.dev)
+        self.noise1 = None
+        self.noise2 = None
+        self.scale = 1.0
+        self.status = 0
+        self.sc_doubles = int(_lib.lib().hops_resident_scalar_doubles(self.S, self.M, self.L))
+
+    def set_state(self, phi, zmem=None):
+        self.phi.copy_(torch.as_tensor(np.asarray(phi), dtype=torch.complex128).to(self.dev, self.phi.dtype))
+        if zmem is not None and self.M:
+            self.zmem[:self.M].copy_(torch.as_tensor(np.asarray(zmem), dtype=torch.complex128))
+        self.scale = 1.0
+
+    def get_state(self):
+        return (self.phi.to(torch.complex128).cpu().numpy() * self.scale,
+                self.zmem[:self.M].cpu().numpy())
+
+    def set_noise(self, noise1, noise2=None):
+        """[L, n_t] complex64 device tensors."""
+        self.noise1 = noise1.contiguous() if noise1 is not None else None
+        self.noise2 = noise2.contiguous() if noise2 is not None else None
+
+
+class ResidentRunner:
+    """Launches hops_resident_propagate over a list of ResidentTrajectory."""
+
+    def __init__(self, device):
+        self.dev = torch.device(device)
+
+    def run(self, trajs, it0, di, n_steps, tau_over_hbar, psi_out=None):
+        """Propagate every trajectory n_steps steps in one launch.
+
+        it0, di, n_steps, tau_over_hbar may be scalars or per-trajectory lists.
+        psi_out: optional list of device tensors [n_steps_i, S_i] complex128.
+        Returns the per-trajectory status array.
+        """
+        n = len(trajs)
+        if n == 0:
+            return np.zeros(0, dtype=np.int32)
+        prec = trajs[0].prec
+        if any(t.prec != prec for t in trajs):
+            raise ValueError("one resident launch needs one precision")
+
+        def per(x, i):
+            return x[i] if isinstance(x, (list, tuple, np.ndarray)) else x
+
+        tasks = (HopsTask * n)()
+        for i, tr in enumerate(trajs):
+            tk = tasks[i]
+            tk.st = tr.st.dev_ptr
+            tk.phi = tr.phi.data_ptr()
+            tk.zmem = tr.zmem.data_ptr()
+            tk.noise1 = tr.noise1.data_ptr() if tr.noise1 is not None else None
+            tk.noise2 = tr.noise2.data_ptr() if tr.noise2 is not None else None
+            tk.n_t1 = tr.noise1.shape[-1] if tr.noise1 is not None else 0
+            tk.n_t2 = tr.noise2.shape[-1] if tr.noise2 is not None else 0
+            tk.psi_out = psi_out[i].data_ptr() if psi_out is not None and psi_out[i] is not None else None
+            tk.scratch = tr.scratch.data_ptr()
+            tk.it0, tk.di, tk.n_steps = int(per(it0, i)), int(per(di, i)), int(per(n_steps, i))
+            last = tk.it0 + 2 * tk.n_steps * tk.di
+            if tk.n_steps > 0 and ((tr.noise1 is not None and last >= tk.n_t1)
+                                   or (tr.noise2 is not None and last >= tk.n_t2)):
+                raise TrajectoryError("Trajectory times longer than the noise time axis")
+            tk.precision = prec
+            tk.eom = tr.eom
+            tk.status = 0
+            tk.tau_over_hbar = float(per(tau_over_hbar, i))
+            tk.scale = tr.scale
+        raw = np.frombuffer(bytes(tasks), dtype=np.uint8).copy()
+        tdev = torch.from_numpy(raw).to(self.dev)
+        max_elems = max(t.N * t.S for t in trajs)
+        max_sc = max(t.sc_doubles for t in trajs)
+        site = int(all(t.st.tables["site_projector"] for t in trajs))
+        rc = _lib.lib().hops_resident_propagate(tdev.data_ptr(), n, max_elems, max_sc, prec, site,
+                                                _stream(self.dev))
+        _lib.check(rc, "hops_resident_propagate")
+        back = tdev.cpu().numpy().tobytes()
+        out = (HopsTask * n).from_buffer_copy(back)
+        status = np.array([out[i].status for i in range(n)], dtype=np.int32)
+        for i, tr in enumerate(trajs):
+            tr.scale = 1.0
+            tr.status = int(status[i])
+        return status

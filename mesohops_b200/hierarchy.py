@@ -1,0 +1,230 @@
+"""Auxiliary hierarchy: generation, ordering and connection tables.
+
+Aux vectors are rows of an integer count matrix [n_hier, n_mode].  Their order
+is the reference's: basis/hops_aux.py:171-201,460-480 sorts by an id string that
+lists each mode index (zero-padded to a fixed width) once per unit of depth,
+shorter strings first and then lexicographically -- i.e. by total depth, then
+lexicographically by the sorted tuple of modes.  For a full triangular
+hierarchy that is the generation order of hops_hierarchy.py:340-368.
+
+Instead of string ids this module ranks each aux exactly: the sorted mode
+tuple c_0 <= ... <= c_{k-1} maps to the strictly increasing b_i = c_i + i in
+[0, n), n = M + k - 1, whose lexicographic rank among the C(n, k)
+combinations is sum_i C(n-1-b_{i-1}, k-i) - C(n-b_i, k-i) (b_{-1} = -1).
+Adding the number of aux of depth < k gives a global key whose order equals
+the reference order, so any aux subset is sorted, and neighbours are found,
+with integer arithmetic (searchsorted) instead of string manipulation.
+"""
+from __future__ import annotations
+
+from math import comb
+
+import numpy as np
+
+from .exceptions import AuxError, UnsupportedRequest
+
+
+def _binom_table(nmax, kmax):
+    t = np.zeros((nmax + 1, kmax + 1), dtype=object)
+    for n in range(nmax + 1):
+        for k in range(kmax + 1):
+            t[n, k] = comb(n, k)
+    return t
+
+
+class AuxKeyer:
+    """Exact global keys of aux vectors for n_mode modes and depth <= maxhier."""
+
+    def __init__(self, n_mode, maxhier):
+        self.M = int(n_mode)
+        self.D = int(maxhier)
+        total = comb(self.M + self.D, self.D)  # aux of depth <= D
+        self.use_int64 = total < (1 << 62)
+        # offsets[k] = number of aux with depth < k = C(M + k - 1, k - 1)
+        self.offsets = [0] + [comb(self.M + k - 1, k - 1) for k in range(1, self.D + 2)]
+        nmax = self.M + self.D
+        self.binom = _binom_table(nmax + 1, self.D + 1)
+        if self.use_int64:
+            self.binom64 = self.binom.astype(np.int64)
+
+    def keys_from_counts(self, counts):
+        """Global keys of aux given as a count matrix [N, M] (any int dtype)."""
+        counts = np.asarray(counts)
+        N = counts.shape[0]
+        depth = counts.sum(axis=1).astype(np.int64)
+        if depth.size and depth.max() > self.D:
+            raise AuxError("aux deeper than MAXHIER")
+        keys = np.zeros(N, dtype=np.int64 if self.use_int64 else object)
+        for k in np.unique(depth):
+            idx = np.nonzero(depth == k)[0]
+            if k == 0:
+                keys[idx] = 0
+                continue
+            sub = counts[idx]
+            # sorted mode tuples of depth k (repeat mode m counts[m] times)
+            rows = np.repeat(np.arange(len(idx)), sub.sum(axis=1))
+            modes = np.nonzero(sub)[1]
+            reps = sub[sub > 0]
+            tup = np.repeat(modes, reps).reshape(len(idx), k)
+            keys[idx] = self._rank(tup, int(k)) + self.offsets[k]
+            del rows
+        return keys
+
+    def _rank(self, tup, k):
+        n = self.M + k - 1
+        b = tup.astype(np.int64) + np.arange(k, dtype=np.int64)[None, :]
+        if self.use_int64:
+            B = self.binom64
+            r = np.zeros(len(tup), dtype=np.int64)
+            prev = np.full(len(tup), -1, dtype=np.int64)
+            for i in range(k):
+                r += B[n - 1 - prev, k - i] - B[n - b[:, i], k - i]
+                prev = b[:, i]
+            return r
+        B = self.binom
+        r = np.zeros(len(tup), dtype=object)
+        prev = np.full(len(tup), -1, dtype=np.int64)
+        for i in range(k):
+            r = r + B[n - 1 - prev, k - i] - B[n - b[:, i], k - i]
+            prev = b[:, i]
+        return r
+
+
+def triangular_counts(n_mode, maxhier):
+    """Count matrix of every aux with depth <= maxhier, in reference order."""
+    blocks = [np.zeros((1, n_mode), dtype=np.int16)]
+    # sorted tuples of depth k in lexicographic order, built from depth k-1 by
+    # appending every mode >= the last one (hops_hierarchy.py:340-368)
+    prev = np.zeros((1, 0), dtype=np.int32)
+    for k in range(1, maxhier + 1):
+        last = prev[:, -1] if k > 1 else np.zeros(1, dtype=np.int32)
+        cnt = n_mode - last
+        rep = np.repeat(np.arange(len(prev)), cnt)
+        starts = np.repeat(last, cnt)
+        offs = np.arange(cnt.sum()) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+        new_last = (starts + offs).astype(np.int32)
+        cur = np.concatenate([prev[rep], new_last[:, None]], axis=1)
+        c = np.zeros((len(cur), n_mode), dtype=np.int16)
+        np.add.at(c, (np.repeat(np.arange(len(cur)), k), cur.ravel()), 1)
+        blocks.append(c)
+        prev = cur
+    return np.concatenate(blocks, axis=0)
+
+
+def apply_static_filters(counts, filters, n_mode):
+    """STATIC_FILTERS of basis/hierarchy_functions.py:7-140 on a count matrix."""
+    keep = np.ones(len(counts), dtype=bool)
+    total = counts.sum(axis=1)
+    for item in filters:
+        name, param = item[0], item[1]
+        if name == "Triangular":
+            mask = np.asarray(param[0], dtype=bool)
+            if len(mask) != n_mode:
+                raise UnsupportedRequest("The number of entries in the list of static filter "
+                                         "booleans does not match the number of hierarchy "
+                                         "modes", "hierarchy_static_filter", override=True)
+            keep &= counts[:, mask].sum(axis=1) <= param[1]
+        elif name == "LongEdge":
+            mask = np.asarray(param[0], dtype=bool)
+            if len(mask) != n_mode:
+                raise UnsupportedRequest("The number of entries in the list of static filter "
+                                         "booleans does not match the number of hierarchy "
+                                         "modes", "hierarchy_static_filter", override=True)
+            keep &= ((total <= param[1]) | (counts[:, mask].sum(axis=1) == 0)
+                     | ((counts > 0).sum(axis=1) <= 1))
+        elif name == "Markovian":
+            mask = np.asarray(param, dtype=bool)
+            if len(mask) != n_mode:
+                raise UnsupportedRequest("The number of entries in the list of static filter "
+                                         "booleans does not match the number of hierarchy "
+                                         "modes", "hierarchy_static_filter", override=True)
+            touches = (counts[:, mask] > 0).any(axis=1)
+            keep &= (total == 0) | ~(touches & (total > 1))
+        else:
+            raise UnsupportedRequest(name, "hierarchy_static_filter")
+    return counts[keep]
+
+
+class AuxBasis:
+    """A sorted aux list with its up/down connection tables.
+
+    counts: [n_hier, n_mode_abs] aux count matrix (absolute modes).
+    modes:  sorted absolute modes of the current mode basis (relative index =
+            position in this list); connections are built along these modes.
+    """
+
+    def __init__(self, counts, keyer, maxhier, modes=None):
+        counts = np.asarray(counts)
+        keys = keyer.keys_from_counts(counts)
+        order = np.argsort(keys, kind="stable")
+        self.counts = counts[order]
+        self.keys = keys[order]
+        if len(self.keys) == 0 or self.counts[0].sum() != 0:
+            raise AuxError("Zero Vector not contained in list_aux!")
+        self.keyer = keyer
+        self.maxhier = maxhier
+        self.n_hier = len(self.counts)
+        n_mode_abs = self.counts.shape[1]
+        self.modes = np.arange(n_mode_abs) if modes is None else np.asarray(modes, dtype=np.int64)
+        self.depth = self.counts.sum(axis=1).astype(np.int64)
+        self._build_connections()
+
+    def index_of(self, counts):
+        """Indices of the given aux (count rows) in this basis, -1 if absent."""
+        k = self.keyer.keys_from_counts(counts)
+        pos = np.searchsorted(self.keys, k)
+        pos = np.minimum(pos, self.n_hier - 1)
+        found = self.keys[pos] == k
+        return np.where(found, pos, -1).astype(np.int64)
+
+    def _build_connections(self):
+        """k+1 / k-1 connections along the basis modes (hops_hierarchy.py:470-523)."""
+        ups_a, ups_u, ups_m = [], [], []
+        below = np.nonzero(self.depth < self.maxhier)[0]
+        for rel, m in enumerate(self.modes):
+            if len(below) == 0:
+                break
+            up = self.counts[below].copy()
+            up[:, m] += 1
+            idx = self.index_of(up)
+            ok = idx >= 0
+            ups_a.append(below[ok])
+            ups_u.append(idx[ok])
+            ups_m.append(np.full(ok.sum(), rel, dtype=np.int64))
+        if ups_a:
+            a = np.concatenate(ups_a)
+            u = np.concatenate(ups_u)
+            m = np.concatenate(ups_m)
+        else:
+            a = u = m = np.zeros(0, dtype=np.int64)
+        o = np.lexsort((m, a))
+        self.up_a, self.up_u, self.up_m = a[o], u[o], m[o]
+        o = np.lexsort((m, u))
+        self.dn_a, self.dn_d, self.dn_m = u[o], a[o], m[o]
+        # depth of the higher aux in the connecting mode (k_m(a) of the down term)
+        self.dn_k = self.counts[self.dn_a, self.modes[self.dn_m]].astype(np.int64)
+        self.up_ptr = np.zeros(self.n_hier + 1, dtype=np.int64)
+        np.add.at(self.up_ptr, self.up_a + 1, 1)
+        self.up_ptr = np.cumsum(self.up_ptr)
+        self.dn_ptr = np.zeros(self.n_hier + 1, dtype=np.int64)
+        np.add.at(self.dn_ptr, self.dn_a + 1, 1)
+        self.dn_ptr = np.cumsum(self.dn_ptr)
+
+    def first_level(self):
+        """(aux index, relative mode) of every depth-1 aux along a basis mode."""
+        out = []
+        for rel, m in enumerate(self.modes):
+            e = np.zeros((1, self.counts.shape[1]), dtype=self.counts.dtype)
+            e[0, m] = 1
+            i = int(self.index_of(e)[0])
+            if i >= 0:
+                out.append((i, rel))
+        return out
+
+
+def triangular_basis(n_mode, maxhier, static_filters=()):
+    keyer = AuxKeyer(n_mode, maxhier)
+    counts = triangular_counts(n_mode, maxhier)
+    if static_filters:
+        counts = apply_static_filters(counts, static_filters, n_mode)
+    return AuxBasis(counts, keyer, maxhier)

@@ -1,0 +1,187 @@
+"""HOPS noise on the device (mirror of noise/hops_noise.py).
+
+Models: FFT_FILTER (correlated complex Gaussian noise), PRE_CALCULATED (a
+given correlated trajectory) and ZERO.  The raw white noise is drawn on the
+host with numpy's PCG64(SEED).jumped(lop) stream, exactly as the reference does
+(hops_noise.py:558-628), so a SEED gives the same raw draws; the circulant-
+embedding filter (hops_noise.py:630-716) runs in FP64 on the GPU through
+``hops_noise_filter``.  The correlated noise is stored as complex64
+(hops_noise.py:247), one row per unique L-operator.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+import torch
+
+from . import _lib
+from .constants import precision
+from .exceptions import UnsupportedRequest
+from .params import NOISE_DICT_DEFAULT, NOISE_DICT_TYPES, initialize_dict
+
+
+def raw_slot_index(ntaus):
+    """Assignment of the 4(n_t-1) draws to the 2(n_t-1) complex samples.
+
+    Keeps the draw used by each time slot independent of the trajectory length
+    (hops_noise.py:592-628): slot j takes draw re[j] for its real part (or
+    Box-Muller radius) and im[j] for its imaginary part (or phase).
+    """
+    n1 = ntaus - 1
+    re = np.concatenate([[0], np.arange(2, 4 * (ntaus - 2), 4), [4 * n1 - 2],
+                         np.arange(4 * (ntaus - 2), 3, -4)]).astype(np.int64)
+    im = np.concatenate([[1], np.arange(3, 4 * (ntaus - 1) - 1, 4), [4 * n1 - 1],
+                         np.arange(4 * (n1 - 1) + 1, 4, -4)]).astype(np.int64)
+    return re, im
+
+
+def raw_white_noise(seed, lops, ntaus, rand_model="SUM_GAUSSIAN"):
+    """Uncorrelated complex64 draws [len(lops), 2(ntaus-1)] (hops_noise.py:453-590)."""
+    re, im = raw_slot_index(ntaus)
+    out = np.empty((len(lops), 2 * (ntaus - 1)), dtype=np.complex64)
+    for i, lop in enumerate(lops):
+        gen = np.random.default_rng(np.random.PCG64(seed=seed).jumped(int(lop)))
+        if rand_model == "SUM_GAUSSIAN":
+            x = gen.normal(loc=0, size=4 * (ntaus - 1))
+            out[i] = np.complex64(x[re] + 1j * x[im])
+        elif rand_model == "BOX_MULLER":
+            x = gen.random(size=4 * (ntaus - 1))
+            out[i] = np.complex64(np.sqrt(-2.0 * np.log(x[re])) * np.exp(2.0j * np.pi * x[im]))
+        else:
+            raise UnsupportedRequest(f"Noise.param[RAND_MODEL] {rand_model}",
+                                     "Noise._prepare_rand")
+    return out
+
+
+def filter_on_device(alpha, z_raw, device):
+    """FP64 circulant-embedding filter on the GPU.
+
+    alpha: complex128 [R, n_t] correlation functions; z_raw: complex64
+    [R, 2(n_t-1)].  Returns (complex64 device tensor [R, n_t], number of
+    clipped negative spectral values).
+    """
+    L = _lib.lib()
+    R, n_t = alpha.shape
+    dev = torch.device(device)
+    a = torch.from_numpy(np.ascontiguousarray(alpha, dtype=np.complex128)).to(dev)
+    z = torch.from_numpy(np.ascontiguousarray(z_raw, dtype=np.complex64)).to(dev)
+    work = torch.empty(int(L.hops_noise_filter_work_doubles(R, n_t)), dtype=torch.float64, device=dev)
+    out64 = torch.empty((R, n_t), dtype=torch.complex64, device=dev)
+    nneg = C.c_int64(0)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    rc = L.hops_noise_filter(a.data_ptr(), z.data_ptr(), R, n_t, work.data_ptr(), None,
+                             out64.data_ptr(), C.byref(nneg), stream)
+    _lib.check(rc, "hops_noise_filter")
+    return out64, int(nneg.value)
+
+
+class HopsNoise:
+    """One noise trajectory (noise 1 or noise 2) of a HOPS trajectory."""
+
+    def __init__(self, noise_param, system, noise_type=1):
+        p = dict(noise_param)
+        if noise_type == 2 and "FLAG_REAL" not in p and p.get("MODEL") != "ZERO":
+            p["FLAG_REAL"] = True   # prepare_functions.py:72-77
+        self.param = initialize_dict(p, NOISE_DICT_DEFAULT, NOISE_DICT_TYPES, "HopsNoise")
+        if self.param["INTERPOLATE"]:
+            raise UnsupportedRequest("INTERPOLATE = True (cubic noise interpolation)",
+                                     "mesohops_b200 HopsNoise")
+        self.system = system
+        self.noise_type = noise_type
+        n_t = int(np.ceil(self.param["TLEN"] / self.param["TAU"])) + 1
+        self.param["T_AXIS"] = np.arange(n_t) * self.param["TAU"]
+        self.n_t = n_t
+        self.n_lop = system.n_lop
+        self._dev = None
+        self._host = None
+        self.n_clipped = 0
+
+    # ------------------------------------------------------------------
+    def _corr(self):
+        """alpha per unique L on the noise time axis (hops_noise.py:167-192)."""
+        sysm = self.system
+        if self.noise_type == 1:
+            fn, params, by_l = sysm.alpha1, sysm.param_noise1, sysm.nmodes1_by_l
+        else:
+            fn, params, by_l = sysm.alpha2, sysm.param_noise2, sysm.nmodes2_by_l
+        t = self.param["T_AXIS"]
+        alpha = np.zeros((self.n_lop, len(t)), dtype=np.complex128)
+        for j, modes in enumerate(by_l):
+            for i in modes:
+                alpha[j] += fn(t, *params[i])
+        return alpha
+
+    def _uncorrelated(self):
+        seed = self.param["SEED"]
+        shape = (self.n_lop, 2 * (self.n_t - 1))
+        if isinstance(seed, str):
+            if not os.path.isfile(seed) or seed[-4:] != ".npy":
+                raise UnsupportedRequest(f"Noise.param[SEED] {seed} is not a valid .npy file",
+                                         "Noise._prepare_rand", True)
+            seed = np.load(seed)
+        if isinstance(seed, np.ndarray):
+            if seed.shape != shape:
+                raise UnsupportedRequest("Noise.param[SEED] is an array of the wrong length",
+                                         "Noise._prepare_rand", True)
+            return seed
+        return raw_white_noise(seed, range(self.n_lop), self.n_t, self.param["RAND_MODEL"])
+
+    def prepare(self, device):
+        """Correlated noise as a complex64 device tensor [n_lop, n_t] (None for ZERO)."""
+        if self._dev is not None or self.param["MODEL"] == "ZERO":
+            return self._dev
+        model = self.param["MODEL"]
+        if model == "FFT_FILTER":
+            z = self._uncorrelated()
+            if self.param["STORE_RAW_NOISE"]:
+                self.param["Z_UNCORRELATED"] = z
+            noise, self.n_clipped = filter_on_device(self._corr(), z, device)
+        elif model == "PRE_CALCULATED":
+            seed = self.param["SEED"]
+            if isinstance(seed, str):
+                if not os.path.isfile(seed) or seed[-4:] != ".npy":
+                    raise UnsupportedRequest(f"Noise.param[SEED] {seed} is not a valid .npy "
+                                             "file", "Noise.prepare_noise", True)
+                seed = np.load(seed)
+            if not isinstance(seed, (list, np.ndarray)):
+                raise UnsupportedRequest(f"Noise.param[SEED] of type {type(seed)}",
+                                         "Noise.prepare_noise")
+            seed = np.asarray(seed)
+            if seed.shape != (self.n_lop, self.n_t):
+                raise UnsupportedRequest("Noise.param[SEED] is an array of the wrong length",
+                                         "Noise.prepare_noise", True)
+            noise = torch.from_numpy(np.ascontiguousarray(seed.astype(np.complex64))).to(device)
+        else:
+            raise UnsupportedRequest(f"Noise.param[MODEL] {model}", "Noise.prepare_noise")
+        if self.param["FLAG_REAL"]:
+            noise = torch.complex(noise.real, torch.zeros_like(noise.real))
+        self._dev = noise.contiguous()
+        return self._dev
+
+    def host(self):
+        if self._host is None and self._dev is not None:
+            self._host = self._dev.cpu().numpy()
+        return self._host
+
+    def time_index(self, t):
+        """Exact index of time t on the noise axis (hops_noise.py:437-447)."""
+        it = int(round(t / self.param["TAU"]))
+        if it < 0 or it >= self.n_t or abs(it * self.param["TAU"] - t) >= precision:
+            raise UnsupportedRequest("Off axis t-samples when INTERPOLATE = False",
+                                     "NoiseModel.get_noise()")
+        return it
+
+    def get_noise(self, t_axis, list_lop=None):
+        """complex64 [len(list_lop), len(t_axis)] samples (hops_noise.py:339-451)."""
+        if list_lop is None:
+            list_lop = np.arange(self.n_lop)
+        if self.param["MODEL"] == "ZERO":
+            return np.zeros((len(list_lop), len(t_axis)), dtype=np.complex64)
+        if self._dev is None:
+            self.prepare("cuda")
+        h = self.host()
+        idx = [self.time_index(t) for t in t_axis]
+        return np.ascontiguousarray(h[np.ix_(np.asarray(list_lop, dtype=np.int64), idx)],
+                                    dtype=np.complex64)

@@ -1,0 +1,270 @@
+"""Drop-in HopsTrajectory running the trajectory hot path on a B200.
+
+Same constructor, parameter dictionaries, ``initialize(psi_0)``,
+``propagate(t_advance, tau)`` and read-outs (``phi``, ``psi``, ``z_mem``,
+``t``, ``storage``) as trajectory/hops_trajectory.py:84-538 of MesoHOPS.  The
+loop body -- noise sampling at t, t+tau/2, t+tau (integrator_rk.py:78-134), the
+RK4 step over the nonlinear HOPS equation (integrator_rk.py:10-75,
+hops_eom.py:196-441) and the renormalisation (hops_trajectory.py:616-634) --
+runs as CUDA kernels; the state stays on the device between calls.
+
+Options of this implementation go in the separate ``device_param`` dictionary
+(PRECISION, DEVICE, KERNEL); the reference dictionaries are validated exactly as
+MesoHOPS validates them.
+"""
+from __future__ import annotations
+
+import time as timer
+
+import numpy as np
+import torch
+
+from .constants import hbar, precision
+from .device import DeviceStructure, build_tables
+from .engine import ResidentRunner, ResidentTrajectory, StreamBatch
+from .exceptions import LockedException, TrajectoryError, UnsupportedRequest
+from .hierarchy import triangular_basis
+from .noise import HopsNoise
+from .params import (DEVICE_DICT_DEFAULT, EOM_DICT_DEFAULT, EOM_DICT_TYPES,
+                     HIERARCHY_DICT_DEFAULT, HIERARCHY_DICT_TYPES, INTEGRATION_DICT_DEFAULT,
+                     INTEGRATION_DICT_TYPES, initialize_dict)
+from .storage import HopsStorage
+from .system import HopsSystem
+
+# Resident (one CTA per trajectory) path when the four stage vectors fit the
+# per-CTA shared memory budget; larger problems use the streaming kernels.
+RESIDENT_MAX_BYTES = 200 * 1024
+
+
+def choose_kernel(n_elem, prec_bytes, requested="auto"):
+    if requested in ("resident", "streaming"):
+        return requested
+    return "resident" if 4 * n_elem * prec_bytes <= RESIDENT_MAX_BYTES else "streaming"
+
+
+class HopsTrajectory:
+    """One HOPS trajectory (drop-in for mesohops.trajectory.hops_trajectory)."""
+
+    def __init__(self, system_param=None, eom_param=None, noise_param=None,
+                 noise2_param=None, hierarchy_param=None, storage_param=None,
+                 integration_param=None, device_param=None):
+        system_param = {} if system_param is None else system_param
+        self.eom_param = initialize_dict(eom_param or {}, EOM_DICT_DEFAULT, EOM_DICT_TYPES,
+                                         "HopsEOM")
+        eom = self.eom_param["EQUATION_OF_MOTION"]
+        if eom not in ("NORMALIZED NONLINEAR", "NONLINEAR", "LINEAR"):
+            raise UnsupportedRequest("EQUATION_OF_MOTION =" + eom, "HopsEOM")
+        if self.eom_param["ADAPTIVE_H"] or self.eom_param["ADAPTIVE_S"]:
+            raise UnsupportedRequest("adaptive eom_param (use make_adaptive)", "HopsTrajectory")
+        self.eom_param["ADAPTIVE"] = False
+        self.system = HopsSystem(system_param)
+        self.hierarchy_param = initialize_dict(hierarchy_param or {}, HIERARCHY_DICT_DEFAULT,
+                                               HIERARCHY_DICT_TYPES, "HopsHierarchy")
+        if self.hierarchy_param["MAXHIER"] > 255:
+            self.hierarchy_param["MAXHIER"] = 255
+        if self.hierarchy_param["TERMINATOR"]:
+            raise UnsupportedRequest("TERMINATOR", "HopsHierarchy")
+        noise_param = {} if noise_param is None else noise_param
+        if noise2_param is None:
+            noise2_param = {"TLEN": noise_param.get("TLEN", 1000.0),
+                            "TAU": noise_param.get("TAU", 1.0), "MODEL": "ZERO", "SEED": None}
+        self.noise_param = noise_param
+        self.noise2_param = noise2_param
+        self.noise1 = HopsNoise(noise_param, self.system, noise_type=1)
+        self.noise2 = HopsNoise(noise2_param, self.system, noise_type=2)
+        if integration_param is None:
+            integration_param = INTEGRATION_DICT_DEFAULT
+        self.integration_param = initialize_dict(integration_param, INTEGRATION_DICT_DEFAULT,
+                                                 INTEGRATION_DICT_TYPES,
+                                                 "integration_param in the HopsTrajectory "
+                                                 "initialization")
+        if self.integration_param["INTEGRATOR"] != "RUNGE_KUTTA":
+            raise UnsupportedRequest("Integrator of type " + str(self.integration_param["INTEGRATOR"]),
+                                     type(self).__name__)
+        if self.integration_param["EFFECTIVE_NOISE_INTEGRATION"]:
+            raise UnsupportedRequest("EFFECTIVE_NOISE_INTEGRATION", "mesohops_b200 HopsTrajectory")
+        self.integrator_step = 0.5
+        self.device_param = dict(DEVICE_DICT_DEFAULT)
+        self.device_param.update(device_param or {})
+        self.storage = HopsStorage(False, storage_param)
+        self.__initialized__ = False
+        self._t = 0.0
+        self._runner = None
+
+    # ------------------------------------------------------------------ setup
+    def initialize(self, psi_0, timer_checkpoint=None):
+        """Build the hierarchy, upload the structure, set phi_0 = [psi_0, 0, ...]."""
+        t0 = timer.time() if timer_checkpoint is None else timer_checkpoint
+        if self.__initialized__:
+            raise LockedException("HopsTrajectory.initialize()", "HopsTrajectory")
+        psi_0 = np.array(psi_0, dtype=np.complex128)
+        dev = torch.device(self.device_param["DEVICE"])
+        self.basis = triangular_basis(self.system.n_mode, self.hierarchy_param["MAXHIER"],
+                                      self.hierarchy_param["STATIC_FILTERS"])
+        self.dstruct = DeviceStructure(build_tables(self.system, self.basis), dev)
+        prec = self.device_param["PRECISION"]
+        prec_bytes = 16 if prec in ("complex128", "c128") else 8
+        n_elem = self.dstruct.n_elem
+        self.kernel = choose_kernel(n_elem, prec_bytes, self.device_param["KERNEL"])
+        eom = self.eom_param["EQUATION_OF_MOTION"]
+        if self.kernel == "resident":
+            self._traj = ResidentTrajectory(self.dstruct, prec, eom)
+            self._runner = ResidentRunner(dev)
+        else:
+            self._traj = StreamBatch(self.dstruct, 1, prec, eom)
+        phi0 = np.zeros(n_elem, dtype=np.complex128)
+        phi0[:self.n_state] = psi_0[self.state_list]
+        self._set_state(phi0, np.zeros(self.system.n_mode, dtype=np.complex128))
+        n1 = self.noise1.prepare(dev)
+        n2 = self.noise2.prepare(dev)
+        self._bind_noise(n1, n2)
+        self._t = 0.0
+        self.storage.store(0.0, psi=phi0[:self.n_state].copy(), phi=phi0.copy(),
+                           z_mem=np.zeros(self.system.n_mode, dtype=np.complex128))
+        self.storage.metadata["INITIALIZATION_TIME"] = timer.time() - t0
+        self.__initialized__ = True
+
+    def _bind_noise(self, n1, n2):
+        self._n1, self._n2 = n1, n2
+        if self.kernel == "resident":
+            self._traj.set_noise(n1, n2)
+        else:
+            self._traj.set_noise(n1.unsqueeze(0) if n1 is not None else None,
+                                 n2.unsqueeze(0) if n2 is not None else None)
+
+    def _set_state(self, phi, zmem):
+        if self.kernel == "resident":
+            self._traj.set_state(phi, zmem)
+        else:
+            self._traj.set_state(phi.reshape(1, -1), zmem.reshape(1, -1))
+
+    def make_adaptive(self, delta_a=1e-4, delta_s=1e-4, update_step=1, f_discard=0.01,
+                      adaptive_noise=True):
+        raise UnsupportedRequest("make_adaptive on HopsTrajectory (use "
+                                 "mesohops_b200.adaptive.AdaptiveTrajectory)", "HopsTrajectory")
+
+    # -------------------------------------------------------------- propagate
+    def _check_tau_step(self, tau):
+        """hops_trajectory.py:579-614"""
+        ok = True
+        for nz in (self.noise1, self.noise2):
+            ts = tau * self.integrator_step / nz.param["TAU"]
+            ok &= (ts - int(round(ts))) < precision
+            ok &= int(round(tau / nz.param["TAU"])) >= 1
+        return ok
+
+    def propagate(self, t_advance, tau, timer_checkpoint=None):
+        t_start = timer.time() if timer_checkpoint is None else timer_checkpoint
+        if not self.__initialized__:
+            raise TrajectoryError("propagate called before initialize")
+        t0 = self.t
+        if not self._check_tau_step(tau):
+            raise TrajectoryError(f"Timesteps({tau * self.integrator_step}) that do not match "
+                                  f"noise.param['TAU'] ({self.noise1.param['TAU']})")
+        if (t0 + t_advance + tau) > self.noise1.param["TLEN"]:
+            raise TrajectoryError("Trajectory times longer than noise.param['TLEN'] ="
+                                  + str(self.noise1.param["TLEN"]))
+        n_steps = int(np.ceil(t_advance / tau))
+        t_axis = t0 + np.arange(1, 1 + n_steps) * tau
+        if n_steps == 0:
+            return
+        it0 = self.noise1.time_index(t0)
+        di = int(round(tau * 0.5 / self.noise1.param["TAU"]))
+        self._align_noise2(it0, di, n_steps)
+        h = tau / hbar
+        dev = self.dstruct.device
+        psi_dev = torch.empty((n_steps, self.n_state), dtype=torch.complex128, device=dev)
+        if self.kernel == "resident":
+            st = self._runner.run([self._traj], it0, di, n_steps, h, psi_out=[psi_dev])
+            if st[0] != 0:
+                raise TrajectoryError("non-finite state during propagation")
+        else:
+            self._traj.propagate(it0, di, n_steps, h, psi_out=psi_dev.view(n_steps, 1, self.n_state))
+            self._traj.check_status()
+        psi = psi_dev.cpu().numpy()
+        need_phi = "phi_traj" in self.storage.data or "z_mem" in self.storage.data
+        phi_end = zmem_end = None
+        if need_phi:
+            phi_end, zmem_end = self._get_state()
+        for k, t in enumerate(t_axis):
+            if self.storage.check_storage_time(t):
+                last = k == n_steps - 1
+                self.storage.store(float(t), psi=psi[k].copy(),
+                                   phi=phi_end if last else None,
+                                   z_mem=zmem_end if last else None)
+        self._t = float(t_axis[-1])
+        self.storage.metadata["LIST_PROPAGATION_TIME"].append(timer.time() - t_start)
+
+    def _align_noise2(self, it0, di, n_steps):
+        """Noise 2 on a different time axis is resampled onto the noise-1 indices."""
+        if self._n2 is None:
+            return
+        if abs(self.noise2.param["TAU"] - self.noise1.param["TAU"]) < precision:
+            return
+        need = it0 + 2 * n_steps * di + 1
+        tau1 = self.noise1.param["TAU"]
+        idx = [self.noise2.time_index(i * tau1) for i in range(need)]
+        n2 = self._n2[:, idx].contiguous()
+        self._bind_noise(self._n1, n2)
+
+    # -------------------------------------------------------------- read-outs
+    def _get_state(self):
+        if self.kernel == "resident":
+            return self._traj.get_state()
+        phi, z = self._traj.get_state()
+        return phi[0], z[0]
+
+    def dsystem_dt(self, phi, z_mem, z_rnd1, z_rnd2):
+        """dsystem_dt closure of hops_eom.py:196-441 evaluated on the GPU.
+
+        Returns (dphi, dz_mem) in cm^-1 (not divided by hbar).  z_mem is indexed by
+        mode; z_rnd1 / z_rnd2 by unique L.
+        """
+        zm = z_mem.toarray().ravel() if hasattr(z_mem, "toarray") else np.asarray(z_mem).ravel()
+        if not hasattr(self, "_deriv_batch"):
+            self._deriv_batch = StreamBatch(self.dstruct, 1, self.device_param["PRECISION"],
+                                            self.eom_param["EQUATION_OF_MOTION"])
+        b = self._deriv_batch
+        b.set_state(np.asarray(phi).reshape(1, -1), zm.reshape(1, -1))
+        dphi, dz = b.dsystem_dt(np.asarray(z_rnd1).reshape(1, -1),
+                                np.asarray(z_rnd2).reshape(1, -1) if z_rnd2 is not None else None)
+        return dphi[0], dz[0]
+
+    @property
+    def phi(self):
+        return self._get_state()[0]
+
+    @property
+    def z_mem(self):
+        return self._get_state()[1]
+
+    @property
+    def psi(self):
+        return self.phi[:self.n_state]
+
+    @property
+    def t(self):
+        return self._t
+
+    @property
+    def n_hier(self):
+        return self.basis.n_hier
+
+    @property
+    def n_state(self):
+        return self.system.n_state
+
+    @property
+    def state_list(self):
+        return np.arange(self.system.n_state)
+
+    @property
+    def auxiliary_list(self):
+        """Aux vectors as dense count rows, in the reference order."""
+        return self.basis.counts
+
+    def normalize(self, phi):
+        """hops_trajectory.py:616-634 (host helper for callers)."""
+        if self.eom_param["EQUATION_OF_MOTION"] == "NORMALIZED NONLINEAR":
+            return phi / np.sqrt(np.sum(np.abs(phi[:self.n_state]) ** 2))
+        return phi

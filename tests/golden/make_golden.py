@@ -1,0 +1,242 @@
+"""Generate golden fixtures by running the UNMODIFIED MesoHOPS reference on CPU.
+
+Run in a container that has the reference source tree (its ``src`` directory on
+``MESOHOPS_SRC`` or at the default path below).  The outputs are small ``.npz``
+files committed next to this script; the GPU box never needs the reference.
+
+    python tests/golden/make_golden.py
+
+Each fixture records the inputs (system, hierarchy depth, noise arrays, psi_0,
+time step) together with the reference outputs (psi_traj, derivative values,
+correlated noise), so that tests can rebuild the same problem through
+``mesohops_b200`` and the oracle.
+"""
+import os
+import sys
+import contextlib
+import tempfile
+import io
+
+import numpy as np
+import scipy.sparse as sps
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SRC = os.environ.get("MESOHOPS_SRC", "/root/reference/src")
+sys.path.insert(0, REF_SRC)
+
+from mesohops.trajectory.hops_trajectory import HopsTrajectory  # noqa: E402
+from mesohops.trajectory.exp_noise import bcf_exp  # noqa: E402
+from mesohops.util.bath_corr_functions import bcf_convert_dl_to_exp  # noqa: E402
+from mesohops.util.physical_constants import hbar  # noqa: E402
+
+
+def quiet(fn, *a, **k):
+    with contextlib.redirect_stdout(io.StringIO()):
+        return fn(*a, **k)
+
+
+def site_system(H, modes_per_site):
+    n = H.shape[0]
+    gw, lops = [], []
+    for i in range(n):
+        L = sps.coo_matrix(([1.0], ([i], [i])), shape=(n, n))
+        for (lam, gam, T) in modes_per_site:
+            g, w = bcf_convert_dl_to_exp(lam, gam, T)
+            gw.append([g, w])
+            lops.append(L)
+    return {"HAMILTONIAN": np.array(H, dtype=np.complex128), "GW_SYSBATH": gw,
+            "L_HIER": lops, "L_NOISE1": lops, "ALPHA_NOISE1": bcf_exp,
+            "PARAM_NOISE1": gw}
+
+
+def dense_lops(sysp):
+    out = []
+    for l in sysp["L_HIER"]:
+        out.append(np.array(l.toarray() if sps.issparse(l) else l, dtype=np.complex128))
+    return np.array(out)
+
+
+def n_unique(sysp):
+    keys = []
+    for l in sysp["L_HIER"]:
+        nz = l.nonzero() if sps.issparse(l) else np.nonzero(l)
+        k = tuple(tuple(int(x) for x in v) for v in nz)
+        if k not in keys:
+            keys.append(k)
+    return len(keys)
+
+
+def run_precalc(name, sysp, depth, psi0, t_max, dt, noise_seed, noise2=None,
+                eom="NORMALIZED NONLINEAR", extra=None):
+    """Propagate with PRE_CALCULATED noise; record psi_traj, phi, z_mem and derivatives."""
+    tau_noise = dt / 2.0
+    tlen = t_max + dt
+    n_t = int(np.ceil(tlen / tau_noise)) + 1
+    nl = n_unique(sysp)
+    rng = np.random.default_rng(noise_seed)
+    # Smooth-ish correlated-looking noise; exactly representable in complex64.
+    noise = (rng.normal(size=(nl, n_t)) + 1j * rng.normal(size=(nl, n_t))) * 40.0
+    noise = noise.astype(np.complex64)
+    # The reference compares the two SEEDs with ==, which fails for two arrays:
+    # hand both over as .npy file paths instead (hops_noise.py:271-283).
+    tmpdir = tempfile.mkdtemp()
+    path1 = os.path.join(tmpdir, "noise1.npy")
+    np.save(path1, noise)
+    noise_param = {"SEED": path1, "MODEL": "PRE_CALCULATED",
+                   "TLEN": float(tlen), "TAU": float(tau_noise)}
+    noise2_param = None
+    if noise2 is not None:
+        path2 = os.path.join(tmpdir, "noise2.npy")
+        np.save(path2, noise2.astype(np.complex64))
+        noise2_param = {"SEED": path2, "MODEL": "PRE_CALCULATED",
+                        "TLEN": float(tlen), "TAU": float(tau_noise),
+                        "FLAG_REAL": False}
+        sysp = dict(sysp)
+        sysp["L_NOISE2"] = sysp["L_HIER"]
+        sysp["ALPHA_NOISE2"] = bcf_exp
+        sysp["PARAM_NOISE2"] = sysp["GW_SYSBATH"]
+    hops = HopsTrajectory(sysp, noise_param=noise_param, noise2_param=noise2_param,
+                          hierarchy_param={"MAXHIER": depth},
+                          eom_param={"EQUATION_OF_MOTION": eom}, storage_param={})
+    quiet(hops.initialize, psi0)
+    # one derivative at a random state with non-zero memory and noise
+    nh, ns = hops.n_hier, hops.n_state
+    phi_r = rng.normal(size=nh * ns) + 1j * rng.normal(size=nh * ns)
+    zmem_r = (rng.normal(size=len(sysp["GW_SYSBATH"]))
+              + 1j * rng.normal(size=len(sysp["GW_SYSBATH"]))) * 5.0
+    z1_r = (rng.normal(size=nl) + 1j * rng.normal(size=nl)).astype(np.complex64) * 30
+    z2_r = (rng.normal(size=nl) + 1j * rng.normal(size=nl)).astype(np.complex64) * 10
+    zmem_sp = sps.csr_array(zmem_r.reshape(-1, 1))
+    dphi_r, dz_r = hops.dsystem_dt(phi_r, zmem_sp, z1_r, z2_r)
+    dz_r = np.asarray(dz_r.toarray()).ravel() if sps.issparse(dz_r) else np.asarray(dz_r)
+    quiet(hops.propagate, t_max, dt)
+    psi_traj = np.array(hops.storage.data["psi_traj"])
+    t_axis = np.array(hops.storage.data["t_axis"])
+    zmem_end = hops.z_mem.toarray().ravel() if sps.issparse(hops.z_mem) else hops.z_mem
+    H = sysp["HAMILTONIAN"]
+    H = H.toarray() if sps.issparse(H) else np.asarray(H)
+    out = dict(
+        H=np.array(H, dtype=np.complex128), G=np.array([g for g, w in sysp["GW_SYSBATH"]]),
+        W=np.array([w for g, w in sysp["GW_SYSBATH"]]), L=dense_lops(sysp),
+        depth=depth, psi0=np.array(psi0, dtype=np.complex128), t_max=t_max, dt=dt,
+        tau_noise=tau_noise, tlen=tlen, noise1=noise,
+        noise2=(noise2 if noise2 is not None else np.zeros_like(noise)),
+        eom=eom, psi_traj=psi_traj, t_axis=t_axis, phi_end=np.array(hops.phi),
+        zmem_end=np.array(zmem_end), n_hier=nh, n_state=ns,
+        deriv_phi=phi_r, deriv_zmem=zmem_r, deriv_z1=z1_r, deriv_z2=z2_r,
+        deriv_dphi=np.array(dphi_r), deriv_dz=np.array(dz_r),
+        aux=np.array([a.todense() for a in hops.auxiliary_list], dtype=np.int64),
+    )
+    if extra:
+        out.update(extra)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, "n_hier", nh, "n_state", ns, "steps", len(psi_traj) - 1)
+
+
+def make_noise_fixture():
+    """Reference FFT_FILTER noise for the dimer (seed 0, SUM_GAUSSIAN and BOX_MULLER)."""
+    H = np.array([[0, 50], [50, 0.0]])
+    sysp = site_system(H, [(50, 50, 295)])
+    out = {}
+    for model in ("SUM_GAUSSIAN", "BOX_MULLER"):
+        hops = HopsTrajectory(sysp, noise_param={"SEED": 0, "MODEL": "FFT_FILTER",
+                                                 "TLEN": 1004.0, "TAU": 2.0,
+                                                 "RAND_MODEL": model,
+                                                 "STORE_RAW_NOISE": True},
+                              hierarchy_param={"MAXHIER": 1}, storage_param={})
+        z = quiet(hops.noise1.get_noise, list(np.arange(0, 1004.0 + 1e-9, 2.0)))
+        out[model + "_eta"] = np.array(z)
+        out[model + "_raw"] = np.array(hops.noise1.param["Z_UNCORRELATED"])
+        out[model + "_alpha"] = np.complex64(hops.noise1._corr_func_by_lop_taxis(
+            hops.noise1.param["T_AXIS"], [0, 1]))
+    out["G"] = np.array([g for g, w in sysp["GW_SYSBATH"]])
+    out["W"] = np.array([w for g, w in sysp["GW_SYSBATH"]])
+    out["tau"] = 2.0
+    out["tlen"] = 1004.0
+    np.savez_compressed(os.path.join(HERE, "noise_dimer.npz"), **out)
+    print("noise_dimer")
+
+
+def main():
+    # c1: dimer, depth 4 (15 aux x 2 states), dt 4 fs, 1000 fs
+    H = np.array([[0, 50], [50, 0.0]])
+    run_precalc("c1_dimer", site_system(H, [(50, 50, 295)]), 4,
+                np.array([1, 0], dtype=np.complex128), 1000.0, 4.0, noise_seed=11)
+
+    # dimer of dimers: 4 sites, two modes per site (DL + Markovian-like), depth 2
+    hs = np.zeros((4, 4))
+    hs[0, 1] = hs[1, 0] = 40
+    hs[1, 2] = hs[2, 1] = 10
+    hs[2, 3] = hs[3, 2] = 40
+    g0, w0 = bcf_convert_dl_to_exp(20.0, 50.0, 140.0)
+    gw, lops = [], []
+    for i in range(4):
+        L = np.zeros((4, 4))
+        L[i, i] = 1.0
+        gw.append([g0, w0])
+        lops.append(sps.coo_matrix(L))
+        gw.append([-1j * np.imag(g0), 500.0])
+        lops.append(L)
+    sysp = {"HAMILTONIAN": np.array(hs, dtype=np.complex128), "GW_SYSBATH": gw,
+            "L_HIER": lops, "L_NOISE1": lops, "ALPHA_NOISE1": bcf_exp,
+            "PARAM_NOISE1": gw}
+    psi0 = np.zeros(4, dtype=np.complex128)
+    psi0[2] = 1.0
+    run_precalc("dod", sysp, 2, psi0, 200.0, 4.0, noise_seed=12)
+
+    # general (off-diagonal, imaginary) L-operators, 3 states, 6 modes, depth 3
+    lg = np.zeros((3, 3, 3), dtype=np.complex128)
+    lg[0, 0, 1] = 1j
+    lg[0, 1, 0] = -1j
+    lg[1, 1, 2] = 1
+    lg[1, 2, 1] = 1
+    lg[2, 0, 0] = 0.5
+    lg[2, 1, 1] = 1
+    lg[2, 2, 2] = -1
+    by_mode = [0, 0, 1, 1, 2, 2]
+    gw6 = [[12.0, 18.0], [7.0, 3.0], [11.0, 9.0], [6.0, 4.0], [10.0, 10.0], [5.0, 5.0]]
+    base_ham = np.array([[1.0, 14.0, 8.0], [14.0, 0, 10.0], [8.0, 10.0, -1.0]])
+    sysg = {"HAMILTONIAN": base_ham, "GW_SYSBATH": gw6,
+            "L_HIER": [lg[i] for i in by_mode], "L_NOISE1": [lg[i] for i in by_mode],
+            "ALPHA_NOISE1": bcf_exp, "PARAM_NOISE1": gw6}
+    rngn2 = np.random.default_rng(99)
+    n2 = (rngn2.normal(size=(3, int(np.ceil(21.0 / 0.5)) + 1)) * 3.0).astype(np.complex64)
+    run_precalc("general_lop", sysg, 3, np.array([1, 0, 0], dtype=np.complex128),
+                20.0, 1.0, noise_seed=13, noise2=n2)
+
+    # small ring (c3 shape, reduced): 6 sites, one DL mode per site, depth 3
+    n = 6
+    rng = np.random.default_rng(2)
+    H = np.diag(rng.uniform(-100, 100, n))
+    for i in range(n):
+        H[i, (i + 1) % n] = H[(i + 1) % n, i] = 80.0
+    psi0 = np.zeros(n, dtype=np.complex128)
+    psi0[0] = 1.0
+    run_precalc("ring6", site_system(H, [(60, 60, 295)]), 3, psi0, 200.0, 4.0,
+                noise_seed=14)
+
+    # chain with two modes per site (c2 shape, reduced): 4 sites, depth 3
+    n = 4
+    rng = np.random.default_rng(1)
+    H = np.diag(rng.normal(0, 50, n))
+    for i in range(n - 1):
+        H[i, i + 1] = H[i + 1, i] = 100.0
+    psi0 = np.zeros(n, dtype=np.complex128)
+    psi0[0] = 1.0
+    run_precalc("chain4_2mode", site_system(H, [(35, 50, 300), (10, 500, 300)]), 3,
+                psi0, 100.0, 2.0, noise_seed=15)
+
+    # non-normalized nonlinear and linear EOM on the dimer
+    H = np.array([[0, 50], [50, 0.0]])
+    run_precalc("c1_nonlinear", site_system(H, [(50, 50, 295)]), 3,
+                np.array([1, 0], dtype=np.complex128), 100.0, 4.0, noise_seed=16,
+                eom="NONLINEAR")
+    run_precalc("c1_linear", site_system(H, [(50, 50, 295)]), 3,
+                np.array([1, 0], dtype=np.complex128), 100.0, 4.0, noise_seed=17,
+                eom="LINEAR")
+
+    make_noise_fixture()
+
+
+if __name__ == "__main__":
+    main()

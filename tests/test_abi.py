@@ -1,0 +1,48 @@
+"""The C-ABI library loads and exports every entry point include/hops_b200.h
+declares (no GPU needed: nothing here launches a kernel)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "hops_b200.h")
+LIB = os.path.join(ROOT, "mesohops_b200", "lib", "libhops_b200.so")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = re.findall(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b(hops_\w+)\s*\(", text, flags=re.M)
+    return sorted(set(names))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    for n in ("hops_rk4_propagate", "hops_dsystem_dt", "hops_resident_propagate",
+              "hops_noise_filter", "hops_last_error"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol():
+    if not os.path.exists(LIB):
+        from mesohops_b200.build import build
+        build()
+    lib = ctypes.CDLL(LIB)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_host_only_calls():
+    from mesohops_b200 import _lib
+    L = _lib.lib()
+    assert L.hops_version() >= 10000
+    assert L.hops_scalar_workspace_doubles(2, 2, 2, 3) > 0
+    assert L.hops_resident_scalar_doubles(2, 2, 2) > 0
+    assert L.hops_noise_filter_work_doubles(2, 10) >= 4 * 2 * 18
+    # argument validation happens before any CUDA call
+    rc = L.hops_resident_propagate(None, 0, 0, 0, 0, 1, None)
+    assert rc == _lib.HOPS_EINVAL
+    assert b"bad resident" in L.hops_last_error()

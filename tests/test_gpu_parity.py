@@ -1,0 +1,111 @@
+"""GPU parity of the trajectory hot path against the reference (through the
+committed golden fixtures) and the CPU oracle.
+
+Tolerances: complex128 <= 1e-10 relative (max |diff| / max |ref|) for
+trajectories and 1e-12 for single derivatives; complex64 (FP64 scalars)
+<= 1e-5 absolute population error."""
+import numpy as np
+import pytest
+
+from conftest import golden_system, load_golden
+
+pytestmark = pytest.mark.gpu
+
+FIXTURES = ["c1_dimer", "dod", "general_lop", "ring6", "chain4_2mode", "c1_nonlinear",
+            "c1_linear"]
+
+
+def make_traj(f, kernel, precision="complex128"):
+    from mesohops_b200 import HopsTrajectory
+    from mesohops_b200.bath import bcf_exp
+    sysp = golden_system(f)
+    noise2 = None
+    if np.any(f["noise2"] != 0):
+        sysp["L_NOISE2"] = sysp["L_HIER"]
+        sysp["ALPHA_NOISE2"] = bcf_exp
+        sysp["PARAM_NOISE2"] = sysp["GW_SYSBATH"]
+        noise2 = {"SEED": f["noise2"], "MODEL": "PRE_CALCULATED", "TLEN": float(f["tlen"]),
+                  "TAU": float(f["tau_noise"]), "FLAG_REAL": False}
+    hops = HopsTrajectory(sysp, noise_param={"SEED": f["noise1"], "MODEL": "PRE_CALCULATED",
+                                             "TLEN": float(f["tlen"]),
+                                             "TAU": float(f["tau_noise"])},
+                          noise2_param=noise2,
+                          hierarchy_param={"MAXHIER": int(f["depth"])},
+                          eom_param={"EQUATION_OF_MOTION": str(f["eom"])},
+                          device_param={"KERNEL": kernel, "PRECISION": precision})
+    hops.initialize(f["psi0"])
+    return hops
+
+
+def rel(a, b):
+    return np.max(np.abs(np.asarray(a) - np.asarray(b))) / np.max(np.abs(np.asarray(b)))
+
+
+@pytest.mark.parametrize("kernel", ["resident", "streaming"])
+@pytest.mark.parametrize("name", FIXTURES)
+def test_trajectory_c128_matches_reference(cuda_device, name, kernel):
+    f = load_golden(name)
+    hops = make_traj(f, kernel)
+    hops.propagate(float(f["t_max"]), float(f["dt"]))
+    psi = np.array(hops.storage["psi_traj"])
+    assert psi.shape == f["psi_traj"].shape
+    np.testing.assert_allclose(hops.storage["t_axis"], f["t_axis"])
+    assert rel(psi, f["psi_traj"]) <= 1e-10
+    assert rel(hops.phi, f["phi_end"]) <= 1e-10
+    if str(f["eom"]) != "LINEAR":
+        zm = f["zmem_end"]
+        assert np.max(np.abs(hops.z_mem - zm)) <= 1e-10 * max(1.0, np.max(np.abs(zm)))
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_derivative_matches_reference(cuda_device, name):
+    f = load_golden(name)
+    hops = make_traj(f, "streaming")
+    dphi, dz = hops.dsystem_dt(f["deriv_phi"], f["deriv_zmem"], f["deriv_z1"], f["deriv_z2"])
+    assert rel(dphi, f["deriv_dphi"]) <= 1e-12
+    if str(f["eom"]) != "LINEAR":
+        assert rel(dz, f["deriv_dz"]) <= 1e-12
+
+
+@pytest.mark.parametrize("kernel", ["resident", "streaming"])
+@pytest.mark.parametrize("name", ["c1_dimer", "ring6", "chain4_2mode", "dod"])
+def test_trajectory_c64_population_error(cuda_device, name, kernel):
+    f = load_golden(name)
+    hops = make_traj(f, kernel, precision="complex64")
+    hops.propagate(float(f["t_max"]), float(f["dt"]))
+    pop = np.abs(np.array(hops.storage["psi_traj"])) ** 2
+    pop_ref = np.abs(f["psi_traj"]) ** 2
+    assert np.max(np.abs(pop - pop_ref)) <= 1e-5
+
+
+def test_propagate_in_pieces_equals_one_call(cuda_device):
+    f = load_golden("ring6")
+    a = make_traj(f, "streaming")
+    a.propagate(float(f["t_max"]), float(f["dt"]))
+    b = make_traj(f, "streaming")
+    half = float(f["t_max"]) / 2
+    b.propagate(half, float(f["dt"]))
+    b.propagate(half, float(f["dt"]))
+    assert rel(b.phi, a.phi) <= 1e-13
+    assert rel(np.array(b.storage["psi_traj"]), np.array(a.storage["psi_traj"])) <= 1e-13
+
+
+def test_resident_equals_streaming(cuda_device):
+    f = load_golden("chain4_2mode")
+    a = make_traj(f, "resident")
+    b = make_traj(f, "streaming")
+    for h in (a, b):
+        h.propagate(float(f["t_max"]), float(f["dt"]))
+    assert rel(a.phi, b.phi) <= 1e-12
+
+
+def test_errors_like_reference(cuda_device):
+    from mesohops_b200.exceptions import LockedException, TrajectoryError
+    f = load_golden("c1_dimer")
+    hops = make_traj(f, "resident")
+    with pytest.raises(LockedException):
+        hops.initialize(f["psi0"])
+    with pytest.raises(TrajectoryError):
+        hops.propagate(float(f["tlen"]) + 10.0, float(f["dt"]))
+    with pytest.raises(TrajectoryError):
+        hops.propagate(8.0, float(f["tau_noise"]) * 0.7)
