@@ -1,0 +1,393 @@
+#!/usr/bin/env python
+"""Headline benchmark: RK4 traj.steps/s of the HOPS trajectory hot path on B200.
+
+Default workload (the one the target is quoted on): 20-site ring, depth 4
+(10626 aux x 20 states), 128 trajectories per GPU, complex64 state / SpMM with
+FP64 <L>, norm and z_mem, dt = 4 fs.  One "step" = one RK4 step of all 128
+trajectories (4 stage kernels + 4 FP64 stage-scalar kernels).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload ring20|chain10]
+  python bench.py --impl reference ...     # CPU reference arm (the oracle port)
+
+Multi-GPU: one process per GPU (torchrun); every rank propagates its own 128
+trajectories (different seeds), no data-path collective ("scaling": "weak");
+the timed region is the max over ranks.  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RK4 traj·steps/s on 1 B200, served/batched vs plain, ≤1e-5 pop. err; p50/p99"
+UNIT = "traj·steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="ring20", choices=["ring20", "chain10"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "complex64", "complex128"],
+                    help="batched path: mixed = complex128 state with complex64 stage vectors")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the plain/accuracy/e2e/CPU legs (profiling runs)")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks --
+class ClockSampler:
+    """nvidia-smi samples of one GPU during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append(parts)
+            except Exception:
+                pass
+        os.remove(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return None
+
+
+# ------------------------------------------------------------- GPU pieces --
+def algorithmic_bytes_per_step(t, B, precision):
+    """Compulsory bytes of one RK4 step: every vector touched once per stage.
+
+    Stage 1 reads phi and writes acc, Y2; stages 2-3 read Y, phi, acc and write
+    acc, Y; stage 4 reads Y, phi, acc and writes phi: 17 vector passes, 5 of
+    them on phi (phi is complex128 in the mixed mode, which also writes the
+    complex64 copy of phi read by stage 1: stage 1 then reads that copy for its
+    own element and phi).  Tables per stage: int32 aux + int32 mode per up/down
+    connection, the down coefficient and k_decay per aux.
+    """
+    n = t["n_hier"] * t["n_state"] * B
+    sv = 16 if precision == "complex128" else 8          # stage vectors
+    sp = 8 if precision == "complex64" else 16            # state
+    if precision == "mixed":
+        per = 12 * sv + 5 * sp + 2 * sv                    # + shadow write and read
+    else:
+        per = 12 * sv + 5 * sp
+    sc = 8 if precision != "complex128" else 16
+    t_idx = (len(t["up_aux"]) * 8 + len(t["dn_aux"]) * (8 + sc) + t["n_hier"] * sc)
+    return n * per + 4 * t_idx
+
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+    from mesohops_b200 import _lib
+    from mesohops_b200.ensemble import HopsEnsemble
+    from mesohops_b200.workloads import WORKLOADS
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    wl = WORKLOADS[args.workload]
+    B, dt, depth = wl["n_traj"], wl["dt"], wl["depth"]
+    K, W = args.steps, max(args.warmup, 3)
+    tau_noise = dt / 2.0
+    tlen = (W + 2 * K + 120 + wl["n_steps"]) * dt + dt
+    noise = {"MODEL": "FFT_FILTER", "TLEN": float(tlen), "TAU": tau_noise,
+             "SEED": list(range(rank * B, rank * B + B))}
+    sysp = wl["system"]()
+    ens = HopsEnsemble(sysp, B, noise_param=noise, hierarchy_param={"MAXHIER": depth},
+                       precision=args.precision, device=dev)
+    psi0 = np.zeros(ens.n_state, dtype=complex)
+    psi0[0] = 1.0
+    ens.initialize(psi0)
+    ens.propagate(W * dt, dt)
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ens.propagate(K * dt, dt)
+    e1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ens.check()
+    value = B * K * world / (ms / 1e3)
+    launches = 8 * K + 3
+
+    result = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
+              "steps": K, "warmup": W, "ms_per_step": round(ms / K, 4),
+              "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+              "dtype": {"mixed": "c64", "complex64": "c64", "complex128": "c128"}[args.precision],
+              "data": "synthetic (seeded)",
+              "gpu_launches": launches}
+    t = ens.dstruct.tables
+    result["config"] = {
+        "workload": wl["desc"] + f"; batched ensemble of {B} trajectories per GPU",
+        "n_hier": t["n_hier"], "n_state": t["n_state"], "n_traj_per_gpu": B,
+        "dt_fs": dt, "precision": {
+            "mixed": "complex64 stage vectors and SpMM, complex128 state, FP64 <L>/norm/z_mem",
+            "complex64": "complex64 state, stage vectors and SpMM, FP64 <L>/norm/z_mem",
+            "complex128": "complex128 throughout"}[args.precision],
+        "l2": f"inputs larger than L2: each stage vector is "
+              f"{t['n_hier'] * t['n_state'] * B * 8 / 1e6:.0f} MB (L2 126 MB)",
+        "parallelism": f"replicas x{world} (trajectory-sharded, no collectives)"}
+
+    # ---- roofline of the dominant kernel (the streaming stage kernel) ----
+    L = _lib.lib()
+    import ctypes as C
+    kr = min(K, 20)
+    L.hops_kernel_timing(1)
+    ens.propagate(kr * dt, dt)
+    torch.cuda.synchronize()
+    tot = C.c_double(0)
+    nl = C.c_int64(0)
+    L.hops_kernel_timing_read(C.byref(tot), C.byref(nl))
+    L.hops_kernel_timing(0)
+    avg_ms = tot.value / max(nl.value, 1)
+    bytes_launch = algorithmic_bytes_per_step(t, B, args.precision) / 4.0
+    peaks = measured_peaks()
+    peak = peaks["hbm_gbs"] if peaks and "hbm_gbs" in peaks else 6650.0
+    achieved = bytes_launch / (avg_ms / 1e3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", f"k_stage_{args.workload}_traffic.json")
+    if os.path.exists(prof):
+        traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+    result["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                          "unit": "GB/s", "frac": round(achieved / peak, 4),
+                          "traffic": traffic, "kernel": "k_stage (streaming RK4 stage)",
+                          "algorithmic_bytes_per_launch": int(bytes_launch),
+                          "avg_launch_ms": round(avg_ms, 5),
+                          "stage_share_of_step": round(tot.value / kr / (ms / K), 3),
+                          "peak_source": "of measured" if peaks else "of fallback"}
+    result["clocks"] = clocks
+
+    if rank == 0 and not args.no_extras:
+        result.update(extras(args, wl, sysp, ens, dev, value, K))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+def extras(args, wl, sysp, ens, dev, value, K):
+    """Plain complex128 path, accuracy of the batched complex64 path, the
+    end-to-end API number and the CPU baseline (rank 0 only)."""
+    import torch
+    from mesohops_b200.ensemble import HopsEnsemble
+    from mesohops_b200.constants import hbar
+    out = {}
+    B, dt, depth = wl["n_traj"], wl["dt"], wl["depth"]
+    tlen = ens.noise_param["TLEN"]
+    # plain: one trajectory at a time, complex128 (the reference's call, on GPU)
+    kp = min(K, 50)
+    plain = HopsEnsemble(sysp, 1, noise_param={"MODEL": "FFT_FILTER", "TLEN": tlen,
+                                               "TAU": dt / 2, "SEED": [0]},
+                         hierarchy_param={"MAXHIER": depth}, precision="complex128", device=dev)
+    psi0 = np.zeros(plain.n_state, dtype=complex)
+    psi0[0] = 1.0
+    plain.initialize(psi0)
+    plain.propagate(3 * dt, dt)
+    torch.cuda.synchronize()
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    a0.record()
+    plain.propagate(kp * dt, dt)
+    a1.record()
+    torch.cuda.synchronize()
+    plain_v = kp / (a0.elapsed_time(a1) / 1e3)
+    out["plain_c128"] = {"value": round(plain_v, 2), "unit": UNIT,
+                         "ms_per_step": round(a0.elapsed_time(a1) / kp, 4),
+                         "note": "one trajectory per call, complex128 everywhere"}
+    out["batched_over_plain"] = round(value / plain_v, 2)
+
+    # accuracy: the batched precision vs complex128 on the same seeds over the
+    # configuration's full run (250 steps)
+    na = wl["n_steps"]
+    res = {}
+    for prec in (args.precision, "complex128"):
+        e = HopsEnsemble(sysp, B, noise_param={"MODEL": "FFT_FILTER", "TLEN": tlen,
+                                               "TAU": dt / 2, "SEED": list(range(B))},
+                         hierarchy_param={"MAXHIER": depth}, precision=prec, device=dev)
+        e.initialize(psi0)
+        psi = torch.empty((na, B, e.n_state), dtype=torch.complex128, device=dev)
+        e.propagate(na * dt, dt, psi_out=psi)
+        res[prec] = psi.cpu().numpy()
+        del e
+    p64, p128 = res[args.precision], res["complex128"]
+    out["accuracy"] = {
+        "precision": args.precision,
+        "max_pop_err_vs_c128": float(np.max(np.abs(np.abs(p64) ** 2 - np.abs(p128) ** 2))),
+        "max_abs_psi_err_vs_c128": float(np.max(np.abs(np.abs(p64) - np.abs(p128)))),
+        "sample": f"{B} trajectories x {na} steps; the complex128 GPU path matches the "
+                  "FP64 CPU oracle to <=1e-10 (tests/test_gpu_parity.py)"}
+
+    # end to end through the public API with host buffers: every step copies its
+    # noise window host->device (pinned) and reads psi back device->host
+    ke = min(K, 50)
+    noise_host = ens.noise.cpu().pin_memory()
+    psi_dev = torch.empty((1, B, ens.n_state), dtype=torch.complex128, device=dev)
+    psi_host = torch.empty((1, B, ens.n_state), dtype=torch.complex128).pin_memory()
+    di = int(round(dt * 0.5 / ens.noise_param["TAU"]))
+    h2d = d2h = 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        it0 = int(round(ens.t / ens.noise_param["TAU"]))
+        sl = slice(it0, it0 + 2 * di + 1)
+        ens.noise[:, :, sl].copy_(noise_host[:, :, sl], non_blocking=True)
+        h2d += noise_host[:, :, sl].numel() * 8
+        ens.propagate(dt, dt, psi_out=psi_dev)
+        psi_host.copy_(psi_dev, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        d2h += psi_host.numel() * 16
+    e2e_s = time.perf_counter() - t0
+    out["e2e"] = {"value": round(B * ke / e2e_s, 2), "unit": UNIT,
+                  "h2d_bytes_per_step": int(h2d / ke), "d2h_bytes_per_step": int(d2h / ke),
+                  "note": "HopsEnsemble.propagate one step per call, noise window h2d "
+                          "from pinned memory and psi d2h each step, host wall clock"}
+    out["cpu_baseline"] = cpu_baseline(wl, sysp)
+    return out
+
+
+# ------------------------------------------------------------- CPU legs --
+def _oracle_worker(args):
+    """One trajectory of the oracle for n_steps steps (single thread)."""
+    wl_name, seed, n_steps = args
+    os.environ["OMP_NUM_THREADS"] = "1"
+    from threadpoolctl import threadpool_limits
+    from oracle import hops_oracle as O
+    from mesohops_b200.workloads import WORKLOADS
+    wl = WORKLOADS[wl_name]
+    sysp = wl["system"]()
+    dt = wl["dt"]
+    with threadpool_limits(1):
+        b = O.OracleBasis(sysp, wl["depth"])
+        n_t = int(np.ceil((n_steps + 2) * dt / (dt / 2))) + 1
+        rng = np.random.default_rng(seed)
+        noise = ((rng.normal(size=(b.sys["L"].__len__(), n_t))
+                  + 1j * rng.normal(size=(len(b.sys["L"]), n_t))) * 40).astype(np.complex64)
+        psi0 = np.zeros(b.nstate, dtype=complex)
+        psi0[0] = 1.0
+        t0 = time.perf_counter()
+        O.propagate(b, psi0, noise, dt / 2, n_steps * dt, dt)
+        return time.perf_counter() - t0
+
+
+def cpu_baseline(wl, sysp, n_steps=4):
+    """The oracle port (numpy, one thread) on one trajectory, n_steps steps."""
+    name = [k for k, v in __import__("mesohops_b200.workloads", fromlist=["x"]).WORKLOADS.items()
+            if v is wl][0]
+    el = _oracle_worker((name, 0, n_steps))
+    return {"value": round(n_steps / el, 3), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"1 trajectory x {n_steps} RK4 steps of the same system with the numpy "
+                      "oracle (single thread)"}
+
+
+def run_reference(args):
+    """CPU arm: the oracle port on every host core, one trajectory per process."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    from mesohops_b200.workloads import WORKLOADS
+    wl = WORKLOADS[args.workload]
+    cores = os.cpu_count() or 1
+    K = max(1, min(args.steps, 3))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        # each worker builds its basis outside its own timed region; the workers
+        # run concurrently, so the wall time of the step loop is the slowest one
+        el = max(pool.map(_oracle_worker, [(args.workload, s, K) for s in range(cores)]))
+    v = cores * K / el
+    line = {"metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": world,
+            "steps": K, "warmup": 1, "ms_per_step": round(el / K * 1e3, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128", "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": wl["desc"] + f"; {cores} trajectories, one per host core"},
+            "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{cores} trajectories x {K} RK4 steps (numpy oracle, "
+                                       "one process per core, one thread each)"},
+            "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_gpu(a)

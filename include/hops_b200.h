@@ -40,6 +40,7 @@ extern "C" {
 
 #define HOPS_PREC_C128 0    /* complex128 state and arithmetic */
 #define HOPS_PREC_C64 1     /* complex64 state/SpMM, FP64 <L>, norm, z_mem */
+#define HOPS_PREC_MIXED 2   /* complex128 state; complex64 stage vectors/SpMM; FP64 scalars */
 
 #define HOPS_EOM_NORMALIZED_NONLINEAR 0
 #define HOPS_EOM_NONLINEAR 1
@@ -49,8 +50,9 @@ extern "C" {
  * One hierarchy basis in device memory (all pointers are device pointers).
  * Complex numbers are stored as interleaved (re, im) doubles; *_f arrays hold
  * the same coefficients rounded to float for HOPS_PREC_C64.
- * Aux index a, state index s; phi element (a, b, s) of a batch of B
- * trajectories lives at ((a * B) + b) * n_state + s.
+ * Aux index a, state index s; phi element (a, s, b) of a batch of B
+ * trajectories lives at ((a * n_state) + s) * B + b (trajectory fastest; for
+ * B = 1 this is the reference's flat index a * n_state + s).
  */
 typedef struct hops_structure {
   int32_t n_hier, n_state, n_mode, n_lop;
@@ -95,11 +97,20 @@ typedef struct hops_structure {
   const int32_t* h_col;
   const double* h_val;  /* complex, already multiplied by -i */
   const float* h_val_f;
+  /* site-projector form, per relative mode m and per down connection p */
+  const int32_t* mode_site;    /* [n_mode] s_{l(m)} */
+  const double* mode_gwv;      /* [n_mode] complex (g_m/w_m) v_{l(m)} */
+  const float* mode_gwv_f;
+  const double* dn_coef_site;  /* [n_dn] complex k_m(a) w_m conj(v_{l(m)}) */
+  const float* dn_coef_site_f;
 } hops_structure;
 
 /*
  * A batch of B trajectories sharing one hops_structure.  Vectors phi, acc,
- * y0, y1 have n_hier * B * n_state complex elements of the batch precision.
+ * y0, y1 have n_hier * n_state * B complex elements, laid out
+ * [aux][state][trajectory]; phi is complex128 for HOPS_PREC_C128 and
+ * HOPS_PREC_MIXED, complex64 for HOPS_PREC_C64; acc, y0, y1 (and phi_lo) are
+ * complex64 unless the precision is HOPS_PREC_C128.
  */
 typedef struct hops_batch {
   int32_t n_traj;
@@ -115,17 +126,20 @@ typedef struct hops_batch {
   const float* noise1; /* [B][n_lop][n_t1] complex64 */
   const float* noise2; /* [B][n_lop][n_t2] complex64, or NULL for zero noise 2 */
   int32_t* status;     /* [B] 0 ok, HOPS_ENONFINITE if a norm went NaN/Inf */
+  void* phi_lo;        /* HOPS_PREC_MIXED: complex64 copy of phi read by stage 1 */
 } hops_batch;
 
 /* One trajectory of hops_resident_propagate (array in device memory). */
 typedef struct hops_task {
   const hops_structure* st; /* device pointer to the structure */
-  void* phi;                /* [n_hier][n_state] in the task precision */
+  void* phi;                /* [n_hier][n_state]: complex64 for HOPS_PREC_C64, else complex128 */
   double* zmem;             /* [n_mode] complex */
   const float* noise1;      /* [n_lop][n_t1] complex64 */
   const float* noise2;      /* [n_lop][n_t2] complex64 or NULL */
   double* psi_out;          /* [n_steps][n_state] complex128, or NULL */
-  void* scratch;            /* 3 * n_hier * n_state elements if the vectors do not fit shared memory */
+  void* scratch;            /* 3 * n_hier * n_state stage elements (complex128 for
+                               HOPS_PREC_C128, else complex64) used when the vectors
+                               do not fit shared memory */
   int32_t n_t1, n_t2;
   int32_t it0;      /* noise index of the start time */
   int32_t di;       /* noise index step per half time step */
@@ -201,6 +215,15 @@ int hops_noise_filter(const double* alpha_dev, const float* z_dev, int32_t n_lop
 
 /* Doubles of device work area hops_noise_filter needs (work_dev). */
 size_t hops_noise_filter_work_doubles(int32_t n_lop, int32_t n_t);
+
+/*
+ * Profiling aid: when enabled, every streaming stage-kernel launch is bracketed
+ * by CUDA events on its stream; hops_kernel_timing_read synchronises, returns
+ * the summed kernel time and the launch count, and clears the record.  Not
+ * thread-safe; has no counterpart in the reference (timing support only).
+ */
+int hops_kernel_timing(int enable);
+int hops_kernel_timing_read(double* total_ms, int64_t* n_launches);
 
 #ifdef __cplusplus
 }

@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libhops_b200.so")
 
 HOPS_OK, HOPS_EINVAL, HOPS_ECUDA, HOPS_ENOTSUP, HOPS_ENONFINITE = 0, 1, 2, 3, 5
-PREC_C128, PREC_C64 = 0, 1
+PREC_C128, PREC_C64, PREC_MIXED = 0, 1, 2
 EOM_CODES = {"NORMALIZED NONLINEAR": 0, "NONLINEAR": 1, "LINEAR": 2}
 
 _p = C.c_void_p
@@ -37,6 +37,8 @@ class HopsStructure(C.Structure):
         ("lh_ptr", _p), ("lh_col", _p), ("lh_val", _p), ("lh_val_f", _p),
         ("lop_active", _p), ("lop_site", _p), ("lop_sval", _p),
         ("h_ptr", _p), ("h_col", _p), ("h_val", _p), ("h_val_f", _p),
+        ("mode_site", _p), ("mode_gwv", _p), ("mode_gwv_f", _p),
+        ("dn_coef_site", _p), ("dn_coef_site_f", _p),
     ]
 
 
@@ -46,6 +48,7 @@ class HopsBatch(C.Structure):
         ("n_traj", _i), ("precision", _i), ("eom", _i), ("n_t1", _i), ("n_t2", _i),
         ("phi", _p), ("acc", _p), ("y0", _p), ("y1", _p),
         ("zmem", _p), ("work", _p), ("noise1", _p), ("noise2", _p), ("status", _p),
+        ("phi_lo", _p),
     ]
 
 
@@ -89,6 +92,8 @@ def lib():
     L.hops_noise_filter.argtypes = [_p, _p, _i, _i, _p, _p, _p, C.POINTER(C.c_int64), _p]
     L.hops_noise_filter_work_doubles.restype = C.c_size_t
     L.hops_noise_filter_work_doubles.argtypes = [_i, _i]
+    L.hops_kernel_timing.argtypes = [C.c_int]
+    L.hops_kernel_timing_read.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_int64)]
     _lib = L
     return L
 
@@ -110,4 +115,5 @@ def exported_symbols():
     return ["hops_last_error", "hops_version", "hops_device_query",
             "hops_scalar_workspace_doubles", "hops_batch_reset", "hops_dsystem_dt",
             "hops_rk4_propagate", "hops_resident_propagate", "hops_resident_scalar_doubles",
-            "hops_noise_filter", "hops_noise_filter_work_doubles"]
+            "hops_noise_filter", "hops_noise_filter_work_doubles", "hops_kernel_timing",
+            "hops_kernel_timing_read"]

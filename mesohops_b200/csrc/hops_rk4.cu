@@ -7,6 +7,7 @@
 #include <string.h>
 #include <stdarg.h>
 #include <algorithm>
+#include <vector>
 #include "hops_common.cuh"
 
 using namespace hops;
@@ -48,100 +49,144 @@ extern "C" int hops_device_query(int device, int* sm_count, int* smem_optin) {
   return HOPS_OK;
 }
 
-extern "C" size_t hops_scalar_workspace_doubles(int32_t S, int32_t M, int32_t L, int32_t B) {
-  ScalarLayout lay(S, M, L);
-  return (size_t)lay.stride * (size_t)B;
-}
-
 // ------------------------------------------------------------- precision ----
+// Structure coefficients in the arithmetic precision R.
 template <typename R> struct Prec;
 template <> struct Prec<double> {
   using T = double2;
   static __device__ __forceinline__ T kdec(const hops_structure& st, int a) { return ld2(st.k_decay, a); }
   static __device__ __forceinline__ T dncoef(const hops_structure& st, int p) { return ld2(st.dn_coef, p); }
+  static __device__ __forceinline__ T dncs(const hops_structure& st, int p) { return ld2(st.dn_coef_site, p); }
   static __device__ __forceinline__ T gw(const hops_structure& st, int m) { return ld2(st.mode_gw, m); }
+  static __device__ __forceinline__ T gwv(const hops_structure& st, int m) { return ld2(st.mode_gwv, m); }
   static __device__ __forceinline__ T lval(const hops_structure& st, int q) { return ld2(st.l_val, q); }
   static __device__ __forceinline__ T lhval(const hops_structure& st, int q) { return ld2(st.lh_val, q); }
   static __device__ __forceinline__ T hval(const hops_structure& st, int q) { return ld2(st.h_val, q); }
-  static __device__ __forceinline__ T sval(const hops_structure& st, int j) { return ld2(st.lop_sval, j); }
-  static __device__ __forceinline__ T diag(const double* ws, const ScalarLayout& l, int s) { return ld2(ws + l.diagD(), s); }
-  static __device__ __forceinline__ T upc(const double* ws, const ScalarLayout& l, int m) { return ld2(ws + l.upc(), m); }
-  static __device__ __forceinline__ T cz(const double* ws, const ScalarLayout& l, int j) { return ld2(ws + l.cz(), j); }
 };
 template <> struct Prec<float> {
   using T = float2;
   static __device__ __forceinline__ T kdec(const hops_structure& st, int a) { return ld2f(st.k_decay_f, a); }
   static __device__ __forceinline__ T dncoef(const hops_structure& st, int p) { return ld2f(st.dn_coef_f, p); }
+  static __device__ __forceinline__ T dncs(const hops_structure& st, int p) { return ld2f(st.dn_coef_site_f, p); }
   static __device__ __forceinline__ T gw(const hops_structure& st, int m) { return ld2f(st.mode_gw_f, m); }
+  static __device__ __forceinline__ T gwv(const hops_structure& st, int m) { return ld2f(st.mode_gwv_f, m); }
   static __device__ __forceinline__ T lval(const hops_structure& st, int q) { return ld2f(st.l_val_f, q); }
   static __device__ __forceinline__ T lhval(const hops_structure& st, int q) { return ld2f(st.lh_val_f, q); }
   static __device__ __forceinline__ T hval(const hops_structure& st, int q) { return ld2f(st.h_val_f, q); }
-  static __device__ __forceinline__ T sval(const hops_structure& st, int j) {
-    double2 v = ld2(st.lop_sval, j);
-    return mkf((float)v.x, (float)v.y);
-  }
-  static __device__ __forceinline__ T diag(const double* ws, const ScalarLayout& l, int s) {
-    return reinterpret_cast<const float2*>(ws + l.diagD_f())[s];
-  }
-  static __device__ __forceinline__ T upc(const double* ws, const ScalarLayout& l, int m) {
-    return reinterpret_cast<const float2*>(ws + l.upc_f())[m];
-  }
-  static __device__ __forceinline__ T cz(const double* ws, const ScalarLayout& l, int j) {
-    double2 v = ld2(ws + l.cz(), j);
-    return mkf((float)v.x, (float)v.y);
+};
+
+// Workspace of a batch: B per-trajectory ScalarLayout blocks followed by the
+// stage coefficients in trajectory-fastest layout ([m][b], [s][b], [j][b]) so
+// that the stage kernel reads them coalesced.
+struct BatchLayout {
+  size_t upcT, upcT_f, diagT, diagT_f, czT, czT_f, ncB, scaleB, total;  // in doubles
+  __host__ __device__ static size_t even(size_t x) { return (x + 1) & ~(size_t)1; }
+  __host__ __device__ BatchLayout(int S, int M, int L, int B) {
+    const ScalarLayout lay(S, M, L);
+    upcT = even((size_t)lay.stride * B);
+    upcT_f = upcT + 2 * (size_t)M * B;
+    diagT = even(upcT_f + (size_t)M * B);
+    diagT_f = diagT + 2 * (size_t)S * B;
+    czT = even(diagT_f + (size_t)S * B);
+    czT_f = czT + 2 * (size_t)L * B;
+    ncB = even(czT_f + (size_t)L * B);
+    scaleB = ncB + B;
+    total = even(scaleB + B);
   }
 };
 
+extern "C" size_t hops_scalar_workspace_doubles(int32_t S, int32_t M, int32_t L, int32_t B) {
+  return BatchLayout(S, M, L, B).total;
+}
+
+// Per-thread stage coefficients of trajectory b read from the transposed arrays.
+template <typename R> struct CoefT {
+  using T = typename Prec<R>::T;
+  const double* ws;
+  BatchLayout bl;
+  int B, b;
+  __device__ __forceinline__ T diag(int s) const {
+    if constexpr (sizeof(R) == 8) return ld2(ws + bl.diagT, s * B + b);
+    else return ld2f(reinterpret_cast<const float*>(ws + bl.diagT_f), s * B + b);
+  }
+  __device__ __forceinline__ T upc(int m) const {
+    if constexpr (sizeof(R) == 8) return ld2(ws + bl.upcT, m * B + b);
+    else return ld2f(reinterpret_cast<const float*>(ws + bl.upcT_f), m * B + b);
+  }
+  __device__ __forceinline__ T cz(int j) const {
+    if constexpr (sizeof(R) == 8) return ld2(ws + bl.czT, j * B + b);
+    else return ld2f(reinterpret_cast<const float*>(ws + bl.czT_f), j * B + b);
+  }
+  __device__ __forceinline__ R nc() const { return (R)ws[bl.ncB + b]; }
+};
+
+// Stage coefficients of one trajectory read from its ScalarLayout block
+// (resident kernel, block in shared memory).
+template <typename R> struct CoefWS {
+  using T = typename Prec<R>::T;
+  const double* ws;
+  ScalarLayout lay;
+  __device__ __forceinline__ T diag(int s) const {
+    if constexpr (sizeof(R) == 8) return ld2(ws + lay.diagD(), s);
+    else return ld2f(reinterpret_cast<const float*>(ws + lay.diagD_f()), s);
+  }
+  __device__ __forceinline__ T upc(int m) const {
+    if constexpr (sizeof(R) == 8) return ld2(ws + lay.upc(), m);
+    else return ld2f(reinterpret_cast<const float*>(ws + lay.upc_f()), m);
+  }
+  __device__ __forceinline__ T cz(int j) const {
+    double2 v = ld2(ws + lay.cz(), j);
+    if constexpr (sizeof(R) == 8) return v;
+    else return mkf((float)v.x, (float)v.y);
+  }
+  __device__ __forceinline__ R nc() const { return (R)ws[lay.nc()]; }
+};
+
 // ------------------------------------------------- derivative of one element --
-// k(a, b, s) of hops_eom.py:389-425 for one trajectory b, reading the stage
-// input Y through the row accessor `row(a)` (pointer to Y[a][b][0]).
-//   K2_k:      k_decay[a] * y
-//   -iH:       sum_s' (-iH)[s,s'] Y[a][s']
-//   noise/nc:  (zhat_j - i z2_j) (L_j Y[a])[s] - nc y
-//   flux up:   sum_{m, u=a+e_m} (g_m/w_m) (conj<L> Y[u][s] - (L Y[u])[s])
-//   flux down: sum_{m, d=a-e_m} k_m(a) w_m (L^H Y[d])[s]
-template <typename R, bool SITE, class Row>
-__device__ __forceinline__ typename Prec<R>::T deriv_elem(const hops_structure& st, const double* ws,
-                                                          const ScalarLayout& lay, int a, int s,
-                                                          Row row) {
+// k(a, s) of hops_eom.py:389-425 for one trajectory, reading the stage input
+// through y(aux, state) and the stage coefficients through cf:
+//   K2_k + noise + norm:  (k_decay[a] + diag(s)) y            (site projectors)
+//                         (k_decay[a] - nc) y + sum_j cz_j (L_j Y[a])[s]   (general L)
+//   -iH:                  sum_s' (-iH)[s,s'] Y[a][s']
+//   flux up (K2_kp1+Z2):  sum_{m, u=a+e_m} (g_m/w_m)(conj<L> Y[u][s] - (L Y[u])[s])
+//   flux down (K2_km1):   sum_{m, d=a-e_m} k_m(a) w_m (L^H Y[d])[s]
+template <typename R, bool SITE, class Y, class Cf>
+__device__ __forceinline__ typename Prec<R>::T deriv_elem(const hops_structure& st, int a, int s,
+                                                          Y y, const Cf& cf) {
   using P = Prec<R>;
   using T = typename P::T;
-  const T* ya = row(a);
-  T y = ya[s];
   T k;
   if (SITE) {
-    k = cmul(cadd(P::kdec(st, a), P::diag(ws, lay, s)), y);
+    k = cmul(cadd(P::kdec(st, a), cf.diag(s)), y(a, s));
   } else {
     T d = P::kdec(st, a);
-    d.x -= (R)ws[lay.nc()];
-    k = cmul(d, y);
+    d.x -= cf.nc();
+    k = cmul(d, y(a, s));
+    const int base_s = s;
     for (int j = 0; j < st.n_lop; ++j) {
       const int base = j * (st.n_state + 1);
-      int q0 = st.l_ptr[base + s], q1 = st.l_ptr[base + s + 1];
+      const int q0 = st.l_ptr[base + base_s], q1 = st.l_ptr[base + base_s + 1];
       if (q0 == q1) continue;
       T acc = czero<T>();
-      for (int q = q0; q < q1; ++q) acc = cfma(P::lval(st, q), ya[st.l_col[q]], acc);
-      k = cfma(P::cz(ws, lay, j), acc, k);
+      for (int q = q0; q < q1; ++q) acc = cfma(P::lval(st, q), y(a, st.l_col[q]), acc);
+      k = cfma(cf.cz(j), acc, k);
     }
   }
-  for (int q = st.h_ptr[s]; q < st.h_ptr[s + 1]; ++q) k = cfma(P::hval(st, q), ya[st.h_col[q]], k);
+  for (int q = st.h_ptr[s]; q < st.h_ptr[s + 1]; ++q) k = cfma(P::hval(st, q), y(a, st.h_col[q]), k);
   const int u0 = st.up_ptr[a], u1 = st.up_ptr[a + 1];
   for (int p = u0; p < u1; ++p) {
     const int u = st.up_aux[p], m = st.up_mode[p];
-    const T* yu = row(u);
-    T c = P::upc(ws, lay, m);
+    T c = cf.upc(m);
     if (SITE) {
-      const int j = st.mode_lop[m];
-      if (st.lop_site[j] == s) c = csub(c, cmul(P::gw(st, m), P::sval(st, j)));
-      k = cfma(c, yu[s], k);
+      if (st.mode_site[m] == s) c = csub(c, P::gwv(st, m));
+      k = cfma(c, y(u, s), k);
     } else {
-      k = cfma(c, yu[s], k);
-      const int j = st.mode_lop[m];
-      const int base = j * (st.n_state + 1);
-      int q0 = st.l_ptr[base + s], q1 = st.l_ptr[base + s + 1];
+      k = cfma(c, y(u, s), k);
+      const int base = st.mode_lop[m] * (st.n_state + 1);
+      const int q0 = st.l_ptr[base + s], q1 = st.l_ptr[base + s + 1];
       if (q0 != q1) {
         T acc = czero<T>();
-        for (int q = q0; q < q1; ++q) acc = cfma(P::lval(st, q), yu[st.l_col[q]], acc);
+        for (int q = q0; q < q1; ++q) acc = cfma(P::lval(st, q), y(u, st.l_col[q]), acc);
         k = csub(k, cmul(P::gw(st, m), acc));
       }
     }
@@ -149,16 +194,14 @@ __device__ __forceinline__ typename Prec<R>::T deriv_elem(const hops_structure& 
   const int d0 = st.dn_ptr[a], d1 = st.dn_ptr[a + 1];
   for (int p = d0; p < d1; ++p) {
     const int d = st.dn_aux[p], m = st.dn_mode[p];
-    const int j = st.mode_lop[m];
-    const T* yd = row(d);
     if (SITE) {
-      if (st.lop_site[j] == s) k = cfma(cmul(P::dncoef(st, p), cconj(P::sval(st, j))), yd[s], k);
+      if (st.mode_site[m] == s) k = cfma(P::dncs(st, p), y(d, s), k);
     } else {
-      const int base = j * (st.n_state + 1);
-      int q0 = st.lh_ptr[base + s], q1 = st.lh_ptr[base + s + 1];
+      const int base = st.mode_lop[m] * (st.n_state + 1);
+      const int q0 = st.lh_ptr[base + s], q1 = st.lh_ptr[base + s + 1];
       if (q0 != q1) {
         T acc = czero<T>();
-        for (int q = q0; q < q1; ++q) acc = cfma(P::lhval(st, q), yd[st.lh_col[q]], acc);
+        for (int q = q0; q < q1; ++q) acc = cfma(P::lhval(st, q), y(d, st.lh_col[q]), acc);
         k = cfma(P::dncoef(st, p), acc, k);
       }
     }
@@ -166,90 +209,268 @@ __device__ __forceinline__ typename Prec<R>::T deriv_elem(const hops_structure& 
   return k;
 }
 
+// ------------------------------------------------------- type conversion ----
+template <typename To> __device__ __forceinline__ To cv(double2 a);
+template <typename To> __device__ __forceinline__ To cv(float2 a);
+template <> __device__ __forceinline__ double2 cv<double2>(double2 a) { return a; }
+template <> __device__ __forceinline__ double2 cv<double2>(float2 a) { return mk(a.x, a.y); }
+template <> __device__ __forceinline__ float2 cv<float2>(float2 a) { return a; }
+template <> __device__ __forceinline__ float2 cv<float2>(double2 a) { return mkf((float)a.x, (float)a.y); }
+
+// Division by a run-time constant d < 2^31 with one multiply-high and a shift
+// (Granlund & Montgomery, "Division by invariant integers using
+// multiplication", 1994): l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1,
+// n / d = (mulhi(m, n) + n) >> l for every 32-bit n.
+struct FastDiv {
+  unsigned d, m, l;
+  FastDiv() : d(1), m(1), l(0) {}
+  explicit FastDiv(unsigned dd) : d(dd) {
+    l = 0;
+    while ((1ull << l) < dd) ++l;
+    m = (unsigned)((((1ull << 32) * ((1ull << l) - dd)) / dd) + 1);
+  }
+  __device__ __forceinline__ unsigned div(unsigned n) const {
+    const unsigned hi = __umulhi(m, n);
+    return (unsigned)(((unsigned long long)hi + n) >> l);
+  }
+};
 
 // ----------------------------------------------------------- stage update ----
-template <typename T, typename R>
-__device__ __forceinline__ T cdiv6(T a) {
-  a.x = a.x / (R)6;
-  a.y = a.y / (R)6;
-  return a;
-}
-
-// RK4 bookkeeping of one element (integrator_rk.py:66-73); phis = phi at the
-// start of the step (normalised).  Stage 4 = plain derivative output.
-template <typename T, typename R>
-__device__ __forceinline__ void rk_update(int stage, R h, T k, T phis, T* acc, T* yout, T* phi,
-                                          size_t e) {
+// RK4 bookkeeping of one element (integrator_rk.py:66-73).  ph: the state at
+// the start of the step (already scaled), in the state precision PT; k, acc and
+// the stage inputs in the stage precision T.  The stage inputs and the new
+// state are formed in PT arithmetic, then rounded to their storage types.
+// Stage 4 = plain derivative output.
+template <typename T, typename PT>
+__device__ __forceinline__ void rk_update(int stage, double h, T k, PT ph, T* acc, T* yout, PT* phi,
+                                          T* shadow, size_t e) {
+  using RP = decltype(ph.x);
+  const RP hh = (RP)h;
   switch (stage) {
-    case 0:
+    case 0: {
       acc[e] = k;
-      yout[e] = cadd(phis, cscale(k, h * (R)0.5));
-      break;
+      yout[e] = cv<T>(cadd(ph, cscale(cv<PT>(k), hh * (RP)0.5)));
+    } break;
     case 1:
-      acc[e] = cadd(acc[e], cscale(k, (R)2));
-      yout[e] = cadd(phis, cscale(k, h * (R)0.5));
-      break;
-    case 2:
-      acc[e] = cadd(acc[e], cscale(k, (R)2));
-      yout[e] = cadd(phis, cscale(k, h));
-      break;
+    case 2: {
+      acc[e] = cadd(acc[e], cscale(k, (decltype(k.x))2));
+      const RP c = stage == 1 ? hh * (RP)0.5 : hh;
+      yout[e] = cv<T>(cadd(ph, cscale(cv<PT>(k), c)));
+    } break;
     case 3: {
-      T sum = cadd(acc[e], k);
-      phi[e] = cadd(phis, cdiv6<T, R>(cscale(sum, h)));
+      PT sum = cv<PT>(cadd(acc[e], k));
+      PT hs = cscale(sum, hh);
+      hs.x = hs.x / (RP)6;
+      hs.y = hs.y / (RP)6;
+      const PT nw = cadd(ph, hs);
+      phi[e] = nw;
+      if (shadow) shadow[e] = cv<T>(nw);
     } break;
     default:
       yout[e] = k;
   }
 }
 
-// ------------------------------------------------ streaming stage kernel ----
-// One RK stage for B trajectories sharing a structure.  Groups of G lanes own
-// one aux a at a time (warp-uniform connection lists); lanes stride over the
-// B*S elements of that aux.  Stage 0 reads the un-normalised phi and folds the
-// pending per-trajectory scale into k (the derivative is linear in Y once the
-// stage scalars are fixed).
-template <typename R, bool SITE>
-__global__ void __launch_bounds__(256) k_stage(hops_structure st, int B, int stage, R h,
-                                               const typename Prec<R>::T* __restrict__ yin,
-                                               typename Prec<R>::T* yout,
-                                               typename Prec<R>::T* phi,
-                                               typename Prec<R>::T* acc,
-                                               const double* __restrict__ ws_all, int G) {
+// ---------------------------------------------------- wide stage kernel ----
+// B >= 32 trajectories: one warp per (aux a, state s); lane l owns the
+// trajectories b = bg + l + 32 j, j < NB.  Connection lists, coefficients and
+// the site test are warp-uniform and loaded once per neighbour for NB x 32
+// trajectories; every Y load is a coalesced 32-trajectory segment and the NB
+// independent loads per neighbour are in flight together.
+template <typename R, typename PT, bool SITE, int NB>
+__global__ void __launch_bounds__(256) k_wide(hops_structure st, int B, int stage, double h,
+                                              const typename Prec<R>::T* __restrict__ yin,
+                                              typename Prec<R>::T* __restrict__ yout, PT* phi,
+                                              typename Prec<R>::T* shadow,
+                                              typename Prec<R>::T* acc,
+                                              const double* __restrict__ ws, FastDiv divS) {
+  using P = Prec<R>;
+  using T = typename P::T;
+  const int S = st.n_state;
+  const BatchLayout bl(S, st.n_mode, st.n_lop, B);
+  const T* upcT = reinterpret_cast<const T*>(ws + (sizeof(R) == 8 ? bl.upcT : bl.upcT_f));
+  const T* diagT = reinterpret_cast<const T*>(ws + (sizeof(R) == 8 ? bl.diagT : bl.diagT_f));
+  const T* czT = reinterpret_cast<const T*>(ws + (sizeof(R) == 8 ? bl.czT : bl.czT_f));
+  const double* ncB = ws + bl.ncB;
+  const double* scaleB = ws + bl.scaleB;
+  const int lane = threadIdx.x & 31;
+  const unsigned ntask = (unsigned)st.n_hier * (unsigned)S;
+  const unsigned nw = (gridDim.x * blockDim.x) >> 5;
+  for (unsigned t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntask; t += nw) {
+    const int a = (int)divS.div(t);
+    const int s = (int)t - a * S;
+    const size_t rowa = ((size_t)a * S + s) * B;
+    const T kd = P::kdec(st, a);
+    const int u0 = st.up_ptr[a], u1 = st.up_ptr[a + 1];
+    const int d0 = st.dn_ptr[a], d1 = st.dn_ptr[a + 1];
+    const int h0 = st.h_ptr[s], h1 = st.h_ptr[s + 1];
+    for (int bg = 0; bg < B; bg += 32 * NB) {
+      T k[NB];
+      bool ok[NB];
+#pragma unroll
+      for (int j = 0; j < NB; ++j) {
+        const int b = bg + lane + 32 * j;
+        ok[j] = b < B;
+        k[j] = czero<T>();
+        if (ok[j]) {
+          T c = kd;
+          if (SITE) {
+            c = cadd(c, diagT[(size_t)s * B + b]);
+          } else {
+            c.x -= (R)ncB[b];
+          }
+          k[j] = cmul(c, yin[rowa + b]);
+        }
+      }
+      if (!SITE) {
+        // noise term sum_j cz_j (L_j Y[a])[s] for general L
+        for (int jl = 0; jl < st.n_lop; ++jl) {
+          const int base = jl * (S + 1);
+          const int q0 = st.l_ptr[base + s], q1 = st.l_ptr[base + s + 1];
+          for (int q = q0; q < q1; ++q) {
+            const T lv = P::lval(st, q);
+            const size_t rb = ((size_t)a * S + st.l_col[q]) * B + bg + lane;
+#pragma unroll
+            for (int j = 0; j < NB; ++j)
+              if (ok[j]) k[j] = cfma(cmul(czT[(size_t)jl * B + bg + lane + 32 * j], lv), yin[rb + 32 * j], k[j]);
+          }
+        }
+      }
+      for (int q = h0; q < h1; ++q) {
+        const T hv = P::hval(st, q);
+        const size_t rb = ((size_t)a * S + st.h_col[q]) * B + bg + lane;
+#pragma unroll
+        for (int j = 0; j < NB; ++j)
+          if (ok[j]) k[j] = cfma(hv, yin[rb + 32 * j], k[j]);
+      }
+      for (int p = u0; p < u1; ++p) {
+        const int u = st.up_aux[p], m = st.up_mode[p];
+        const size_t rb = ((size_t)u * S + s) * B + bg + lane;
+        const T* up = upcT + (size_t)m * B + bg + lane;
+        if (SITE) {
+          const bool hit = st.mode_site[m] == s;
+          const T corr = hit ? P::gwv(st, m) : czero<T>();
+#pragma unroll
+          for (int j = 0; j < NB; ++j)
+            if (ok[j]) k[j] = cfma(csub(up[32 * j], corr), yin[rb + 32 * j], k[j]);
+        } else {
+#pragma unroll
+          for (int j = 0; j < NB; ++j)
+            if (ok[j]) k[j] = cfma(up[32 * j], yin[rb + 32 * j], k[j]);
+          const int base = st.mode_lop[m] * (S + 1);
+          const int q0 = st.l_ptr[base + s], q1 = st.l_ptr[base + s + 1];
+          for (int q = q0; q < q1; ++q) {
+            const T lv = cmul(P::gw(st, m), P::lval(st, q));
+            const size_t rb2 = ((size_t)u * S + st.l_col[q]) * B + bg + lane;
+#pragma unroll
+            for (int j = 0; j < NB; ++j)
+              if (ok[j]) k[j] = csub(k[j], cmul(lv, yin[rb2 + 32 * j]));
+          }
+        }
+      }
+      for (int p = d0; p < d1; ++p) {
+        const int d = st.dn_aux[p], m = st.dn_mode[p];
+        if (SITE) {
+          if (st.mode_site[m] != s) continue;
+          const T cf = P::dncs(st, p);
+          const size_t rb = ((size_t)d * S + s) * B + bg + lane;
+#pragma unroll
+          for (int j = 0; j < NB; ++j)
+            if (ok[j]) k[j] = cfma(cf, yin[rb + 32 * j], k[j]);
+        } else {
+          const int base = st.mode_lop[m] * (S + 1);
+          const int q0 = st.lh_ptr[base + s], q1 = st.lh_ptr[base + s + 1];
+          for (int q = q0; q < q1; ++q) {
+            const T cf = cmul(P::dncoef(st, p), P::lhval(st, q));
+            const size_t rb = ((size_t)d * S + st.lh_col[q]) * B + bg + lane;
+#pragma unroll
+            for (int j = 0; j < NB; ++j)
+              if (ok[j]) k[j] = cfma(cf, yin[rb + 32 * j], k[j]);
+          }
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < NB; ++j) {
+        if (!ok[j]) continue;
+        const int b = bg + lane + 32 * j;
+        const size_t e = rowa + b;
+        const double sc = scaleB[b];
+        T kk = k[j];
+        if (stage == 0 || stage == 4) kk = cscale(kk, (R)sc);
+        const PT ph = stage == 4 ? PT{} : cscale(phi[e], (decltype(PT{}.x))sc);
+        rk_update<T, PT>(stage, h, kk, ph, acc, yout, phi, shadow, e);
+      }
+    }
+  }
+}
+
+// -------------------------------------------------- narrow stage kernel ----
+// B < 32 trajectories: one warp per aux a (warp-uniform connection lists),
+// lanes over the S*B elements (state s, trajectory b) of that aux.
+template <typename R, typename PT, bool SITE>
+__global__ void __launch_bounds__(256) k_narrow(hops_structure st, int B, int stage, double h,
+                                                const typename Prec<R>::T* __restrict__ yin,
+                                                typename Prec<R>::T* __restrict__ yout, PT* phi,
+                                                typename Prec<R>::T* shadow,
+                                                typename Prec<R>::T* acc,
+                                                const double* __restrict__ ws, FastDiv divB) {
   using T = typename Prec<R>::T;
   const int S = st.n_state;
-  const int BS = B * S;
-  const ScalarLayout lay(S, st.n_mode, st.n_lop);
+  const int SB = S * B;
+  const BatchLayout bl(S, st.n_mode, st.n_lop, B);
+  const double* scaleB = ws + bl.scaleB;
   const int lane = threadIdx.x & 31;
-  const int gpw = 32 / G;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  const int sub = lane / G, r0 = lane - sub * G;
-  for (int a = warp * gpw + sub; a < st.n_hier; a += nwarps * gpw) {
-    for (int r = r0; r < BS; r += G) {
-      const int b = r / S, s = r - b * S;
-      const double* ws = ws_all + (size_t)b * lay.stride;
-      auto row = [&](int x) { return yin + ((size_t)x * B + b) * S; };
-      T k = deriv_elem<R, SITE>(st, ws, lay, a, s, row);
-      const size_t e = (size_t)a * BS + r;
-      const R sc = (R)ws[lay.scale()];
-      T phis;
-      if (stage == 0 || stage == 4) {
-        k = cscale(k, sc);
-        phis = cscale(yin[e], sc);
-      } else {
-        phis = cscale(phi[e], sc);
-      }
-      rk_update<T, R>(stage, h, k, phis, acc, yout, phi, e);
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; a < st.n_hier; a += nw) {
+    for (int r = lane; r < SB; r += 32) {
+      const int s = (int)divB.div((unsigned)r);
+      const int b = r - s * B;
+      auto y = [&](int x, int sp) { return yin[((size_t)x * S + sp) * B + b]; };
+      const CoefT<R> cf{ws, bl, B, b};
+      T k = deriv_elem<R, SITE>(st, a, s, y, cf);
+      const size_t e = (size_t)a * SB + r;
+      const double sc = scaleB[b];
+      if (stage == 0 || stage == 4) k = cscale(k, (R)sc);
+      const PT ph = stage == 4 ? PT{} : cscale(phi[e], (decltype(PT{}.x))sc);
+      rk_update<T, PT>(stage, h, k, ph, acc, yout, phi, shadow, e);
     }
   }
 }
 
 // ----------------------------------------------- streaming scalar kernel ----
-// One CTA per trajectory: FP64 stage scalars (stage_scalars) of stage `stage`
-// from the stage input yin.  With recompute_scale, first renormalises the state
-// produced by the previous step (hops_trajectory.py:616-634) by recording the
-// factor 1/||psi_0|| that the stage kernels apply on the fly.
-template <typename R>
+// One CTA per trajectory b: FP64 stage scalars (stage_scalars) of stage
+// `stage`, then published in trajectory-fastest layout for the stage kernels.
+// Stage 0 / 4 read the state phi (precision PT) with the pending scale; the
+// other stages read the stage input (precision T).  With recompute_scale the
+// CTA first renormalises the state produced by the previous step
+// (hops_trajectory.py:616-634) by recording 1/||psi_0||, which every stage
+// kernel applies on the fly.
+__device__ void publish(const hops_structure& st, const BatchLayout& bl, double* wsall, int B,
+                        int b, const double* ws) {
+  const int S = st.n_state, M = st.n_mode, L = st.n_lop;
+  const ScalarLayout lay(S, M, L);
+  for (int m = threadIdx.x; m < M; m += blockDim.x) {
+    double2 v = ld2(ws + lay.upc(), m);
+    reinterpret_cast<double2*>(wsall + bl.upcT)[(size_t)m * B + b] = v;
+    reinterpret_cast<float2*>(wsall + bl.upcT_f)[(size_t)m * B + b] = mkf((float)v.x, (float)v.y);
+  }
+  for (int s = threadIdx.x; s < S; s += blockDim.x) {
+    double2 v = ld2(ws + lay.diagD(), s);
+    reinterpret_cast<double2*>(wsall + bl.diagT)[(size_t)s * B + b] = v;
+    reinterpret_cast<float2*>(wsall + bl.diagT_f)[(size_t)s * B + b] = mkf((float)v.x, (float)v.y);
+  }
+  for (int j = threadIdx.x; j < L; j += blockDim.x) {
+    double2 v = ld2(ws + lay.cz(), j);
+    reinterpret_cast<double2*>(wsall + bl.czT)[(size_t)j * B + b] = v;
+    reinterpret_cast<float2*>(wsall + bl.czT_f)[(size_t)j * B + b] = mkf((float)v.x, (float)v.y);
+  }
+  if (threadIdx.x == 0) {
+    wsall[bl.ncB + b] = ws[lay.nc()];
+    wsall[bl.scaleB + b] = ws[lay.scale()];
+  }
+}
+
+template <typename R, typename PT>
 __global__ void __launch_bounds__(128) k_scalars(hops_structure st, hops_batch bt, int stage, int it,
                                                  double h, const void* yin, int recompute_scale,
                                                  double* psi_prev, const float* z1s,
@@ -261,14 +482,15 @@ __global__ void __launch_bounds__(128) k_scalars(hops_structure st, hops_batch b
   const int b = blockIdx.x;
   const int S = st.n_state, M = st.n_mode, L = st.n_lop, B = bt.n_traj;
   const ScalarLayout lay(S, M, L);
+  const BatchLayout bl(S, M, L, B);
   double* ws = bt.work + (size_t)b * lay.stride;
-  const T* ph = static_cast<const T*>(bt.phi);
+  const PT* ph = static_cast<const PT*>(bt.phi);
   if (recompute_scale || psi_prev) {
     double sc = ws[lay.scale()];
     if (recompute_scale) {
       double p = 0.0;
       for (int s = threadIdx.x; s < S; s += blockDim.x) {
-        double2 v = to_d(ph[(size_t)b * S + s]);
+        double2 v = to_d(ph[(size_t)s * B + b]);
         p += v.x * v.x + v.y * v.y;
       }
       const double n2 = block_sum(p, red);
@@ -282,10 +504,11 @@ __global__ void __launch_bounds__(128) k_scalars(hops_structure st, hops_batch b
     }
     if (psi_prev)
       for (int s = threadIdx.x; s < S; s += blockDim.x)
-        reinterpret_cast<double2*>(psi_prev)[(size_t)b * S + s] = cscale(to_d(ph[(size_t)b * S + s]), sc);
+        reinterpret_cast<double2*>(psi_prev)[(size_t)b * S + s] = cscale(to_d(ph[(size_t)s * B + b]), sc);
     __syncthreads();
   }
-  const double sc = (stage == 0 || stage == 4) ? ws[lay.scale()] : 1.0;
+  const bool from_phi = stage == 0 || stage == 4;
+  const double sc = from_phi ? ws[lay.scale()] : 1.0;
   StageIO io;
   io.zmem = bt.zmem + (size_t)b * M * 2;
   if (stage == 4) {
@@ -309,27 +532,29 @@ __global__ void __launch_bounds__(128) k_scalars(hops_structure st, hops_batch b
   io.ws = ws;
   const T* y = static_cast<const T*>(yin);
   auto get = [&](int a, int s) -> double2 {
-    return cscale(to_d(y[((size_t)a * B + b) * S + s]), sc);
+    const size_t i = ((size_t)a * S + s) * B + b;
+    return from_phi ? cscale(to_d(ph[i]), sc) : to_d(y[i]);
   };
   stage_scalars(st, io, get, red, sh);
+  publish(st, bl, bt.work, B, b, ws);
 }
 
 // Normalisation after the last step of a call: records 1/||psi_0|| per
 // trajectory and writes the last psi_0.
-template <typename R>
+template <typename PT>
 __global__ void __launch_bounds__(128) k_finalize(hops_structure st, hops_batch bt, double* psi_last,
                                                   int normalize) {
-  using T = typename Prec<R>::T;
   __shared__ double red[32];
-  const int b = blockIdx.x, S = st.n_state;
+  const int b = blockIdx.x, S = st.n_state, B = bt.n_traj;
   const ScalarLayout lay(S, st.n_mode, st.n_lop);
+  const BatchLayout bl(S, st.n_mode, st.n_lop, B);
   double* ws = bt.work + (size_t)b * lay.stride;
-  const T* ph = static_cast<const T*>(bt.phi);
+  const PT* ph = static_cast<const PT*>(bt.phi);
   double sc = 1.0;
   if (normalize) {
     double p = 0.0;
     for (int s = threadIdx.x; s < S; s += blockDim.x) {
-      double2 v = to_d(ph[(size_t)b * S + s]);
+      double2 v = to_d(ph[(size_t)s * B + b]);
       p += v.x * v.x + v.y * v.y;
     }
     const double n2 = block_sum(p, red);
@@ -339,26 +564,31 @@ __global__ void __launch_bounds__(128) k_finalize(hops_structure st, hops_batch 
       sc = 1.0;
     }
   }
-  if (threadIdx.x == 0) ws[lay.scale()] = sc;
+  if (threadIdx.x == 0) {
+    ws[lay.scale()] = sc;
+    bt.work[bl.scaleB + b] = sc;
+  }
   if (psi_last)
     for (int s = threadIdx.x; s < S; s += blockDim.x)
-      reinterpret_cast<double2*>(psi_last)[(size_t)b * S + s] = cscale(to_d(ph[(size_t)b * S + s]), sc);
+      reinterpret_cast<double2*>(psi_last)[(size_t)b * S + s] = cscale(to_d(ph[(size_t)s * B + b]), sc);
 }
 
-template <typename R>
-__global__ void k_apply_scale(typename Prec<R>::T* phi, int B, int S, size_t E,
-                              const double* ws, int stride) {
+template <typename PT, typename T>
+__global__ void k_apply_scale(PT* phi, T* shadow, int B, size_t E, const double* scaleB) {
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < E;
        e += (size_t)gridDim.x * blockDim.x) {
-    const int b = (int)((e / S) % B);
-    phi[e] = cscale(phi[e], (R)ws[(size_t)b * stride]);
+    const PT v = cscale(phi[e], (decltype(PT{}.x))scaleB[e % B]);
+    phi[e] = v;
+    if (shadow) shadow[e] = cv<T>(v);
   }
 }
 
-__global__ void k_reset(double* ws, int stride, int B, int32_t* status, int clear_status) {
+__global__ void k_reset(double* ws, int stride, size_t scale_off, int B, int32_t* status,
+                        int clear_status) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b < B) {
     ws[(size_t)b * stride] = 1.0;
+    ws[scale_off + b] = 1.0;
     if (clear_status && status) status[b] = 0;
   }
 }
@@ -369,10 +599,11 @@ __global__ void k_reset(double* ws, int stride, int B, int32_t* status, int clea
 // between them (no grid-wide synchronisation).  Vectors live in shared memory
 // when they fit (mode 2: phi, acc, y0, y1; mode 1: y0, y1), else in the task's
 // scratch.  Tasks may carry different structures (uneven adaptive bases).
-template <typename R, bool SITE>
-__global__ void __launch_bounds__(512) k_resident(hops_task* tasks, int mode, int max_elems,
-                                                  int sc_doubles) {
+template <typename R, typename PT, bool SITE>
+__global__ void __launch_bounds__(512, 1) k_resident(hops_task* tasks, int mode, int max_elems,
+                                                     int sc_doubles) {
   using T = typename Prec<R>::T;
+  using RP = decltype(PT{}.x);
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ hops_structure st;
   __shared__ double red[32];
@@ -385,17 +616,19 @@ __global__ void __launch_bounds__(512) k_resident(hops_task* tasks, int mode, in
   double* ws = reinterpret_cast<double*>(smraw);
   double* zm = ws + lay.stride;
   double* sh = zm + 2 * M;
-  T* vec = reinterpret_cast<T*>(smraw + (size_t)sc_doubles * sizeof(double));
-  T *phi, *acc, *y0, *y1;
-  T* gphi = static_cast<T*>(tk->phi);
+  unsigned char* vbase = smraw + (size_t)sc_doubles * sizeof(double);
+  PT* gphi = static_cast<PT*>(tk->phi);
+  PT* phi;
+  T *acc, *y0, *y1;
   if (mode == 2) {
-    phi = vec;
-    acc = vec + max_elems;
-    y0 = vec + 2 * max_elems;
-    y1 = vec + 3 * max_elems;
+    phi = reinterpret_cast<PT*>(vbase);
+    T* v = reinterpret_cast<T*>(vbase + (size_t)max_elems * sizeof(PT));
+    acc = v;
+    y0 = v + max_elems;
+    y1 = v + 2 * max_elems;
   } else if (mode == 1) {
-    y0 = vec;
-    y1 = vec + max_elems;
+    y0 = reinterpret_cast<T*>(vbase);
+    y1 = y0 + max_elems;
     phi = gphi;
     acc = static_cast<T*>(tk->scratch);
   } else {
@@ -404,13 +637,12 @@ __global__ void __launch_bounds__(512) k_resident(hops_task* tasks, int mode, in
     y0 = acc + E;
     y1 = acc + 2 * E;
   }
-  const R sc0 = (R)tk->scale;
+  const RP sc0 = (RP)tk->scale;
   for (int e = threadIdx.x; e < E; e += blockDim.x) phi[e] = cscale(gphi[e], sc0);
   for (int m = threadIdx.x; m < M; m += blockDim.x)
     reinterpret_cast<double2*>(zm)[m] = reinterpret_cast<const double2*>(tk->zmem)[m];
   __syncthreads();
   const bool normalized = tk->eom == HOPS_EOM_NORMALIZED_NONLINEAR;
-  const R h = (R)tk->tau_over_hbar;
   int status = 0;
   StageIO io;
   io.zmem = zm;
@@ -422,19 +654,31 @@ __global__ void __launch_bounds__(512) k_resident(hops_task* tasks, int mode, in
   io.eom = tk->eom;
   io.h = tk->tau_over_hbar;
   io.ws = ws;
+  const CoefWS<R> cf{ws, lay};
   for (int n = 0; n < tk->n_steps; ++n) {
     for (int stage = 0; stage < 4; ++stage) {
-      const T* yin = stage == 0 ? phi : (stage == 1 ? y0 : (stage == 2 ? y1 : y0));
+      const T* yin = stage == 1 ? y0 : (stage == 2 ? y1 : y0);
       T* yout = stage == 0 ? y0 : (stage == 1 ? y1 : (stage == 2 ? y0 : nullptr));
       io.it = tk->it0 + 2 * n * tk->di + rk_noise_slot(stage) * tk->di;
       io.stage = stage;
-      auto get = [&](int a, int s) -> double2 { return to_d(yin[a * S + s]); };
-      stage_scalars(st, io, get, red, sh);
-      auto row = [&](int x) { return yin + x * S; };
-      for (int e = threadIdx.x; e < E; e += blockDim.x) {
-        const int a = e / S, s = e - a * S;
-        T k = deriv_elem<R, SITE>(st, ws, lay, a, s, row);
-        rk_update<T, R>(stage, h, k, phi[e], acc, yout, phi, (size_t)e);
+      if (stage == 0) {
+        auto get = [&](int a, int s) -> double2 { return to_d(phi[a * S + s]); };
+        stage_scalars(st, io, get, red, sh);
+        auto y = [&](int x, int sp) { return cv<T>(phi[x * S + sp]); };
+        for (int e = threadIdx.x; e < E; e += blockDim.x) {
+          const int a = e / S, s = e - a * S;
+          const T k = deriv_elem<R, SITE>(st, a, s, y, cf);
+          rk_update<T, PT>(stage, io.h, k, phi[e], acc, yout, phi, (T*)nullptr, (size_t)e);
+        }
+      } else {
+        auto get = [&](int a, int s) -> double2 { return to_d(yin[a * S + s]); };
+        stage_scalars(st, io, get, red, sh);
+        auto y = [&](int x, int sp) { return yin[x * S + sp]; };
+        for (int e = threadIdx.x; e < E; e += blockDim.x) {
+          const int a = e / S, s = e - a * S;
+          const T k = deriv_elem<R, SITE>(st, a, s, y, cf);
+          rk_update<T, PT>(stage, io.h, k, phi[e], acc, yout, phi, (T*)nullptr, (size_t)e);
+        }
       }
       __syncthreads();
     }
@@ -450,7 +694,7 @@ __global__ void __launch_bounds__(512) k_resident(hops_task* tasks, int mode, in
         status = HOPS_ENONFINITE;
         sc = 1.0;
       }
-      for (int e = threadIdx.x; e < E; e += blockDim.x) phi[e] = cscale(phi[e], (R)sc);
+      for (int e = threadIdx.x; e < E; e += blockDim.x) phi[e] = cscale(phi[e], (RP)sc);
       __syncthreads();
     }
     if (tk->psi_out)
@@ -471,6 +715,44 @@ __global__ void __launch_bounds__(512) k_resident(hops_task* tasks, int mode, in
 // ============================================================= C ABI =========
 static int g_sm_count = 0;
 
+// Optional CUDA-event timing of the stage kernels (profiling aid; one host
+// thread at a time).  Each stage-kernel launch is bracketed by two events on
+// its stream; hops_kernel_timing_read sums the elapsed times.
+static bool g_timing = false;
+static std::vector<cudaEvent_t> g_ev;
+static size_t g_ev_used = 0;
+
+static cudaEvent_t timing_event() {
+  if (g_ev_used == g_ev.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    g_ev.push_back(e);
+  }
+  return g_ev[g_ev_used++];
+}
+
+extern "C" int hops_kernel_timing(int enable) {
+  g_timing = enable != 0;
+  g_ev_used = 0;
+  return HOPS_OK;
+}
+
+extern "C" int hops_kernel_timing_read(double* total_ms, int64_t* n_launches) {
+  double tot = 0.0;
+  int64_t n = 0;
+  for (size_t i = 0; i + 1 < g_ev_used; i += 2) {
+    float ms = 0.f;
+    CUDA_TRY(cudaEventSynchronize(g_ev[i + 1]));
+    CUDA_TRY(cudaEventElapsedTime(&ms, g_ev[i], g_ev[i + 1]));
+    tot += ms;
+    ++n;
+  }
+  if (total_ms) *total_ms = tot;
+  if (n_launches) *n_launches = n;
+  g_ev_used = 0;
+  return HOPS_OK;
+}
+
 static int sm_count() {
   if (g_sm_count == 0) {
     int dev = 0;
@@ -486,39 +768,37 @@ static int check_structure(const hops_structure* st) {
   if (st->n_hier <= 0 || st->n_state <= 0 || st->n_mode < 0 || st->n_lop < 0)
     return set_err(HOPS_EINVAL, "bad structure sizes n_hier=%d n_state=%d n_mode=%d n_lop=%d",
                    st->n_hier, st->n_state, st->n_mode, st->n_lop);
+  if ((long)st->n_hier * st->n_state >= (1L << 31))
+    return set_err(HOPS_ENOTSUP, "n_hier * n_state must be below 2^31");
   if (!st->k_decay || !st->up_ptr || !st->dn_ptr || !st->h_ptr || !st->l_ptr || !st->lop_active)
     return set_err(HOPS_EINVAL, "structure has null tables");
-  if (st->site_projector && (!st->lop_site || !st->lop_sval))
-    return set_err(HOPS_EINVAL, "site-projector structure without lop_site/lop_sval");
+  if (st->site_projector && (!st->lop_site || !st->lop_sval || !st->mode_site || !st->mode_gwv ||
+                             !st->mode_gwv_f || !st->dn_coef_site || !st->dn_coef_site_f))
+    return set_err(HOPS_EINVAL, "site-projector structure without its site tables");
   return HOPS_OK;
 }
 
 static int check_batch(const hops_structure* st, const hops_batch* bt) {
   if (!bt) return set_err(HOPS_EINVAL, "null batch");
   if (bt->n_traj <= 0) return set_err(HOPS_EINVAL, "n_traj must be positive");
-  if (bt->precision != HOPS_PREC_C128 && bt->precision != HOPS_PREC_C64)
+  if (bt->precision != HOPS_PREC_C128 && bt->precision != HOPS_PREC_C64 &&
+      bt->precision != HOPS_PREC_MIXED)
     return set_err(HOPS_EINVAL, "unknown precision %d", bt->precision);
   if (bt->eom < 0 || bt->eom > 2) return set_err(HOPS_EINVAL, "unknown eom %d", bt->eom);
   if (!bt->phi || !bt->acc || !bt->y0 || !bt->y1 || !bt->zmem || !bt->work || !bt->status)
     return set_err(HOPS_EINVAL, "batch has null buffers");
-  if (bt->precision == HOPS_PREC_C64 &&
+  if (bt->precision == HOPS_PREC_MIXED && !bt->phi_lo)
+    return set_err(HOPS_EINVAL, "mixed-precision batch needs phi_lo");
+  if (bt->precision != HOPS_PREC_C128 &&
       (!st->k_decay_f || !st->dn_coef_f || !st->mode_gw_f || !st->h_val_f || !st->l_val_f ||
        !st->lh_val_f))
     return set_err(HOPS_EINVAL, "complex64 batch needs the float coefficient tables");
-  (void)st;
+  if ((long)st->n_hier * st->n_state * bt->n_traj >= (1L << 40))
+    return set_err(HOPS_ENOTSUP, "batch too large");
   return HOPS_OK;
 }
 
-static int group_lanes(int bs) {
-  if (bs >= 32) return 32;
-  int g = 1;
-  while (g < bs) g <<= 1;
-  return g;
-}
-
-static int stage_grid(const hops_structure* st, int G) {
-  const int gpw = 32 / G;
-  const long warps = (st->n_hier + gpw - 1) / gpw;
+static int grid_for_warps(long warps) {
   long blocks = (warps * 32 + 255) / 256;
   const long cap = (long)sm_count() * 16;
   if (blocks > cap) blocks = cap;
@@ -526,19 +806,52 @@ static int stage_grid(const hops_structure* st, int G) {
   return (int)blocks;
 }
 
-template <typename R>
-static int run_stage(const hops_structure* st, int B, int stage, double h, const void* yin,
-                     void* yout, void* phi, void* acc, const double* ws, cudaStream_t s) {
+template <typename R, typename PT, bool SITE, int NB>
+static void launch_wide(const hops_structure* st, int B, int stage, double h, const void* yin,
+                        void* yout, void* phi, void* shadow, void* acc, const double* ws,
+                        cudaStream_t s) {
   using T = typename Prec<R>::T;
-  const int G = group_lanes(B * st->n_state);
-  const int grid = stage_grid(st, G);
+  const int grid = grid_for_warps((long)st->n_hier * st->n_state);
+  k_wide<R, PT, SITE, NB><<<grid, 256, 0, s>>>(*st, B, stage, h, (const T*)yin, (T*)yout,
+                                               (PT*)phi, (T*)shadow, (T*)acc, ws,
+                                               FastDiv((unsigned)st->n_state));
+}
+
+template <typename R, typename PT, bool SITE>
+static void launch_stage(const hops_structure* st, int B, int stage, double h, const void* yin,
+                         void* yout, void* phi, void* shadow, void* acc, const double* ws,
+                         cudaStream_t s) {
+  using T = typename Prec<R>::T;
+  if (B >= 32) {
+    const int nb = (B + 31) / 32;
+    if (nb <= 1) launch_wide<R, PT, SITE, 1>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, s);
+    else if (nb <= 2) launch_wide<R, PT, SITE, 2>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, s);
+    else if (nb <= 4) launch_wide<R, PT, SITE, 4>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, s);
+    else launch_wide<R, PT, SITE, 8>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, s);
+  } else {
+    const int grid = grid_for_warps(st->n_hier);
+    k_narrow<R, PT, SITE><<<grid, 256, 0, s>>>(*st, B, stage, h, (const T*)yin, (T*)yout,
+                                               (PT*)phi, (T*)shadow, (T*)acc, ws,
+                                               FastDiv((unsigned)B));
+  }
+}
+
+template <typename R, typename PT>
+static int run_stage(const hops_structure* st, int B, int stage, double h, const void* yin,
+                     void* yout, void* phi, void* shadow, void* acc, const double* ws,
+                     cudaStream_t s) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (g_timing) {
+    e0 = timing_event();
+    e1 = timing_event();
+    if (e0) cudaEventRecord(e0, s);
+  }
   if (st->site_projector)
-    k_stage<R, true><<<grid, 256, 0, s>>>(*st, B, stage, (R)h, (const T*)yin, (T*)yout, (T*)phi,
-                                          (T*)acc, ws, G);
+    launch_stage<R, PT, true>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, s);
   else
-    k_stage<R, false><<<grid, 256, 0, s>>>(*st, B, stage, (R)h, (const T*)yin, (T*)yout, (T*)phi,
-                                           (T*)acc, ws, G);
+    launch_stage<R, PT, false>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, s);
   LAUNCH_CHECK();
+  if (g_timing && e1) cudaEventRecord(e1, s);
   return HOPS_OK;
 }
 
@@ -546,7 +859,7 @@ static size_t scalar_smem(const hops_structure* st) {
   return (size_t)(32 + 4 * st->n_lop + 2) * sizeof(double);
 }
 
-template <typename R>
+template <typename R, typename PT>
 static int propagate_impl(const hops_structure* st, hops_batch* bt, int32_t it0, int32_t di,
                           int32_t n_steps, double h, double* psi_out, cudaStream_t s) {
   using T = typename Prec<R>::T;
@@ -554,33 +867,38 @@ static int propagate_impl(const hops_structure* st, hops_batch* bt, int32_t it0,
   const size_t smem = scalar_smem(st);
   const bool normalized = bt->eom == HOPS_EOM_NORMALIZED_NONLINEAR;
   const size_t psi_stride = (size_t)B * S * 2;
+  void* shadow = bt->precision == HOPS_PREC_MIXED ? bt->phi_lo : nullptr;
   for (int n = 0; n < n_steps; ++n) {
     for (int i = 0; i < 4; ++i) {
       const int slot = i == 0 ? 0 : (i == 3 ? 2 : 1);
       const int it = it0 + 2 * n * di + slot * di;
-      const void* yin = i == 0 ? bt->phi : (i == 1 ? bt->y0 : (i == 2 ? bt->y1 : bt->y0));
+      // stage 0 gathers from the state (or its complex64 shadow in mixed mode)
+      const void* yin = i == 0 ? (shadow ? shadow : bt->phi)
+                               : (i == 1 ? bt->y0 : (i == 2 ? bt->y1 : bt->y0));
       void* yout = i == 0 ? bt->y0 : (i == 1 ? bt->y1 : (i == 2 ? bt->y0 : nullptr));
       const int recompute = (i == 0 && n > 0 && normalized) ? 1 : 0;
       double* psi_prev = (i == 0 && n > 0 && psi_out) ? psi_out + (size_t)(n - 1) * psi_stride : nullptr;
-      k_scalars<R><<<B, 128, smem, s>>>(*st, *bt, i, it, h, yin, recompute, psi_prev, nullptr,
-                                        nullptr, nullptr);
+      k_scalars<R, PT><<<B, 128, smem, s>>>(*st, *bt, i, it, h, yin, recompute, psi_prev, nullptr,
+                                            nullptr, nullptr);
       LAUNCH_CHECK();
-      int rc = run_stage<R>(st, B, i, h, yin, yout, bt->phi, bt->acc, bt->work, s);
+      int rc = run_stage<R, PT>(st, B, i, h, yin, yout, bt->phi, shadow, bt->acc, bt->work, s);
       if (rc) return rc;
     }
   }
   if (n_steps > 0) {
     double* psi_last = psi_out ? psi_out + (size_t)(n_steps - 1) * psi_stride : nullptr;
-    k_finalize<R><<<B, 128, 0, s>>>(*st, *bt, psi_last, normalized ? 1 : 0);
+    k_finalize<PT><<<B, 128, 0, s>>>(*st, *bt, psi_last, normalized ? 1 : 0);
     LAUNCH_CHECK();
     if (normalized) {
       const size_t E = (size_t)st->n_hier * B * S;
       long blocks = (long)((E + 255) / 256);
       if (blocks > (long)sm_count() * 8) blocks = (long)sm_count() * 8;
       const ScalarLayout lay(S, st->n_mode, st->n_lop);
-      k_apply_scale<R><<<(int)blocks, 256, 0, s>>>((T*)bt->phi, B, S, E, bt->work, lay.stride);
+      const BatchLayout bl(S, st->n_mode, st->n_lop, B);
+      k_apply_scale<PT, T><<<(int)blocks, 256, 0, s>>>((PT*)bt->phi, (T*)shadow, B, E,
+                                                        bt->work + bl.scaleB);
       LAUNCH_CHECK();
-      k_reset<<<(B + 127) / 128, 128, 0, s>>>(bt->work, lay.stride, B, nullptr, 0);
+      k_reset<<<(B + 127) / 128, 128, 0, s>>>(bt->work, lay.stride, bl.scaleB, B, nullptr, 0);
       LAUNCH_CHECK();
     }
   }
@@ -592,8 +910,9 @@ extern "C" int hops_batch_reset(const hops_structure* st, hops_batch* bt, void* 
   if (rc) return rc;
   if ((rc = check_batch(st, bt))) return rc;
   const ScalarLayout lay(st->n_state, st->n_mode, st->n_lop);
-  k_reset<<<(bt->n_traj + 127) / 128, 128, 0, (cudaStream_t)stream>>>(bt->work, lay.stride,
-                                                                       bt->n_traj, bt->status, 1);
+  const BatchLayout bl(st->n_state, st->n_mode, st->n_lop, bt->n_traj);
+  k_reset<<<(bt->n_traj + 127) / 128, 128, 0, (cudaStream_t)stream>>>(
+      bt->work, lay.stride, bl.scaleB, bt->n_traj, bt->status, 1);
   LAUNCH_CHECK();
   return HOPS_OK;
 }
@@ -605,7 +924,6 @@ extern "C" int hops_rk4_propagate(const hops_structure* st, hops_batch* bt, int3
   if (rc) return rc;
   if ((rc = check_batch(st, bt))) return rc;
   if (n_steps < 0 || it0 < 0 || di < 0) return set_err(HOPS_EINVAL, "negative step/noise index");
-  if (!bt->noise1 && bt->eom != HOPS_EOM_LINEAR && false) return set_err(HOPS_EINVAL, "no noise");
   const long last = (long)it0 + 2L * n_steps * di;
   if (n_steps > 0 && bt->noise1 && last >= bt->n_t1)
     return set_err(HOPS_EINVAL, "noise 1 too short: needs index %ld, has %d samples", last, bt->n_t1);
@@ -614,8 +932,21 @@ extern "C" int hops_rk4_propagate(const hops_structure* st, hops_batch* bt, int3
   if (scalar_smem(st) > 48 * 1024) return set_err(HOPS_ENOTSUP, "too many L operators (%d)", st->n_lop);
   cudaStream_t s = (cudaStream_t)stream;
   if (bt->precision == HOPS_PREC_C128)
-    return propagate_impl<double>(st, bt, it0, di, n_steps, tau_over_hbar, psi_out_dev, s);
-  return propagate_impl<float>(st, bt, it0, di, n_steps, tau_over_hbar, psi_out_dev, s);
+    return propagate_impl<double, double2>(st, bt, it0, di, n_steps, tau_over_hbar, psi_out_dev, s);
+  if (bt->precision == HOPS_PREC_MIXED)
+    return propagate_impl<float, double2>(st, bt, it0, di, n_steps, tau_over_hbar, psi_out_dev, s);
+  return propagate_impl<float, float2>(st, bt, it0, di, n_steps, tau_over_hbar, psi_out_dev, s);
+}
+
+template <typename R, typename PT>
+static int dsys_impl(const hops_structure* st, hops_batch* bt, const float* z1, const float* z2,
+                     void* dphi, double* dz, cudaStream_t s) {
+  k_scalars<R, PT><<<bt->n_traj, 128, scalar_smem(st), s>>>(*st, *bt, 4, 0, 0.0, bt->phi, 0, nullptr,
+                                                            z1, z2, dz);
+  LAUNCH_CHECK();
+  // stage 4 reads the state itself (mixed mode: its complex64 shadow)
+  const void* yin = bt->precision == HOPS_PREC_MIXED ? bt->phi_lo : bt->phi;
+  return run_stage<R, PT>(st, bt->n_traj, 4, 0.0, yin, dphi, bt->phi, nullptr, bt->acc, bt->work, s);
 }
 
 extern "C" int hops_dsystem_dt(const hops_structure* st, hops_batch* bt, const float* z1_dev,
@@ -627,55 +958,47 @@ extern "C" int hops_dsystem_dt(const hops_structure* st, hops_batch* bt, const f
   if (!dphi_dev || !dzmem_dev) return set_err(HOPS_EINVAL, "null outputs");
   if (scalar_smem(st) > 48 * 1024) return set_err(HOPS_ENOTSUP, "too many L operators (%d)", st->n_lop);
   cudaStream_t s = (cudaStream_t)stream;
-  const size_t smem = scalar_smem(st);
-  if (bt->precision == HOPS_PREC_C128) {
-    k_scalars<double><<<bt->n_traj, 128, smem, s>>>(*st, *bt, 4, 0, 0.0, bt->phi, 0, nullptr,
-                                                    z1_dev, z2_dev, dzmem_dev);
-    LAUNCH_CHECK();
-    return run_stage<double>(st, bt->n_traj, 4, 0.0, bt->phi, dphi_dev, bt->phi, bt->acc, bt->work, s);
-  }
-  k_scalars<float><<<bt->n_traj, 128, smem, s>>>(*st, *bt, 4, 0, 0.0, bt->phi, 0, nullptr, z1_dev,
-                                                 z2_dev, dzmem_dev);
-  LAUNCH_CHECK();
-  return run_stage<float>(st, bt->n_traj, 4, 0.0, bt->phi, dphi_dev, bt->phi, bt->acc, bt->work, s);
+  if (bt->precision == HOPS_PREC_C128)
+    return dsys_impl<double, double2>(st, bt, z1_dev, z2_dev, dphi_dev, dzmem_dev, s);
+  if (bt->precision == HOPS_PREC_MIXED)
+    return dsys_impl<float, double2>(st, bt, z1_dev, z2_dev, dphi_dev, dzmem_dev, s);
+  return dsys_impl<float, float2>(st, bt, z1_dev, z2_dev, dphi_dev, dzmem_dev, s);
 }
 
-static size_t resident_sc_doubles(int max_sc) {
-  // scalar block + z_mem copy + stage scratch, rounded to 16 bytes
-  return (size_t)((max_sc + 1) & ~1);
-}
+static size_t resident_sc_doubles(int max_sc) { return (size_t)((max_sc + 1) & ~1); }
 
-template <typename R>
-static int resident_impl(hops_task* tasks, int n_tasks, int max_elems, int max_sc,
-                         int site, cudaStream_t s) {
+template <typename R, typename PT>
+static int resident_impl(hops_task* tasks, int n_tasks, int max_elems, int max_sc, int site,
+                         cudaStream_t s) {
   using T = typename Prec<R>::T;
   int dev = 0, optin = 0;
   CUDA_TRY(cudaGetDevice(&dev));
   CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   const size_t scb = resident_sc_doubles(max_sc) * sizeof(double);
   const size_t budget = (size_t)optin - sizeof(hops_structure) - 32 * sizeof(double) - 64;
+  const size_t full = scb + (size_t)max_elems * (sizeof(PT) + 3 * sizeof(T));
+  const size_t half = scb + 2 * (size_t)max_elems * sizeof(T);
   int mode = 0;
   size_t smem = scb;
-  if (scb + 4 * (size_t)max_elems * sizeof(T) <= budget) {
+  if (full <= budget) {
     mode = 2;
-    smem = scb + 4 * (size_t)max_elems * sizeof(T);
-  } else if (scb + 2 * (size_t)max_elems * sizeof(T) <= budget) {
+    smem = full;
+  } else if (half <= budget) {
     mode = 1;
-    smem = scb + 2 * (size_t)max_elems * sizeof(T);
+    smem = half;
   } else if (scb > budget) {
     return set_err(HOPS_ENOTSUP, "resident scalar block of %zu bytes exceeds shared memory", scb);
   }
   int threads = ((max_elems + 31) / 32) * 32;
   if (threads < 64) threads = 64;
   if (threads > 512) threads = 512;
+  const int scd = (int)resident_sc_doubles(max_sc);
   if (site) {
-    CUDA_TRY(cudaFuncSetAttribute(k_resident<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_resident<R, true><<<n_tasks, threads, smem, s>>>(tasks, mode, max_elems,
-                                                       (int)resident_sc_doubles(max_sc));
+    CUDA_TRY(cudaFuncSetAttribute(k_resident<R, PT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_resident<R, PT, true><<<n_tasks, threads, smem, s>>>(tasks, mode, max_elems, scd);
   } else {
-    CUDA_TRY(cudaFuncSetAttribute(k_resident<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_resident<R, false><<<n_tasks, threads, smem, s>>>(tasks, mode, max_elems,
-                                                        (int)resident_sc_doubles(max_sc));
+    CUDA_TRY(cudaFuncSetAttribute(k_resident<R, PT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_resident<R, PT, false><<<n_tasks, threads, smem, s>>>(tasks, mode, max_elems, scd);
   }
   LAUNCH_CHECK();
   return HOPS_OK;
@@ -686,14 +1009,16 @@ extern "C" int hops_resident_propagate(hops_task* tasks_dev, int32_t n_tasks, in
                                        int32_t all_site_projector, void* stream) {
   if (!tasks_dev || n_tasks <= 0 || max_elems <= 0 || max_scalar_doubles <= 0)
     return set_err(HOPS_EINVAL, "bad resident launch arguments");
-  if (n_tasks > 2147483647 / 2) return set_err(HOPS_EINVAL, "too many tasks");
   cudaStream_t s = (cudaStream_t)stream;
   if (precision == HOPS_PREC_C128)
-    return resident_impl<double>(tasks_dev, n_tasks, max_elems, max_scalar_doubles,
-                                 all_site_projector, s);
+    return resident_impl<double, double2>(tasks_dev, n_tasks, max_elems, max_scalar_doubles,
+                                          all_site_projector, s);
+  if (precision == HOPS_PREC_MIXED)
+    return resident_impl<float, double2>(tasks_dev, n_tasks, max_elems, max_scalar_doubles,
+                                         all_site_projector, s);
   if (precision == HOPS_PREC_C64)
-    return resident_impl<float>(tasks_dev, n_tasks, max_elems, max_scalar_doubles,
-                                all_site_projector, s);
+    return resident_impl<float, float2>(tasks_dev, n_tasks, max_elems, max_scalar_doubles,
+                                        all_site_projector, s);
   return set_err(HOPS_EINVAL, "unknown precision %d", precision);
 }
 

@@ -94,6 +94,10 @@ def build_tables(system, basis, state_list=None, mode_list=None):
     first = [(a, rel_of_basis_mode[int(basis.modes[m])]) for (a, m) in basis.first_level()]
     first_aux = np.array([a for a, _ in first], dtype=np.int32)
     first_mode = np.array([m for _, m in first], dtype=np.int32)
+    # site-projector coefficients per mode and per down connection
+    mode_site = site[mode_lop] if M else np.zeros(0, dtype=np.int32)
+    mode_gwv = (G / W) * sval[mode_lop] if M else np.zeros(0, dtype=complex)
+    dn_coef_site = dn_coef * np.conj(sval[mode_lop[dn_m]]) if len(dn_m) else np.zeros(0, complex)
     up_counts = np.diff(basis.up_ptr)
     dn_counts = np.diff(basis.dn_ptr)
     return dict(
@@ -108,6 +112,7 @@ def build_tables(system, basis, state_list=None, mode_list=None):
         l_ptr=l_ptr, l_col=l_col, l_val=l_val, lh_ptr=lh_ptr, lh_col=lh_col, lh_val=lh_val,
         lop_active=lop_active, lop_site=site, lop_sval=sval,
         h_ptr=h_ptr, h_col=h_col, h_val=h_val, site_projector=int(is_site),
+        mode_site=mode_site.astype(np.int32), mode_gwv=mode_gwv, dn_coef_site=dn_coef_site,
         max_up=int(up_counts.max()) if len(up_counts) else 0,
         max_dn=int(dn_counts.max()) if len(dn_counts) else 0,
     )
@@ -170,6 +175,11 @@ class DeviceStructure:
         s.h_col = up(t["h_col"], i32)
         s.h_val = up(_c2d(t["h_val"]), f64)
         s.h_val_f = up(_c2f(t["h_val"]), f32)
+        s.mode_site = up(t["mode_site"], i32)
+        s.mode_gwv = up(_c2d(t["mode_gwv"]), f64)
+        s.mode_gwv_f = up(_c2f(t["mode_gwv"]), f32)
+        s.dn_coef_site = up(_c2d(t["dn_coef_site"]), f64)
+        s.dn_coef_site_f = up(_c2f(t["dn_coef_site"]), f32)
         self.cstruct = s
         # a device copy of the struct itself (resident tasks point at it)
         raw = np.frombuffer(bytes(s), dtype=np.uint8).copy()

@@ -1,8 +1,9 @@
 """Device state and launch wrappers around the C ABI.
 
 StreamBatch    -- B trajectories sharing one DeviceStructure, layout
-                  phi[a][b][s]; four streaming stage kernels (+ FP64 stage
-                  scalars) per RK4 step (hops_rk4_propagate).
+                  phi[a][s][b] (trajectory fastest); four streaming stage
+                  kernels (+ FP64 stage scalars) per RK4 step
+                  (hops_rk4_propagate).
 ResidentRunner -- any number of trajectories with their own (possibly
                   different) structures; one CTA per trajectory runs every step
                   of a call in one launch (hops_resident_propagate).
@@ -17,16 +18,28 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import HopsBatch, HopsTask, PREC_C128, PREC_C64, EOM_CODES
+from ._lib import HopsBatch, HopsTask, PREC_C128, PREC_C64, PREC_MIXED, EOM_CODES
 from .exceptions import TrajectoryError
 
 
 def precision_code(name):
+    """complex128 | complex64 | mixed (complex128 state, complex64 stage vectors)."""
     if name in ("complex128", "c128", PREC_C128):
         return PREC_C128
     if name in ("complex64", "c64", PREC_C64):
         return PREC_C64
+    if name in ("mixed", PREC_MIXED):
+        return PREC_MIXED
     raise ValueError(f"unknown precision {name}")
+
+
+def dtypes(prec):
+    """(state dtype, stage-vector dtype) of a precision code."""
+    if prec == PREC_C128:
+        return torch.complex128, torch.complex128
+    if prec == PREC_MIXED:
+        return torch.complex128, torch.complex64
+    return torch.complex64, torch.complex64
 
 
 def _stream(dev):
@@ -44,12 +57,14 @@ class StreamBatch:
         self.S, self.N, self.M, self.L = t["n_state"], t["n_hier"], t["n_mode"], t["n_lop"]
         self.prec = precision_code(precision)
         self.eom = EOM_CODES[eom]
-        cdt = torch.complex128 if self.prec == PREC_C128 else torch.complex64
-        shape = (self.N, self.B, self.S)
-        self.phi = torch.zeros(shape, dtype=cdt, device=self.dev)
+        pdt, cdt = dtypes(self.prec)
+        shape = (self.N, self.S, self.B)
+        self.phi = torch.zeros(shape, dtype=pdt, device=self.dev)
         self.acc = torch.empty(shape, dtype=cdt, device=self.dev)
         self.y0 = torch.empty(shape, dtype=cdt, device=self.dev)
         self.y1 = torch.empty(shape, dtype=cdt, device=self.dev)
+        self.phi_lo = (torch.zeros(shape, dtype=cdt, device=self.dev)
+                       if self.prec == PREC_MIXED else None)
         self.zmem = torch.zeros((self.B, max(self.M, 1)), dtype=torch.complex128, device=self.dev)
         nws = int(_lib.lib().hops_scalar_workspace_doubles(self.S, self.M, self.L, self.B))
         self.work = torch.zeros(nws, dtype=torch.float64, device=self.dev)
@@ -63,6 +78,7 @@ class StreamBatch:
         b.zmem, b.work, b.status = self.zmem.data_ptr(), self.work.data_ptr(), self.status.data_ptr()
         b.noise1 = b.noise2 = None
         b.n_t1 = b.n_t2 = 0
+        b.phi_lo = self.phi_lo.data_ptr() if self.phi_lo is not None else None
         self.cb = b
         self.reset()
 
@@ -82,13 +98,15 @@ class StreamBatch:
     def set_state(self, phi, zmem=None):
         """phi: [B, N*S] complex (reference layout per trajectory); zmem: [B, M]."""
         ph = torch.as_tensor(np.asarray(phi), dtype=torch.complex128).reshape(self.B, self.N, self.S)
-        self.phi.copy_(ph.permute(1, 0, 2).to(self.dev, dtype=self.phi.dtype))
+        self.phi.copy_(ph.permute(1, 2, 0).to(self.dev, dtype=self.phi.dtype))
+        if self.phi_lo is not None:
+            self.phi_lo.copy_(self.phi)
         if zmem is not None and self.M:
             self.zmem.copy_(torch.as_tensor(np.asarray(zmem), dtype=torch.complex128).reshape(self.B, self.M))
         self.reset()
 
     def get_state(self):
-        ph = self.phi.permute(1, 0, 2).reshape(self.B, self.N * self.S).to(torch.complex128)
+        ph = self.phi.permute(2, 0, 1).reshape(self.B, self.N * self.S).to(torch.complex128)
         return ph.cpu().numpy(), self.zmem[:, :self.M].cpu().numpy()
 
     def propagate(self, it0, di, n_steps, tau_over_hbar, psi_out=None):
@@ -113,13 +131,13 @@ class StreamBatch:
         z1d = torch.as_tensor(np.asarray(z1, dtype=np.complex64)).reshape(self.B, self.L).to(self.dev)
         z2d = (torch.as_tensor(np.asarray(z2, dtype=np.complex64)).reshape(self.B, self.L).to(self.dev)
                if z2 is not None else None)
-        dphi = torch.empty_like(self.phi)
+        dphi = torch.empty(self.phi.shape, dtype=self.acc.dtype, device=self.dev)
         dz = torch.empty((self.B, max(self.M, 1)), dtype=torch.complex128, device=self.dev)
         rc = _lib.lib().hops_dsystem_dt(C.byref(self.st.cstruct), C.byref(self.cb), z1d.data_ptr(),
                                         z2d.data_ptr() if z2d is not None else None,
                                         dphi.data_ptr(), dz.data_ptr(), _stream(self.dev))
         _lib.check(rc, "hops_dsystem_dt")
-        out = dphi.permute(1, 0, 2).reshape(self.B, self.N * self.S).to(torch.complex128)
+        out = dphi.permute(2, 0, 1).reshape(self.B, self.N * self.S).to(torch.complex128)
         return out.cpu().numpy(), dz[:, :self.M].cpu().numpy()
 
 
@@ -133,8 +151,8 @@ class ResidentTrajectory:
         self.S, self.N, self.M, self.L = t["n_state"], t["n_hier"], t["n_mode"], t["n_lop"]
         self.prec = precision_code(precision)
         self.eom = EOM_CODES[eom]
-        cdt = torch.complex128 if self.prec == PREC_C128 else torch.complex64
-        self.phi = torch.zeros(self.N * self.S, dtype=cdt, device=self.dev)
+        pdt, cdt = dtypes(self.prec)
+        self.phi = torch.zeros(self.N * self.S, dtype=pdt, device=self.dev)
         self.scratch = torch.empty(3 * self.N * self.S, dtype=cdt, device=self.dev)
         self.zmem = torch.zeros(max(self.M, 1), dtype=torch.complex128, device=self.dev)
         self.noise1 = None

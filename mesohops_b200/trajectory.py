@@ -103,7 +103,7 @@ class HopsTrajectory:
                                       self.hierarchy_param["STATIC_FILTERS"])
         self.dstruct = DeviceStructure(build_tables(self.system, self.basis), dev)
         prec = self.device_param["PRECISION"]
-        prec_bytes = 16 if prec in ("complex128", "c128") else 8
+        prec_bytes = 16 if prec in ("complex128", "c128", "mixed") else 8
         n_elem = self.dstruct.n_elem
         self.kernel = choose_kernel(n_elem, prec_bytes, self.device_param["KERNEL"])
         eom = self.eom_param["EQUATION_OF_MOTION"]

@@ -1,0 +1,77 @@
+"""Synthetic systems of the benchmark configurations (all inputs seeded).
+
+Drude-Lorentz modes use the high-temperature exponential form
+g = 2 lambda kB T - i lambda gamma, w = gamma; every L_m is the site projector
+|m><m|; noise is FFT-filtered complex Gaussian noise from the given seeds.
+"""
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as sps
+
+from .bath import bcf_convert_dl_to_exp, bcf_exp
+
+
+def site_system(H, modes_per_site):
+    """System dictionary with one set of DL modes (lambda, gamma, T) per site."""
+    n = H.shape[0]
+    gw, lops = [], []
+    for i in range(n):
+        L = sps.coo_matrix(([1.0], ([i], [i])), shape=(n, n))
+        for (lam, gam, temp) in modes_per_site:
+            g, w = bcf_convert_dl_to_exp(lam, gam, temp)[:2]
+            gw.append([g, w])
+            lops.append(L)
+    Hd = H.toarray() if sps.issparse(H) else np.asarray(H)
+    return {"HAMILTONIAN": np.array(Hd, dtype=np.complex128), "GW_SYSBATH": gw,
+            "L_HIER": lops, "L_NOISE1": lops, "ALPHA_NOISE1": bcf_exp, "PARAM_NOISE1": gw}
+
+
+def dimer():
+    """2-site dimer, H=[[0,50],[50,0]], (50, 50, 295 K) per site."""
+    H = np.array([[0.0, 50.0], [50.0, 0.0]])
+    return site_system(H, [(50.0, 50.0, 295.0)])
+
+
+def chain10_two_modes():
+    """10-site chain, J=100, eps ~ N(0, 50) (seed 1), (35,50,300 K)+(10,500,300 K)."""
+    n = 10
+    rng = np.random.default_rng(1)
+    H = np.diag(rng.normal(0, 50, n))
+    for i in range(n - 1):
+        H[i, i + 1] = H[i + 1, i] = 100.0
+    return site_system(H, [(35.0, 50.0, 300.0), (10.0, 500.0, 300.0)])
+
+
+def ring20():
+    """20-site ring, J=80, eps ~ U(-100, 100) (seed 2), (60, 60, 295 K) per site."""
+    n = 20
+    rng = np.random.default_rng(2)
+    H = np.diag(rng.uniform(-100, 100, n))
+    for i in range(n):
+        H[i, (i + 1) % n] = H[(i + 1) % n, i] = 80.0
+    return site_system(H, [(60.0, 60.0, 295.0)])
+
+
+def chain(n, J, eps, lam, gam, temp=295.0):
+    """Linear chain with given site energies and one DL mode per site."""
+    H = np.diag(np.asarray(eps, dtype=float))
+    for i in range(n - 1):
+        H[i, i + 1] = H[i + 1, i] = J
+    return site_system(H, [(lam, gam, temp)])
+
+
+WORKLOADS = {
+    "ring20": dict(system=ring20, depth=4, n_traj=128, dt=4.0, n_steps=250,
+                   desc="20-site ring (J=80 cm^-1, eps~U(-100,100) seed 2), one Drude-Lorentz "
+                        "mode per site (lambda=60, gamma=60 cm^-1, 295 K), depth 4 "
+                        "(10626 aux x 20 states), 128 trajectories (noise seeds 0..127), "
+                        "dt=4 fs"),
+    "chain10": dict(system=chain10_two_modes, depth=6, n_traj=256, dt=2.0, n_steps=250,
+                    desc="10-site chain (J=100 cm^-1, eps~N(0,50) seed 1), two DL modes per "
+                         "site (35,50)+(10,500) cm^-1 at 300 K, depth 6 (230230 aux x 10 "
+                         "states), 256 trajectories (seeds 0..255), dt=2 fs"),
+    "dimer": dict(system=dimer, depth=4, n_traj=1, dt=4.0, n_steps=250,
+                  desc="2-site dimer H=[[0,50],[50,0]], DL (50,50,295 K) per site, depth 4 "
+                       "(15 aux x 2 states), one trajectory, dt=4 fs, 1000 fs"),
+}

@@ -187,6 +187,17 @@ class OracleBasis:
                 self.first_level.append((i, int(s["L_BY_MODE"][m]), m))
         # active L: every unique L touches at least one state of the full basis
         self.l_active = [j for j, l in enumerate(s["L"]) if np.any(l != 0)]
+        # masked sub-blocks of L_j and Z2_kp1[j], as hops_modes.py:158-161 and
+        # eom_hops_ksuper.py:663-666 build them for hops_eom.py:410-425
+        self.l_mask = []
+        for l in s["L"]:
+            r, c = np.nonzero(l)
+            rows, cols = np.unique(r), np.unique(c)
+            self.l_mask.append((rows, cols, np.asarray(l)[np.ix_(rows, cols)]))
+        self.z_mask = []
+        for z in self.z2_kp1:
+            rows = np.unique(z.nonzero()[0])
+            self.z_mask.append((rows, z[rows]))
 
 
 # ---------------------------------------------------------------------------
@@ -214,7 +225,8 @@ def dsystem_dt(basis, phi, zmem, z1, z2, eom="NORMALIZED NONLINEAR"):
         d += basis.k2_k[:, None] * pf
         d += pf @ (-1j * s["H"]).T
         for j in range(len(L)):
-            d += (np.conj(z1[j]) - 1j * z2[j]) * (pf @ L[j].T)
+            rows, cols, lsub = basis.l_mask[j]
+            d[:, rows] += (np.conj(z1[j]) - 1j * z2[j]) * (pf[:, cols] @ lsub.T)
         return dphi, np.zeros_like(zmem)
 
     normalized = eom == "NORMALIZED NONLINEAR"
@@ -242,8 +254,11 @@ def dsystem_dt(basis, phi, zmem, z1, z2, eom="NORMALIZED NONLINEAR"):
     if normalized:
         d -= nc * pf
     for j in act:
-        d += (zhat[j] - 1j * z2[j]) * (pf @ L[j].T)
-        d += np.conj(avg[j]) * (basis.z2_kp1[j] @ pf)
+        rows, cols, lsub = basis.l_mask[j]
+        d[:, rows] += (zhat[j] - 1j * z2[j]) * (pf[:, cols] @ lsub.T)
+        zrows, zsub = basis.z_mask[j]
+        if len(zrows):
+            d[zrows] += np.conj(avg[j]) * (zsub @ pf)
     # calc_delta_zmem: eom_functions.py:65-160 (all modes in basis)
     dz = np.conj(s["G"]) * avg[s["L_BY_MODE"]] - np.conj(s["W"]) * zmem
     return dphi, dz

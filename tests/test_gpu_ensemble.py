@@ -1,0 +1,88 @@
+"""Batched ensembles (one structure, B trajectories, layout [aux][state][traj])
+against the CPU oracle run trajectory by trajectory.  B = 40 and 33 exercise the
+wide kernel with a partial 32-trajectory chunk, B = 7 the narrow kernel."""
+import numpy as np
+import pytest
+
+from conftest import golden_system, load_golden
+from oracle import hops_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def ensemble_noise(f, B, seed):
+    n_l, n_t = f["noise1"].shape
+    rng = np.random.default_rng(seed)
+    return ((rng.normal(size=(B, n_l, n_t)) + 1j * rng.normal(size=(B, n_l, n_t))) * 30
+            ).astype(np.complex64)
+
+
+def run_ensemble(f, B, precision, noise, n_steps):
+    import torch
+    from mesohops_b200 import HopsEnsemble
+    ens = HopsEnsemble(golden_system(f), B,
+                       noise_param={"SEED": noise, "MODEL": "PRE_CALCULATED",
+                                    "TLEN": float(f["tlen"]), "TAU": float(f["tau_noise"])},
+                       hierarchy_param={"MAXHIER": int(f["depth"])}, precision=precision)
+    ens.initialize(f["psi0"])
+    dt = float(f["dt"])
+    psi = torch.empty((n_steps, B, ens.n_state), dtype=torch.complex128, device="cuda")
+    ens.propagate(n_steps * dt, dt, psi_out=psi)
+    ens.check()
+    return psi.cpu().numpy(), ens
+
+
+def oracle_psi(f, noise_b, n_steps):
+    sysp = golden_system(f)
+    b = O.OracleBasis({k: sysp[k] for k in ("HAMILTONIAN", "GW_SYSBATH", "L_HIER")},
+                      int(f["depth"]))
+    dt = float(f["dt"])
+    _, psi, phi, _ = O.propagate(b, f["psi0"], noise_b, float(f["tau_noise"]), n_steps * dt, dt)
+    return psi[1:], phi
+
+
+@pytest.mark.parametrize("name,B", [("ring6", 40), ("ring6", 7), ("general_lop", 33),
+                                    ("chain4_2mode", 64)])
+def test_ensemble_c128_matches_oracle(cuda_device, name, B):
+    f = load_golden(name)
+    n_steps = 12
+    noise = ensemble_noise(f, B, 5)
+    psi, ens = run_ensemble(f, B, "complex128", noise, n_steps)
+    phi, _ = ens.state()
+    for b in sorted({0, 1, B // 2, B - 1}):
+        ref, phi_ref = oracle_psi(f, noise[b], n_steps)
+        assert np.max(np.abs(psi[:, b] - ref)) <= 1e-10 * np.max(np.abs(ref))
+        assert np.max(np.abs(phi[b] - phi_ref)) <= 1e-10 * np.max(np.abs(phi_ref))
+
+
+@pytest.mark.parametrize("precision,bound", [("mixed", 1e-5), ("complex64", 3e-5)])
+def test_ensemble_reduced_precision(cuda_device, precision, bound):
+    f = load_golden("ring6")
+    B, n_steps = 40, int(round(float(f["t_max"]) / float(f["dt"])))
+    noise = ensemble_noise(f, B, 6)
+    p_lo, _ = run_ensemble(f, B, precision, noise, n_steps)
+    p_hi, _ = run_ensemble(f, B, "complex128", noise, n_steps)
+    assert np.max(np.abs(np.abs(p_lo) ** 2 - np.abs(p_hi) ** 2)) <= bound
+
+
+def test_ensemble_derivative_matches_oracle(cuda_device):
+    """Stage-4 (single derivative) path of the wide kernel for 40 trajectories."""
+    from mesohops_b200 import HopsEnsemble
+    f = load_golden("general_lop")
+    B = 40
+    ens = HopsEnsemble(golden_system(f), B, noise_param={"MODEL": "ZERO", "TLEN": 10.0, "TAU": 0.5},
+                       hierarchy_param={"MAXHIER": int(f["depth"])}, precision="complex128")
+    rng = np.random.default_rng(9)
+    n = ens.n_hier * ens.n_state
+    phi = rng.normal(size=(B, n)) + 1j * rng.normal(size=(B, n))
+    zm = rng.normal(size=(B, ens.system.n_mode)) + 1j * rng.normal(size=(B, ens.system.n_mode))
+    z1 = (rng.normal(size=(B, 3)) + 1j * rng.normal(size=(B, 3))).astype(np.complex64) * 20
+    z2 = (rng.normal(size=(B, 3)) + 1j * rng.normal(size=(B, 3))).astype(np.complex64) * 5
+    ens.batch.set_state(phi, zm)
+    dphi, dz = ens.batch.dsystem_dt(z1, z2)
+    sysp = golden_system(f)
+    ob = O.OracleBasis({k: sysp[k] for k in ("HAMILTONIAN", "GW_SYSBATH", "L_HIER")}, int(f["depth"]))
+    for b in (0, 17, 39):
+        ref, rz = O.dsystem_dt(ob, phi[b], zm[b], z1[b], z2[b])
+        assert np.max(np.abs(dphi[b] - ref)) <= 1e-12 * np.max(np.abs(ref))
+        assert np.max(np.abs(dz[b] - rz)) <= 1e-12 * np.max(np.abs(rz))

@@ -67,15 +67,25 @@ def test_derivative_matches_reference(cuda_device, name):
         assert rel(dz, f["deriv_dz"]) <= 1e-12
 
 
+# Population error bounds against the FP64 reference trajectory.  The fixtures
+# drive the dynamics with white noise of amplitude ~57 cm^-1, much rougher than
+# the FFT-filtered noise of the benchmark systems.  "mixed" keeps the state in
+# complex128 and meets 1e-5; pure complex64 rounds the state every step and
+# reaches ~1.2e-5 on c1_dimer (the same value a numpy emulation of complex64
+# storage gives), so its bound here is 3e-5.
+POP_BOUND = {"mixed": 1e-5, "complex64": 3e-5}
+
+
+@pytest.mark.parametrize("precision", ["mixed", "complex64"])
 @pytest.mark.parametrize("kernel", ["resident", "streaming"])
 @pytest.mark.parametrize("name", ["c1_dimer", "ring6", "chain4_2mode", "dod"])
-def test_trajectory_c64_population_error(cuda_device, name, kernel):
+def test_trajectory_c64_population_error(cuda_device, name, kernel, precision):
     f = load_golden(name)
-    hops = make_traj(f, kernel, precision="complex64")
+    hops = make_traj(f, kernel, precision=precision)
     hops.propagate(float(f["t_max"]), float(f["dt"]))
     pop = np.abs(np.array(hops.storage["psi_traj"])) ** 2
     pop_ref = np.abs(f["psi_traj"]) ** 2
-    assert np.max(np.abs(pop - pop_ref)) <= 1e-5
+    assert np.max(np.abs(pop - pop_ref)) <= POP_BOUND[precision]
 
 
 def test_propagate_in_pieces_equals_one_call(cuda_device):
