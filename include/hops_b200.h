@@ -225,6 +225,29 @@ size_t hops_noise_filter_work_doubles(int32_t n_lop, int32_t n_t);
 int hops_kernel_timing(int enable);
 int hops_kernel_timing_read(double* total_ms, int64_t* n_launches);
 
+/*
+ * No counterpart in the reference.  hops_rk4_propagate without any device
+ * allocation, for callers that cannot call cudaMalloc when they step: hosts
+ * whose own pool owns all device memory, and per-step callbacks that must not
+ * synchronise the device.  The caller passes the state (phi in the batch
+ * layout and precision, z_mem), the noise, psi_out and one int32 status word
+ * per trajectory; the stage vectors, accumulator and scalar workspace live in a
+ * static device array of HOPS_NOALLOC_SCRATCH_BYTES that every GPU loading the
+ * library keeps until exit.  Problems needing more scratch than that
+ * (hops_noalloc_scratch_bytes) are rejected with HOPS_EINVAL.  The first call on
+ * each device looks the array up with cudaGetSymbolAddress; make it before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * (different streams or threads without ordering) race and corrupt each other.
+ */
+#define HOPS_NOALLOC_SCRATCH_BYTES (64u << 20)
+size_t hops_noalloc_scratch_bytes(const hops_structure* st, int32_t n_traj, int32_t precision);
+int hops_rk4_propagate_noalloc(const hops_structure* st, int32_t n_traj, int32_t precision,
+                               int32_t eom, void* phi_dev, double* zmem_dev,
+                               const float* noise1_dev, int32_t n_t1, const float* noise2_dev,
+                               int32_t n_t2, int32_t it0, int32_t di, int32_t n_steps,
+                               double tau_over_hbar, double* psi_out_dev, int32_t* status_dev,
+                               void* stream);
+
 #ifdef __cplusplus
 }
 #endif

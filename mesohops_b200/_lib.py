@@ -92,6 +92,10 @@ def lib():
     L.hops_noise_filter.argtypes = [_p, _p, _i, _i, _p, _p, _p, C.POINTER(C.c_int64), _p]
     L.hops_noise_filter_work_doubles.restype = C.c_size_t
     L.hops_noise_filter_work_doubles.argtypes = [_i, _i]
+    L.hops_noalloc_scratch_bytes.restype = C.c_size_t
+    L.hops_noalloc_scratch_bytes.argtypes = [C.POINTER(HopsStructure), _i, _i]
+    L.hops_rk4_propagate_noalloc.argtypes = [C.POINTER(HopsStructure), _i, _i, _i, _p, _p, _p,
+                                             _i, _p, _i, _i, _i, _i, C.c_double, _p, _p, _p]
     L.hops_kernel_timing.argtypes = [C.c_int]
     L.hops_kernel_timing_read.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_int64)]
     _lib = L
@@ -116,4 +120,5 @@ def exported_symbols():
             "hops_scalar_workspace_doubles", "hops_batch_reset", "hops_dsystem_dt",
             "hops_rk4_propagate", "hops_resident_propagate", "hops_resident_scalar_doubles",
             "hops_noise_filter", "hops_noise_filter_work_doubles", "hops_kernel_timing",
-            "hops_kernel_timing_read"]
+            "hops_kernel_timing_read", "hops_noalloc_scratch_bytes",
+            "hops_rk4_propagate_noalloc"]
