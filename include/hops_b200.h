@@ -40,7 +40,8 @@ extern "C" {
 
 #define HOPS_PREC_C128 0    /* complex128 state and arithmetic */
 #define HOPS_PREC_C64 1     /* complex64 state/SpMM, FP64 <L>, norm, z_mem */
-#define HOPS_PREC_MIXED 2   /* complex128 state; complex64 stage vectors/SpMM; FP64 scalars */
+#define HOPS_PREC_MIXED 2   /* complex128 state; complex64 storage of the stage vectors;
+                               FP64 arithmetic and scalars */
 
 #define HOPS_EOM_NORMALIZED_NONLINEAR 0
 #define HOPS_EOM_NONLINEAR 1
@@ -215,6 +216,14 @@ int hops_noise_filter(const double* alpha_dev, const float* z_dev, int32_t n_lop
 
 /* Doubles of device work area hops_noise_filter needs (work_dev). */
 size_t hops_noise_filter_work_doubles(int32_t n_lop, int32_t n_t);
+
+/*
+ * Shape of the batched stage kernel: 32*nb trajectories per warp task and
+ * chunk-major task order (1) or not (0); nb = 0 / chunk_major = -1 restore the
+ * automatic choice.  Process-wide setting used by the autotuner; has no
+ * counterpart in the reference.
+ */
+int hops_stage_tuning(int32_t nb, int32_t chunk_major);
 
 /*
  * Profiling aid: when enabled, every streaming stage-kernel launch is bracketed

@@ -96,6 +96,7 @@ def lib():
     L.hops_noalloc_scratch_bytes.argtypes = [C.POINTER(HopsStructure), _i, _i]
     L.hops_rk4_propagate_noalloc.argtypes = [C.POINTER(HopsStructure), _i, _i, _i, _p, _p, _p,
                                              _i, _p, _i, _i, _i, _i, C.c_double, _p, _p, _p]
+    L.hops_stage_tuning.argtypes = [_i, _i]
     L.hops_kernel_timing.argtypes = [C.c_int]
     L.hops_kernel_timing_read.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_int64)]
     _lib = L
@@ -121,4 +122,4 @@ def exported_symbols():
             "hops_rk4_propagate", "hops_resident_propagate", "hops_resident_scalar_doubles",
             "hops_noise_filter", "hops_noise_filter_work_doubles", "hops_kernel_timing",
             "hops_kernel_timing_read", "hops_noalloc_scratch_bytes",
-            "hops_rk4_propagate_noalloc"]
+            "hops_rk4_propagate_noalloc", "hops_stage_tuning"]

@@ -238,53 +238,72 @@ struct FastDiv {
 
 // ----------------------------------------------------------- stage update ----
 // RK4 bookkeeping of one element (integrator_rk.py:66-73).  ph: the state at
-// the start of the step (already scaled), in the state precision PT; k, acc and
-// the stage inputs in the stage precision T.  The stage inputs and the new
-// state are formed in PT arithmetic, then rounded to their storage types.
+// the start of the step (already scaled) in the state type PT; k in the
+// arithmetic type T; acc, the stage inputs and phi's complex64 copy stored in
+// the stage type ST.  Stage inputs and the new state are formed in PT
+// arithmetic and rounded once to their storage types.  GHINT (stage kernels,
+// whose buffers are always in global memory): the accumulator is touched only
+// by its owner thread, so it is loaded and stored evict-first.  The resident
+// kernel keeps acc in shared memory and must not use the global-only hints.
 // Stage 4 = plain derivative output.
-template <typename T, typename PT>
-__device__ __forceinline__ void rk_update(int stage, double h, T k, PT ph, T* acc, T* yout, PT* phi,
-                                          T* shadow, size_t e) {
+template <bool GHINT, typename ST>
+__device__ __forceinline__ ST acc_load(const ST* p) {
+  if constexpr (GHINT) return __ldcs(p);
+  else return *p;
+}
+template <bool GHINT, typename ST>
+__device__ __forceinline__ void acc_store(ST* p, ST v) {
+  if constexpr (GHINT) __stcs(p, v);
+  else *p = v;
+}
+
+template <bool GHINT, typename T, typename ST, typename PT>
+__device__ __forceinline__ void rk_update(int stage, double h, T k, PT ph, ST* acc, ST* yout,
+                                          PT* phi, ST* shadow, size_t e) {
   using RP = decltype(ph.x);
   const RP hh = (RP)h;
   switch (stage) {
     case 0: {
-      acc[e] = k;
-      yout[e] = cv<T>(cadd(ph, cscale(cv<PT>(k), hh * (RP)0.5)));
+      acc_store<GHINT>(acc + e, cv<ST>(k));
+      yout[e] = cv<ST>(cadd(ph, cscale(cv<PT>(k), hh * (RP)0.5)));
     } break;
     case 1:
     case 2: {
-      acc[e] = cadd(acc[e], cscale(k, (decltype(k.x))2));
+      const T a0 = cv<T>(acc_load<GHINT>(acc + e));
+      acc_store<GHINT>(acc + e, cv<ST>(cadd(a0, cscale(k, (decltype(k.x))2))));
       const RP c = stage == 1 ? hh * (RP)0.5 : hh;
-      yout[e] = cv<T>(cadd(ph, cscale(cv<PT>(k), c)));
+      yout[e] = cv<ST>(cadd(ph, cscale(cv<PT>(k), c)));
     } break;
     case 3: {
-      PT sum = cv<PT>(cadd(acc[e], k));
+      PT sum = cv<PT>(cadd(cv<T>(acc_load<GHINT>(acc + e)), k));
       PT hs = cscale(sum, hh);
       hs.x = hs.x / (RP)6;
       hs.y = hs.y / (RP)6;
       const PT nw = cadd(ph, hs);
       phi[e] = nw;
-      if (shadow) shadow[e] = cv<T>(nw);
+      if (shadow) shadow[e] = cv<ST>(nw);
     } break;
     default:
-      yout[e] = k;
+      yout[e] = cv<ST>(k);
   }
 }
 
 // ---------------------------------------------------- wide stage kernel ----
-// B >= 32 trajectories: one warp per (aux a, state s); lane l owns the
-// trajectories b = bg + l + 32 j, j < NB.  Connection lists, coefficients and
-// the site test are warp-uniform and loaded once per neighbour for NB x 32
-// trajectories; every Y load is a coalesced 32-trajectory segment and the NB
-// independent loads per neighbour are in flight together.
-template <typename R, typename PT, bool SITE, int NB>
+// B >= 32 trajectories: one warp per (aux a, state s, chunk of 32*NB
+// trajectories); lane l owns the trajectories bg + l + 32 j, j < NB.
+// Connection lists, coefficients and the site test are warp-uniform and loaded
+// once per neighbour for the whole chunk; every Y load is a coalesced
+// 32-trajectory segment and the NB loads per neighbour are in flight together.
+// chunk_major: the chunk is the outermost task index, so the warps in flight
+// all gather from one chunk's slice of Y, which stays resident in L2 (a slice
+// of 32 trajectories of the 20-site ring is 54 MB in complex64); otherwise each
+// warp walks every chunk of its (a, s).
+template <typename R, typename ST, typename PT, bool SITE, int NB>
 __global__ void __launch_bounds__(256) k_wide(hops_structure st, int B, int stage, double h,
-                                              const typename Prec<R>::T* __restrict__ yin,
-                                              typename Prec<R>::T* __restrict__ yout, PT* phi,
-                                              typename Prec<R>::T* shadow,
-                                              typename Prec<R>::T* acc,
-                                              const double* __restrict__ ws, FastDiv divS) {
+                                              const ST* __restrict__ yin, ST* __restrict__ yout,
+                                              PT* phi, ST* shadow, ST* acc,
+                                              const double* __restrict__ ws, FastDiv divS,
+                                              FastDiv divAS, int chunk_major) {
   using P = Prec<R>;
   using T = typename P::T;
   const int S = st.n_state;
@@ -295,17 +314,27 @@ __global__ void __launch_bounds__(256) k_wide(hops_structure st, int B, int stag
   const double* ncB = ws + bl.ncB;
   const double* scaleB = ws + bl.scaleB;
   const int lane = threadIdx.x & 31;
-  const unsigned ntask = (unsigned)st.n_hier * (unsigned)S;
+  constexpr int CH = 32 * NB;
+  const unsigned n_as = (unsigned)st.n_hier * (unsigned)S;
+  const unsigned nchunk = (unsigned)((B + CH - 1) / CH);
+  const unsigned ntask = chunk_major ? n_as * nchunk : n_as;
   const unsigned nw = (gridDim.x * blockDim.x) >> 5;
   for (unsigned t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntask; t += nw) {
-    const int a = (int)divS.div(t);
-    const int s = (int)t - a * S;
+    unsigned as = t, c0 = 0, c1 = nchunk;
+    if (chunk_major) {
+      c0 = divAS.div(t);
+      as = t - c0 * n_as;
+      c1 = c0 + 1;
+    }
+    const int a = (int)divS.div(as);
+    const int s = (int)as - a * S;
     const size_t rowa = ((size_t)a * S + s) * B;
     const T kd = P::kdec(st, a);
     const int u0 = st.up_ptr[a], u1 = st.up_ptr[a + 1];
     const int d0 = st.dn_ptr[a], d1 = st.dn_ptr[a + 1];
     const int h0 = st.h_ptr[s], h1 = st.h_ptr[s + 1];
-    for (int bg = 0; bg < B; bg += 32 * NB) {
+    for (unsigned ci = c0; ci < c1; ++ci) {
+      const int bg = (int)ci * CH;
       T k[NB];
       bool ok[NB];
 #pragma unroll
@@ -320,11 +349,10 @@ __global__ void __launch_bounds__(256) k_wide(hops_structure st, int B, int stag
           } else {
             c.x -= (R)ncB[b];
           }
-          k[j] = cmul(c, yin[rowa + b]);
+          k[j] = cmul(c, cv<T>(yin[rowa + b]));
         }
       }
       if (!SITE) {
-        // noise term sum_j cz_j (L_j Y[a])[s] for general L
         for (int jl = 0; jl < st.n_lop; ++jl) {
           const int base = jl * (S + 1);
           const int q0 = st.l_ptr[base + s], q1 = st.l_ptr[base + s + 1];
@@ -333,7 +361,8 @@ __global__ void __launch_bounds__(256) k_wide(hops_structure st, int B, int stag
             const size_t rb = ((size_t)a * S + st.l_col[q]) * B + bg + lane;
 #pragma unroll
             for (int j = 0; j < NB; ++j)
-              if (ok[j]) k[j] = cfma(cmul(czT[(size_t)jl * B + bg + lane + 32 * j], lv), yin[rb + 32 * j], k[j]);
+              if (ok[j])
+                k[j] = cfma(cmul(czT[(size_t)jl * B + bg + lane + 32 * j], lv), cv<T>(yin[rb + 32 * j]), k[j]);
           }
         }
       }
@@ -342,7 +371,7 @@ __global__ void __launch_bounds__(256) k_wide(hops_structure st, int B, int stag
         const size_t rb = ((size_t)a * S + st.h_col[q]) * B + bg + lane;
 #pragma unroll
         for (int j = 0; j < NB; ++j)
-          if (ok[j]) k[j] = cfma(hv, yin[rb + 32 * j], k[j]);
+          if (ok[j]) k[j] = cfma(hv, cv<T>(yin[rb + 32 * j]), k[j]);
       }
       for (int p = u0; p < u1; ++p) {
         const int u = st.up_aux[p], m = st.up_mode[p];
@@ -353,11 +382,11 @@ __global__ void __launch_bounds__(256) k_wide(hops_structure st, int B, int stag
           const T corr = hit ? P::gwv(st, m) : czero<T>();
 #pragma unroll
           for (int j = 0; j < NB; ++j)
-            if (ok[j]) k[j] = cfma(csub(up[32 * j], corr), yin[rb + 32 * j], k[j]);
+            if (ok[j]) k[j] = cfma(csub(up[32 * j], corr), cv<T>(yin[rb + 32 * j]), k[j]);
         } else {
 #pragma unroll
           for (int j = 0; j < NB; ++j)
-            if (ok[j]) k[j] = cfma(up[32 * j], yin[rb + 32 * j], k[j]);
+            if (ok[j]) k[j] = cfma(up[32 * j], cv<T>(yin[rb + 32 * j]), k[j]);
           const int base = st.mode_lop[m] * (S + 1);
           const int q0 = st.l_ptr[base + s], q1 = st.l_ptr[base + s + 1];
           for (int q = q0; q < q1; ++q) {
@@ -365,7 +394,7 @@ __global__ void __launch_bounds__(256) k_wide(hops_structure st, int B, int stag
             const size_t rb2 = ((size_t)u * S + st.l_col[q]) * B + bg + lane;
 #pragma unroll
             for (int j = 0; j < NB; ++j)
-              if (ok[j]) k[j] = csub(k[j], cmul(lv, yin[rb2 + 32 * j]));
+              if (ok[j]) k[j] = csub(k[j], cmul(lv, cv<T>(yin[rb2 + 32 * j])));
           }
         }
       }
@@ -377,7 +406,7 @@ __global__ void __launch_bounds__(256) k_wide(hops_structure st, int B, int stag
           const size_t rb = ((size_t)d * S + s) * B + bg + lane;
 #pragma unroll
           for (int j = 0; j < NB; ++j)
-            if (ok[j]) k[j] = cfma(cf, yin[rb + 32 * j], k[j]);
+            if (ok[j]) k[j] = cfma(cf, cv<T>(yin[rb + 32 * j]), k[j]);
         } else {
           const int base = st.mode_lop[m] * (S + 1);
           const int q0 = st.lh_ptr[base + s], q1 = st.lh_ptr[base + s + 1];
@@ -386,7 +415,7 @@ __global__ void __launch_bounds__(256) k_wide(hops_structure st, int B, int stag
             const size_t rb = ((size_t)d * S + st.lh_col[q]) * B + bg + lane;
 #pragma unroll
             for (int j = 0; j < NB; ++j)
-              if (ok[j]) k[j] = cfma(cf, yin[rb + 32 * j], k[j]);
+              if (ok[j]) k[j] = cfma(cf, cv<T>(yin[rb + 32 * j]), k[j]);
           }
         }
       }
@@ -398,8 +427,10 @@ __global__ void __launch_bounds__(256) k_wide(hops_structure st, int B, int stag
         const double sc = scaleB[b];
         T kk = k[j];
         if (stage == 0 || stage == 4) kk = cscale(kk, (R)sc);
-        const PT ph = stage == 4 ? PT{} : cscale(phi[e], (decltype(PT{}.x))sc);
-        rk_update<T, PT>(stage, h, kk, ph, acc, yout, phi, shadow, e);
+        // stages 1-3 read phi once (pure stream); stage 0 also gathers phi
+        PT ph = PT{};
+        if (stage != 4) ph = cscale(stage == 0 ? phi[e] : __ldcs(phi + e), (decltype(PT{}.x))sc);
+        rk_update<true, T, ST, PT>(stage, h, kk, ph, acc, yout, phi, shadow, e);
       }
     }
   }
@@ -408,13 +439,12 @@ __global__ void __launch_bounds__(256) k_wide(hops_structure st, int B, int stag
 // -------------------------------------------------- narrow stage kernel ----
 // B < 32 trajectories: one warp per aux a (warp-uniform connection lists),
 // lanes over the S*B elements (state s, trajectory b) of that aux.
-template <typename R, typename PT, bool SITE>
+template <typename R, typename ST, typename PT, bool SITE>
 __global__ void __launch_bounds__(256) k_narrow(hops_structure st, int B, int stage, double h,
-                                                const typename Prec<R>::T* __restrict__ yin,
-                                                typename Prec<R>::T* __restrict__ yout, PT* phi,
-                                                typename Prec<R>::T* shadow,
-                                                typename Prec<R>::T* acc,
-                                                const double* __restrict__ ws, FastDiv divB) {
+                                                const ST* __restrict__ yin,
+                                                ST* __restrict__ yout, PT* phi, ST* shadow,
+                                                ST* acc, const double* __restrict__ ws,
+                                                FastDiv divB) {
   using T = typename Prec<R>::T;
   const int S = st.n_state;
   const int SB = S * B;
@@ -426,14 +456,14 @@ __global__ void __launch_bounds__(256) k_narrow(hops_structure st, int B, int st
     for (int r = lane; r < SB; r += 32) {
       const int s = (int)divB.div((unsigned)r);
       const int b = r - s * B;
-      auto y = [&](int x, int sp) { return yin[((size_t)x * S + sp) * B + b]; };
+      auto y = [&](int x, int sp) { return cv<T>(yin[((size_t)x * S + sp) * B + b]); };
       const CoefT<R> cf{ws, bl, B, b};
       T k = deriv_elem<R, SITE>(st, a, s, y, cf);
       const size_t e = (size_t)a * SB + r;
       const double sc = scaleB[b];
       if (stage == 0 || stage == 4) k = cscale(k, (R)sc);
       const PT ph = stage == 4 ? PT{} : cscale(phi[e], (decltype(PT{}.x))sc);
-      rk_update<T, PT>(stage, h, k, ph, acc, yout, phi, shadow, e);
+      rk_update<true, T, ST, PT>(stage, h, k, ph, acc, yout, phi, shadow, e);
     }
   }
 }
@@ -471,7 +501,7 @@ __device__ void publish(const hops_structure& st, const BatchLayout& bl, double*
   }
 }
 
-template <typename R, typename PT>
+template <typename R, typename ST, typename PT>
 __global__ void __launch_bounds__(128) k_scalars(hops_structure st, hops_batch bt, int stage, int it,
                                                  double h, const void* yin, int recompute_scale,
                                                  double* psi_prev, const float* z1s,
@@ -531,7 +561,7 @@ __global__ void __launch_bounds__(128) k_scalars(hops_structure st, hops_batch b
   io.eom = bt.eom;
   io.h = h;
   io.ws = ws;
-  const T* y = static_cast<const T*>(yin);
+  const ST* y = static_cast<const ST*>(yin);
   auto get = [&](int a, int s) -> double2 {
     const size_t i = ((size_t)a * S + s) * B + b;
     return from_phi ? cscale(to_d(ph[i]), sc) : to_d(y[i]);
@@ -600,7 +630,7 @@ __global__ void k_reset(double* ws, int stride, size_t scale_off, int B, int32_t
 // between them (no grid-wide synchronisation).  Vectors live in shared memory
 // when they fit (mode 2: phi, acc, y0, y1; mode 1: y0, y1), else in the task's
 // scratch.  Tasks may carry different structures (uneven adaptive bases).
-template <typename R, typename PT, bool SITE>
+template <typename R, typename ST, typename PT, bool SITE>
 __global__ void __launch_bounds__(512, 1) k_resident(hops_task* tasks, int mode, int max_elems,
                                                      int sc_doubles) {
   using T = typename Prec<R>::T;
@@ -620,21 +650,21 @@ __global__ void __launch_bounds__(512, 1) k_resident(hops_task* tasks, int mode,
   unsigned char* vbase = smraw + (size_t)sc_doubles * sizeof(double);
   PT* gphi = static_cast<PT*>(tk->phi);
   PT* phi;
-  T *acc, *y0, *y1;
+  ST *acc, *y0, *y1;
   if (mode == 2) {
     phi = reinterpret_cast<PT*>(vbase);
-    T* v = reinterpret_cast<T*>(vbase + (size_t)max_elems * sizeof(PT));
+    ST* v = reinterpret_cast<ST*>(vbase + (size_t)max_elems * sizeof(PT));
     acc = v;
     y0 = v + max_elems;
     y1 = v + 2 * max_elems;
   } else if (mode == 1) {
-    y0 = reinterpret_cast<T*>(vbase);
+    y0 = reinterpret_cast<ST*>(vbase);
     y1 = y0 + max_elems;
     phi = gphi;
-    acc = static_cast<T*>(tk->scratch);
+    acc = static_cast<ST*>(tk->scratch);
   } else {
     phi = gphi;
-    acc = static_cast<T*>(tk->scratch);
+    acc = static_cast<ST*>(tk->scratch);
     y0 = acc + E;
     y1 = acc + 2 * E;
   }
@@ -658,8 +688,8 @@ __global__ void __launch_bounds__(512, 1) k_resident(hops_task* tasks, int mode,
   const CoefWS<R> cf{ws, lay};
   for (int n = 0; n < tk->n_steps; ++n) {
     for (int stage = 0; stage < 4; ++stage) {
-      const T* yin = stage == 1 ? y0 : (stage == 2 ? y1 : y0);
-      T* yout = stage == 0 ? y0 : (stage == 1 ? y1 : (stage == 2 ? y0 : nullptr));
+      const ST* yin = stage == 1 ? y0 : (stage == 2 ? y1 : y0);
+      ST* yout = stage == 0 ? y0 : (stage == 1 ? y1 : (stage == 2 ? y0 : nullptr));
       io.it = tk->it0 + 2 * n * tk->di + rk_noise_slot(stage) * tk->di;
       io.stage = stage;
       if (stage == 0) {
@@ -669,16 +699,16 @@ __global__ void __launch_bounds__(512, 1) k_resident(hops_task* tasks, int mode,
         for (int e = threadIdx.x; e < E; e += blockDim.x) {
           const int a = e / S, s = e - a * S;
           const T k = deriv_elem<R, SITE>(st, a, s, y, cf);
-          rk_update<T, PT>(stage, io.h, k, phi[e], acc, yout, phi, (T*)nullptr, (size_t)e);
+          rk_update<false, T, ST, PT>(stage, io.h, k, phi[e], acc, yout, phi, (ST*)nullptr, (size_t)e);
         }
       } else {
         auto get = [&](int a, int s) -> double2 { return to_d(yin[a * S + s]); };
         stage_scalars(st, io, get, red, sh);
-        auto y = [&](int x, int sp) { return yin[x * S + sp]; };
+        auto y = [&](int x, int sp) { return cv<T>(yin[x * S + sp]); };
         for (int e = threadIdx.x; e < E; e += blockDim.x) {
           const int a = e / S, s = e - a * S;
           const T k = deriv_elem<R, SITE>(st, a, s, y, cf);
-          rk_update<T, PT>(stage, io.h, k, phi[e], acc, yout, phi, (T*)nullptr, (size_t)e);
+          rk_update<false, T, ST, PT>(stage, io.h, k, phi[e], acc, yout, phi, (ST*)nullptr, (size_t)e);
         }
       }
       __syncthreads();
@@ -807,37 +837,58 @@ static int grid_for_warps(long warps) {
   return (int)blocks;
 }
 
-template <typename R, typename PT, bool SITE, int NB>
-static void launch_wide(const hops_structure* st, int B, int stage, double h, const void* yin,
-                        void* yout, void* phi, void* shadow, void* acc, const double* ws,
-                        cudaStream_t s) {
-  using T = typename Prec<R>::T;
-  const int grid = grid_for_warps((long)st->n_hier * st->n_state);
-  k_wide<R, PT, SITE, NB><<<grid, 256, 0, s>>>(*st, B, stage, h, (const T*)yin, (T*)yout,
-                                               (PT*)phi, (T*)shadow, (T*)acc, ws,
-                                               FastDiv((unsigned)st->n_state));
+// Stage-kernel shape: trajectories per chunk (32 * nb) and chunk-major order.
+// 0 = choose automatically; set by hops_stage_tuning (the autotuner).
+static int g_tune_nb = 0, g_tune_cm = -1;
+
+extern "C" int hops_stage_tuning(int32_t nb, int32_t chunk_major) {
+  if (nb != 0 && nb != 1 && nb != 2 && nb != 4 && nb != 8)
+    return set_err(HOPS_EINVAL, "nb must be 0 (auto), 1, 2, 4 or 8");
+  g_tune_nb = nb;
+  g_tune_cm = chunk_major;
+  return HOPS_OK;
 }
 
-template <typename R, typename PT, bool SITE>
+template <typename R, typename ST, typename PT, bool SITE, int NB>
+static void launch_wide(const hops_structure* st, int B, int stage, double h, const void* yin,
+                        void* yout, void* phi, void* shadow, void* acc, const double* ws,
+                        int chunk_major, cudaStream_t s) {
+  const unsigned n_as = (unsigned)st->n_hier * st->n_state;
+  const long nchunk = (B + 32 * NB - 1) / (32 * NB);
+  const int grid = grid_for_warps(chunk_major ? (long)n_as * nchunk : (long)n_as);
+  k_wide<R, ST, PT, SITE, NB><<<grid, 256, 0, s>>>(*st, B, stage, h, (const ST*)yin, (ST*)yout,
+                                                   (PT*)phi, (ST*)shadow, (ST*)acc, ws,
+                                                   FastDiv((unsigned)st->n_state), FastDiv(n_as),
+                                                   chunk_major);
+}
+
+template <typename R, typename ST, typename PT, bool SITE>
 static void launch_stage(const hops_structure* st, int B, int stage, double h, const void* yin,
                          void* yout, void* phi, void* shadow, void* acc, const double* ws,
                          cudaStream_t s) {
-  using T = typename Prec<R>::T;
   if (B >= 32) {
-    const int nb = (B + 31) / 32;
-    if (nb <= 1) launch_wide<R, PT, SITE, 1>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, s);
-    else if (nb <= 2) launch_wide<R, PT, SITE, 2>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, s);
-    else if (nb <= 4) launch_wide<R, PT, SITE, 4>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, s);
-    else launch_wide<R, PT, SITE, 8>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, s);
+    const int nbmax = (B + 31) / 32;
+    // auto (measured on the 20-site ring, 128 trajectories): 64 trajectories
+    // per warp task with FP32 arithmetic, 128 with FP64 arithmetic, natural
+    // task order; the autotuner overrides this per problem class
+    int cm = g_tune_cm >= 0 ? g_tune_cm : 0;
+    int nb = g_tune_nb;
+    if (nb == 0) nb = sizeof(typename Prec<R>::T) == 8 ? 2 : 4;
+    if (nb > nbmax) nb = nbmax >= 4 ? 4 : (nbmax >= 2 ? 2 : 1);
+    if (nb > 8) nb = 8;
+    if (nb == 1) launch_wide<R, ST, PT, SITE, 1>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, cm, s);
+    else if (nb == 2) launch_wide<R, ST, PT, SITE, 2>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, cm, s);
+    else if (nb == 4) launch_wide<R, ST, PT, SITE, 4>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, cm, s);
+    else launch_wide<R, ST, PT, SITE, 8>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, cm, s);
   } else {
     const int grid = grid_for_warps(st->n_hier);
-    k_narrow<R, PT, SITE><<<grid, 256, 0, s>>>(*st, B, stage, h, (const T*)yin, (T*)yout,
-                                               (PT*)phi, (T*)shadow, (T*)acc, ws,
-                                               FastDiv((unsigned)B));
+    k_narrow<R, ST, PT, SITE><<<grid, 256, 0, s>>>(*st, B, stage, h, (const ST*)yin, (ST*)yout,
+                                                   (PT*)phi, (ST*)shadow, (ST*)acc, ws,
+                                                   FastDiv((unsigned)B));
   }
 }
 
-template <typename R, typename PT>
+template <typename R, typename ST, typename PT>
 static int run_stage(const hops_structure* st, int B, int stage, double h, const void* yin,
                      void* yout, void* phi, void* shadow, void* acc, const double* ws,
                      cudaStream_t s) {
@@ -848,9 +899,9 @@ static int run_stage(const hops_structure* st, int B, int stage, double h, const
     if (e0) cudaEventRecord(e0, s);
   }
   if (st->site_projector)
-    launch_stage<R, PT, true>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, s);
+    launch_stage<R, ST, PT, true>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, s);
   else
-    launch_stage<R, PT, false>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, s);
+    launch_stage<R, ST, PT, false>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, s);
   LAUNCH_CHECK();
   if (g_timing && e1) cudaEventRecord(e1, s);
   return HOPS_OK;
@@ -860,10 +911,9 @@ static size_t scalar_smem(const hops_structure* st) {
   return (size_t)(32 + 4 * st->n_lop + 2) * sizeof(double);
 }
 
-template <typename R, typename PT>
+template <typename R, typename ST, typename PT>
 static int propagate_impl(const hops_structure* st, hops_batch* bt, int32_t it0, int32_t di,
                           int32_t n_steps, double h, double* psi_out, cudaStream_t s) {
-  using T = typename Prec<R>::T;
   const int B = bt->n_traj, S = st->n_state;
   const size_t smem = scalar_smem(st);
   const bool normalized = bt->eom == HOPS_EOM_NORMALIZED_NONLINEAR;
@@ -873,16 +923,16 @@ static int propagate_impl(const hops_structure* st, hops_batch* bt, int32_t it0,
     for (int i = 0; i < 4; ++i) {
       const int slot = i == 0 ? 0 : (i == 3 ? 2 : 1);
       const int it = it0 + 2 * n * di + slot * di;
-      // stage 0 gathers from the state (or its complex64 shadow in mixed mode)
+      // stage 0 gathers from the state (or its complex64 copy in mixed mode)
       const void* yin = i == 0 ? (shadow ? shadow : bt->phi)
                                : (i == 1 ? bt->y0 : (i == 2 ? bt->y1 : bt->y0));
       void* yout = i == 0 ? bt->y0 : (i == 1 ? bt->y1 : (i == 2 ? bt->y0 : nullptr));
       const int recompute = (i == 0 && n > 0 && normalized) ? 1 : 0;
       double* psi_prev = (i == 0 && n > 0 && psi_out) ? psi_out + (size_t)(n - 1) * psi_stride : nullptr;
-      k_scalars<R, PT><<<B, 128, smem, s>>>(*st, *bt, i, it, h, yin, recompute, psi_prev, nullptr,
-                                            nullptr, nullptr);
+      k_scalars<R, ST, PT><<<B, 128, smem, s>>>(*st, *bt, i, it, h, yin, recompute, psi_prev,
+                                                nullptr, nullptr, nullptr);
       LAUNCH_CHECK();
-      int rc = run_stage<R, PT>(st, B, i, h, yin, yout, bt->phi, shadow, bt->acc, bt->work, s);
+      int rc = run_stage<R, ST, PT>(st, B, i, h, yin, yout, bt->phi, shadow, bt->acc, bt->work, s);
       if (rc) return rc;
     }
   }
@@ -896,8 +946,8 @@ static int propagate_impl(const hops_structure* st, hops_batch* bt, int32_t it0,
       if (blocks > (long)sm_count() * 8) blocks = (long)sm_count() * 8;
       const ScalarLayout lay(S, st->n_mode, st->n_lop);
       const BatchLayout bl(S, st->n_mode, st->n_lop, B);
-      k_apply_scale<PT, T><<<(int)blocks, 256, 0, s>>>((PT*)bt->phi, (T*)shadow, B, E,
-                                                        bt->work + bl.scaleB);
+      k_apply_scale<PT, ST><<<(int)blocks, 256, 0, s>>>((PT*)bt->phi, (ST*)shadow, B, E,
+                                                         bt->work + bl.scaleB);
       LAUNCH_CHECK();
       k_reset<<<(B + 127) / 128, 128, 0, s>>>(bt->work, lay.stride, bl.scaleB, B, nullptr, 0);
       LAUNCH_CHECK();
@@ -933,21 +983,22 @@ extern "C" int hops_rk4_propagate(const hops_structure* st, hops_batch* bt, int3
   if (scalar_smem(st) > 48 * 1024) return set_err(HOPS_ENOTSUP, "too many L operators (%d)", st->n_lop);
   cudaStream_t s = (cudaStream_t)stream;
   if (bt->precision == HOPS_PREC_C128)
-    return propagate_impl<double, double2>(st, bt, it0, di, n_steps, tau_over_hbar, psi_out_dev, s);
+    return propagate_impl<double, double2, double2>(st, bt, it0, di, n_steps, tau_over_hbar, psi_out_dev, s);
   if (bt->precision == HOPS_PREC_MIXED)
-    return propagate_impl<float, double2>(st, bt, it0, di, n_steps, tau_over_hbar, psi_out_dev, s);
-  return propagate_impl<float, float2>(st, bt, it0, di, n_steps, tau_over_hbar, psi_out_dev, s);
+    return propagate_impl<double, float2, double2>(st, bt, it0, di, n_steps, tau_over_hbar, psi_out_dev, s);
+  return propagate_impl<float, float2, float2>(st, bt, it0, di, n_steps, tau_over_hbar, psi_out_dev, s);
 }
 
-template <typename R, typename PT>
+template <typename R, typename ST, typename PT>
 static int dsys_impl(const hops_structure* st, hops_batch* bt, const float* z1, const float* z2,
                      void* dphi, double* dz, cudaStream_t s) {
-  k_scalars<R, PT><<<bt->n_traj, 128, scalar_smem(st), s>>>(*st, *bt, 4, 0, 0.0, bt->phi, 0, nullptr,
-                                                            z1, z2, dz);
+  k_scalars<R, ST, PT><<<bt->n_traj, 128, scalar_smem(st), s>>>(*st, *bt, 4, 0, 0.0, bt->phi, 0,
+                                                                nullptr, z1, z2, dz);
   LAUNCH_CHECK();
-  // stage 4 reads the state itself (mixed mode: its complex64 shadow)
+  // stage 4 reads the state itself (mixed mode: its complex64 copy)
   const void* yin = bt->precision == HOPS_PREC_MIXED ? bt->phi_lo : bt->phi;
-  return run_stage<R, PT>(st, bt->n_traj, 4, 0.0, yin, dphi, bt->phi, nullptr, bt->acc, bt->work, s);
+  return run_stage<R, ST, PT>(st, bt->n_traj, 4, 0.0, yin, dphi, bt->phi, nullptr, bt->acc,
+                              bt->work, s);
 }
 
 extern "C" int hops_dsystem_dt(const hops_structure* st, hops_batch* bt, const float* z1_dev,
@@ -960,18 +1011,18 @@ extern "C" int hops_dsystem_dt(const hops_structure* st, hops_batch* bt, const f
   if (scalar_smem(st) > 48 * 1024) return set_err(HOPS_ENOTSUP, "too many L operators (%d)", st->n_lop);
   cudaStream_t s = (cudaStream_t)stream;
   if (bt->precision == HOPS_PREC_C128)
-    return dsys_impl<double, double2>(st, bt, z1_dev, z2_dev, dphi_dev, dzmem_dev, s);
+    return dsys_impl<double, double2, double2>(st, bt, z1_dev, z2_dev, dphi_dev, dzmem_dev, s);
   if (bt->precision == HOPS_PREC_MIXED)
-    return dsys_impl<float, double2>(st, bt, z1_dev, z2_dev, dphi_dev, dzmem_dev, s);
-  return dsys_impl<float, float2>(st, bt, z1_dev, z2_dev, dphi_dev, dzmem_dev, s);
+    return dsys_impl<double, float2, double2>(st, bt, z1_dev, z2_dev, dphi_dev, dzmem_dev, s);
+  return dsys_impl<float, float2, float2>(st, bt, z1_dev, z2_dev, dphi_dev, dzmem_dev, s);
 }
 
 static size_t resident_sc_doubles(int max_sc) { return (size_t)((max_sc + 1) & ~1); }
 
-template <typename R, typename PT>
+template <typename R, typename ST, typename PT>
 static int resident_impl(hops_task* tasks, int n_tasks, int max_elems, int max_sc, int site,
                          cudaStream_t s) {
-  using T = typename Prec<R>::T;
+  using T = ST;
   int dev = 0, optin = 0;
   CUDA_TRY(cudaGetDevice(&dev));
   CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -995,11 +1046,11 @@ static int resident_impl(hops_task* tasks, int n_tasks, int max_elems, int max_s
   if (threads > 512) threads = 512;
   const int scd = (int)resident_sc_doubles(max_sc);
   if (site) {
-    CUDA_TRY(cudaFuncSetAttribute(k_resident<R, PT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_resident<R, PT, true><<<n_tasks, threads, smem, s>>>(tasks, mode, max_elems, scd);
+    CUDA_TRY(cudaFuncSetAttribute(k_resident<R, ST, PT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_resident<R, ST, PT, true><<<n_tasks, threads, smem, s>>>(tasks, mode, max_elems, scd);
   } else {
-    CUDA_TRY(cudaFuncSetAttribute(k_resident<R, PT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_resident<R, PT, false><<<n_tasks, threads, smem, s>>>(tasks, mode, max_elems, scd);
+    CUDA_TRY(cudaFuncSetAttribute(k_resident<R, ST, PT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_resident<R, ST, PT, false><<<n_tasks, threads, smem, s>>>(tasks, mode, max_elems, scd);
   }
   LAUNCH_CHECK();
   return HOPS_OK;
@@ -1012,14 +1063,14 @@ extern "C" int hops_resident_propagate(hops_task* tasks_dev, int32_t n_tasks, in
     return set_err(HOPS_EINVAL, "bad resident launch arguments");
   cudaStream_t s = (cudaStream_t)stream;
   if (precision == HOPS_PREC_C128)
-    return resident_impl<double, double2>(tasks_dev, n_tasks, max_elems, max_scalar_doubles,
-                                          all_site_projector, s);
+    return resident_impl<double, double2, double2>(tasks_dev, n_tasks, max_elems,
+                                                   max_scalar_doubles, all_site_projector, s);
   if (precision == HOPS_PREC_MIXED)
-    return resident_impl<float, double2>(tasks_dev, n_tasks, max_elems, max_scalar_doubles,
-                                         all_site_projector, s);
+    return resident_impl<double, float2, double2>(tasks_dev, n_tasks, max_elems,
+                                                  max_scalar_doubles, all_site_projector, s);
   if (precision == HOPS_PREC_C64)
-    return resident_impl<float, float2>(tasks_dev, n_tasks, max_elems, max_scalar_doubles,
-                                        all_site_projector, s);
+    return resident_impl<float, float2, float2>(tasks_dev, n_tasks, max_elems,
+                                                max_scalar_doubles, all_site_projector, s);
   return set_err(HOPS_EINVAL, "unknown precision %d", precision);
 }
 

@@ -46,6 +46,11 @@ def _stream(dev):
     return torch.cuda.current_stream(dev).cuda_stream
 
 
+# Autotuned stage-kernel shapes per problem class:
+# (n_hier, n_state, n_mode, B, precision, site projector) -> (nb, chunk_major)
+_TUNE_CACHE = {}
+
+
 class StreamBatch:
     """B trajectories sharing one structure, propagated by the streaming kernels."""
 
@@ -109,9 +114,60 @@ class StreamBatch:
         ph = self.phi.permute(2, 0, 1).reshape(self.B, self.N * self.S).to(torch.complex128)
         return ph.cpu().numpy(), self.zmem[:, :self.M].cpu().numpy()
 
-    def propagate(self, it0, di, n_steps, tau_over_hbar, psi_out=None):
+    def tune_key(self):
+        return (self.N, self.S, self.M, self.B, self.prec, self.st.tables["site_projector"])
+
+    def autotune(self, it0, di, tau_over_hbar, steps=2):
+        """Pick the stage-kernel shape (trajectories per warp task, task order).
+
+        Times every candidate for `steps` RK4 steps on the current state, then
+        restores the state; the winner is cached per problem class.  Batches of
+        fewer than 32 trajectories use the narrow kernel and need no tuning.
+        """
+        self.tuning = None
+        if self.B < 32:
+            return None
+        # timing only: run from noise index 0 and stay inside the noise axis
+        it0 = 0
+        n_t = min([x for x in (self.cb.n_t1, self.cb.n_t2) if x > 0] or [1 << 30])
+        if 2 * (steps + 1) * di >= n_t:
+            return None
+        key = self.tune_key()
+        if key in _TUNE_CACHE:
+            self.tuning = _TUNE_CACHE[key]
+            return self.tuning
+        L = _lib.lib()
+        saved = [t.clone() for t in (self.phi, self.zmem, self.work, self.status)]
+        if self.phi_lo is not None:
+            saved.append(self.phi_lo.clone())
+        nbmax = (self.B + 31) // 32
+        cands = [(nb, cm) for nb in (1, 2, 4, 8) if nb == 1 or nb <= 2 * nbmax for cm in (0, 1)]
+        best, best_ms = None, float("inf")
+        for nb, cm in cands:
+            L.hops_stage_tuning(nb, cm)
+            self.propagate(it0, di, 1, tau_over_hbar, tuned=False)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            self.propagate(it0, di, steps, tau_over_hbar, tuned=False)
+            e1.record()
+            torch.cuda.synchronize(self.dev)
+            ms = e0.elapsed_time(e1)
+            if ms < best_ms:
+                best, best_ms = (nb, cm), ms
+            for dst, src in zip((self.phi, self.zmem, self.work, self.status, self.phi_lo), saved):
+                dst.copy_(src)
+        L.hops_stage_tuning(0, -1)
+        _TUNE_CACHE[key] = best
+        self.tuning = best
+        return best
+
+    def propagate(self, it0, di, n_steps, tau_over_hbar, psi_out=None, tuned=True):
         """n_steps RK4 steps; psi_out: optional device tensor [n_steps, B, S] complex128."""
         L = _lib.lib()
+        if tuned:
+            nb, cm = getattr(self, "tuning", None) or (0, -1)
+            L.hops_stage_tuning(nb, cm)
         ptr = psi_out.data_ptr() if psi_out is not None else None
         rc = L.hops_rk4_propagate(C.byref(self.st.cstruct), C.byref(self.cb), int(it0), int(di),
                                   int(n_steps), float(tau_over_hbar), ptr, _stream(self.dev))

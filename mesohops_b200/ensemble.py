@@ -2,7 +2,7 @@
 
 Every trajectory has its own noise (seeds SEEDS[b] or precomputed arrays) and
 its own state; the structure tables are uploaded once and every stage kernel
-streams all B trajectories through each connection list (layout phi[a][b][s]).
+streams all B trajectories through each connection list (layout phi[a][s][b]).
 This is the batched form of running HopsTrajectory B times (the reference runs
 trajectories as independent processes, README.md:26-27).
 """
@@ -31,7 +31,7 @@ class HopsEnsemble:
     """
 
     def __init__(self, system_param, n_traj, eom_param=None, noise_param=None,
-                 hierarchy_param=None, precision="complex64", device="cuda:0"):
+                 hierarchy_param=None, precision="mixed", device="cuda:0", autotune=True):
         self.system = HopsSystem(system_param)
         self.eom_param = initialize_dict(eom_param or {}, EOM_DICT_DEFAULT, EOM_DICT_TYPES, "HopsEOM")
         self.hierarchy_param = initialize_dict(hierarchy_param or {}, HIERARCHY_DICT_DEFAULT,
@@ -51,6 +51,8 @@ class HopsEnsemble:
                                  self.eom_param["EQUATION_OF_MOTION"])
         self.t = 0.0
         self.noise = None
+        self.autotune = autotune
+        self._tuned = False
 
     @property
     def n_hier(self):
@@ -116,6 +118,9 @@ class HopsEnsemble:
     def propagate(self, t_advance, tau, psi_out=None):
         """Propagate all trajectories; psi_out: optional device tensor [n, B, S] c128."""
         n, it0, di = self.steps_for(t_advance, tau)
+        if self.autotune and not self._tuned:
+            self.batch.autotune(it0, di, tau / hbar)
+            self._tuned = True
         self.batch.propagate(it0, di, n, tau / hbar, psi_out=psi_out)
         self.t += n * tau
         return n
