@@ -152,6 +152,23 @@ typedef struct hops_task {
   double scale;     /* pending normalisation factor of phi (1 = none) */
 } hops_task;
 
+/* One trajectory of hops_flux_errors (array in device memory). */
+typedef struct hops_flux_task {
+  const hops_structure* st; /* device pointer to the structure of the current basis */
+  const double* phi;        /* [n_hier][n_state] complex128, normalised */
+  const double* zmem;       /* [n_mode] complex128 noise memory */
+  const float* z1;          /* [n_lop] complex64 noise 1 at the current time */
+  const float* z2;          /* [n_lop] complex64 noise 2 or NULL */
+  const int32_t* aux_mask;  /* [n_hier] 1 = keep, 0 = zero before the derivative; or NULL */
+  double* e_deriv;          /* out [n_hier][n_state] */
+  double* e_up;             /* out [n_mode][n_hier], or NULL to skip e_up/e_down */
+  double* e_down;           /* out [n_mode][n_hier] */
+  const uint8_t* k_aux;     /* [n_mode][n_hier] depth of each aux in each mode */
+  double dt;                /* time step of the error estimate [fs] */
+  int32_t eom;
+  int32_t pad;
+} hops_flux_task;
+
 const char* hops_last_error(void);
 int hops_version(void);
 int hops_device_query(int device, int* sm_count, int* smem_optin_bytes);
@@ -195,6 +212,16 @@ int hops_rk4_propagate(const hops_structure* st, hops_batch* bt, int32_t it0,
 int hops_resident_propagate(hops_task* tasks_dev, int32_t n_tasks, int32_t max_elems,
                             int32_t max_scalar_doubles, int32_t precision,
                             int32_t all_site_projector, void* stream);
+
+/*
+ * Adaptive-basis error estimates, one CTA per task, FP64 (replaces the array
+ * parts of basis/basis_functions_adaptive.py: error_deriv :10-74,
+ * error_flux_up_hier_stable :165-266, error_flux_down_hier_stable :517-624).
+ * max_smem_doubles: largest hops_flux_errors_smem_doubles() of any task.
+ */
+int hops_flux_errors(hops_flux_task* tasks_dev, int32_t n_tasks, int32_t max_smem_doubles,
+                     double hbar, void* stream);
+int32_t hops_flux_errors_smem_doubles(int32_t n_state, int32_t n_mode, int32_t n_lop);
 
 /* Shared-memory doubles of per-stage scalars one resident task needs. */
 int32_t hops_resident_scalar_doubles(int32_t n_state, int32_t n_mode, int32_t n_lop);

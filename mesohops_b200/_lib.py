@@ -63,6 +63,15 @@ class HopsTask(C.Structure):
     ]
 
 
+class HopsFluxTask(C.Structure):
+    """Mirror of ``hops_flux_task``."""
+    _fields_ = [
+        ("st", _p), ("phi", _p), ("zmem", _p), ("z1", _p), ("z2", _p), ("aux_mask", _p),
+        ("e_deriv", _p), ("e_up", _p), ("e_down", _p), ("k_aux", _p), ("dt", C.c_double),
+        ("eom", _i), ("pad", _i),
+    ]
+
+
 _lib = None
 
 
@@ -97,6 +106,9 @@ def lib():
     L.hops_rk4_propagate_noalloc.argtypes = [C.POINTER(HopsStructure), _i, _i, _i, _p, _p, _p,
                                              _i, _p, _i, _i, _i, _i, C.c_double, _p, _p, _p]
     L.hops_stage_tuning.argtypes = [_i, _i]
+    L.hops_flux_errors.argtypes = [_p, _i, _i, C.c_double, _p]
+    L.hops_flux_errors_smem_doubles.restype = _i
+    L.hops_flux_errors_smem_doubles.argtypes = [_i, _i, _i]
     L.hops_kernel_timing.argtypes = [C.c_int]
     L.hops_kernel_timing_read.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_int64)]
     _lib = L
@@ -122,4 +134,5 @@ def exported_symbols():
             "hops_rk4_propagate", "hops_resident_propagate", "hops_resident_scalar_doubles",
             "hops_noise_filter", "hops_noise_filter_work_doubles", "hops_kernel_timing",
             "hops_kernel_timing_read", "hops_noalloc_scratch_bytes",
-            "hops_rk4_propagate_noalloc", "hops_stage_tuning"]
+            "hops_rk4_propagate_noalloc", "hops_stage_tuning", "hops_flux_errors",
+            "hops_flux_errors_smem_doubles"]

@@ -373,7 +373,37 @@ __global__ void __launch_bounds__(256) k_wide(hops_structure st, int B, int stag
         for (int j = 0; j < NB; ++j)
           if (ok[j]) k[j] = cfma(hv, cv<T>(yin[rb + 32 * j]), k[j]);
       }
-      for (int p = u0; p < u1; ++p) {
+      int p0 = u0;
+      if (SITE) {
+        // two neighbours per iteration: their 2 x NB row segments are loaded
+        // before either is consumed, so twice as many loads are in flight
+        for (; p0 + 2 <= u1; p0 += 2) {
+          const int ua = __ldg(st.up_aux + p0), ma = __ldg(st.up_mode + p0);
+          const int ub = __ldg(st.up_aux + p0 + 1), mb = __ldg(st.up_mode + p0 + 1);
+          const size_t ra = ((size_t)ua * S + s) * B + bg + lane;
+          const size_t rb = ((size_t)ub * S + s) * B + bg + lane;
+          ST ya[NB], yb[NB];
+#pragma unroll
+          for (int j = 0; j < NB; ++j) {
+            if (ok[j]) {
+              ya[j] = yin[ra + 32 * j];
+              yb[j] = yin[rb + 32 * j];
+            }
+          }
+          const T* upa = upcT + (size_t)ma * B + bg + lane;
+          const T* upb = upcT + (size_t)mb * B + bg + lane;
+          const T corra = __ldg(st.mode_site + ma) == s ? P::gwv(st, ma) : czero<T>();
+          const T corrb = __ldg(st.mode_site + mb) == s ? P::gwv(st, mb) : czero<T>();
+#pragma unroll
+          for (int j = 0; j < NB; ++j) {
+            if (ok[j]) {
+              k[j] = cfma(csub(upa[32 * j], corra), cv<T>(ya[j]), k[j]);
+              k[j] = cfma(csub(upb[32 * j], corrb), cv<T>(yb[j]), k[j]);
+            }
+          }
+        }
+      }
+      for (int p = p0; p < u1; ++p) {
         const int u = st.up_aux[p], m = st.up_mode[p];
         const size_t rb = ((size_t)u * S + s) * B + bg + lane;
         const T* up = upcT + (size_t)m * B + bg + lane;
@@ -1077,6 +1107,132 @@ extern "C" int hops_resident_propagate(hops_task* tasks_dev, int32_t n_tasks, in
 extern "C" int32_t hops_resident_scalar_doubles(int32_t n_state, int32_t n_mode, int32_t n_lop) {
   const ScalarLayout lay(n_state, n_mode, n_lop);
   return lay.stride + 2 * n_mode + 4 * n_lop + 2;
+}
+
+// ================================================== adaptive flux errors ====
+// Error estimates of the adaptive basis update for a list of trajectories, one
+// CTA each (basis/basis_functions_adaptive.py):
+//   e_deriv[a*S+s] = |dPhi/dt / hbar + Phi / dt|^2           (error_deriv, :10-74)
+//                    with Phi zeroed on aux whose mask entry is 0 (stable-aux
+//                    variant used for the state basis) and e_deriv = 0 there
+//   e_up[m*N+a]    = |w_m|^2 (1 + k_m(a))^2 sum_s |L_m[s,s]|^2 |Phi[s,a]|^2 / hbar^2
+//                                                             (error_flux_up_hier_stable, :165-266)
+//   e_down[m*N+a]  = |g_m/w_m|^2 sum_s |L_m[s,s] - <L_m>|^2 |Phi[s,a]|^2 / hbar^2
+//                                                             (error_flux_down_hier_stable, :517-624)
+// <L_m> is the expectation in the unmasked psi_0 (hops_basis.py:1105-1112);
+// for modes whose L has no diagonal entry at s the diagonal is 0.  All FP64.
+__global__ void __launch_bounds__(256) k_flux_errors(hops_flux_task* tasks, double hbar) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ hops_structure st;
+  __shared__ double red[32];
+  hops_flux_task* tk = tasks + blockIdx.x;
+  if (threadIdx.x == 0) st = *tk->st;
+  __syncthreads();
+  const int S = st.n_state, M = st.n_mode, L = st.n_lop, N = st.n_hier;
+  const int E = N * S;
+  const ScalarLayout lay(S, M, L);
+  double* ws = reinterpret_cast<double*>(smraw);
+  double* sh = ws + lay.stride;                 // 4L + 2 doubles
+  double* zdummy = sh + 4 * L + 2;              // 2M doubles (dz of the single derivative)
+  const double2* phi = reinterpret_cast<const double2*>(tk->phi);
+  const int32_t* mask = tk->aux_mask;
+  // <L> of the unmasked psi_0 for e_down (hops_basis.py psi setter)
+  double2* avg_full = reinterpret_cast<double2*>(zdummy + 2 * M);  // L doubles2
+  {
+    double p = 0.0;
+    for (int s = threadIdx.x; s < S; s += blockDim.x) {
+      const double2 v = phi[s];
+      p += v.x * v.x + v.y * v.y;
+    }
+    const double n2 = block_sum(p, red);
+    for (int j = threadIdx.x; j < L; j += blockDim.x) {
+      double2 num = mk(0.0, 0.0);
+      const int base = j * (S + 1);
+      for (int r = 0; r < S; ++r) {
+        const int q0 = st.l_ptr[base + r], q1 = st.l_ptr[base + r + 1];
+        if (q0 == q1) continue;
+        double2 row = mk(0.0, 0.0);
+        for (int q = q0; q < q1; ++q) row = cfma(ld2(st.l_val, q), phi[st.l_col[q]], row);
+        num = cadd(num, cconjmul(phi[r], row));
+      }
+      avg_full[j] = mk(num.x / n2, num.y / n2);
+    }
+  }
+  StageIO io;
+  io.zmem = tk->zmem;
+  io.noise1 = reinterpret_cast<const float2*>(tk->z1);
+  io.noise2 = reinterpret_cast<const float2*>(tk->z2);
+  io.n_t1 = 1;
+  io.n_t2 = 1;
+  io.it = 0;
+  io.stage = 4;
+  io.eom = tk->eom;
+  io.h = 0.0;
+  io.ws = ws;
+  io.zmem_out = zdummy;
+  auto get = [&](int a, int s) -> double2 {
+    return (mask && !mask[a]) ? mk(0.0, 0.0) : phi[a * S + s];
+  };
+  stage_scalars(st, io, get, red, sh);
+  const CoefWS<double> cf{ws, lay};
+  auto y = [&](int x, int sp) -> double2 { return (mask && !mask[x]) ? mk(0.0, 0.0) : phi[x * S + sp]; };
+  const double inv_dt = 1.0 / tk->dt, inv_h = 1.0 / hbar;
+  for (int e = threadIdx.x; e < E; e += blockDim.x) {
+    const int a = e / S, s = e - a * S;
+    double val = 0.0;
+    if (!mask || mask[a]) {
+      const double2 k = st.site_projector ? deriv_elem<double, true>(st, a, s, y, cf)
+                                          : deriv_elem<double, false>(st, a, s, y, cf);
+      const double2 ph = phi[e];
+      const double re = k.x * inv_h + ph.x * inv_dt, im = k.y * inv_h + ph.y * inv_dt;
+      val = re * re + im * im;
+    }
+    tk->e_deriv[e] = val;
+  }
+  if (tk->e_up) {
+    const double ih2 = inv_h * inv_h;
+    for (int i = threadIdx.x; i < M * N; i += blockDim.x) {
+      const int m = i / N, a = i - m * N;
+      const int j = st.mode_lop[m];
+      const int base = j * (S + 1);
+      const double2 w = ld2(st.mode_w, m), gw = ld2(st.mode_gw, m);
+      const double w2 = w.x * w.x + w.y * w.y, gw2 = gw.x * gw.x + gw.y * gw.y;
+      // k_m(a): depth of aux a in mode m (K2_aux_by_mode, hops_basis.py:1128-1140)
+      const int km = tk->k_aux[i];
+      const double2 al = avg_full[j];
+      double sup = 0.0, sdn = 0.0;
+      for (int s = 0; s < S; ++s) {
+        double2 d = mk(0.0, 0.0);
+        for (int q = st.l_ptr[base + s]; q < st.l_ptr[base + s + 1]; ++q)
+          if (st.l_col[q] == s) d = ld2(st.l_val, q);
+        const double2 v = phi[a * S + s];
+        const double p2 = v.x * v.x + v.y * v.y;
+        sup += (d.x * d.x + d.y * d.y) * p2;
+        const double2 dd = csub(d, al);
+        sdn += (dd.x * dd.x + dd.y * dd.y) * p2;
+      }
+      const double f = 1.0 + km;
+      tk->e_up[i] = w2 * f * f * sup * ih2;
+      tk->e_down[i] = gw2 * sdn * ih2;
+    }
+  }
+}
+
+extern "C" int32_t hops_flux_errors_smem_doubles(int32_t n_state, int32_t n_mode, int32_t n_lop) {
+  const ScalarLayout lay(n_state, n_mode, n_lop);
+  return lay.stride + 4 * n_lop + 2 + 2 * n_mode + 2 * n_lop + 2;
+}
+
+extern "C" int hops_flux_errors(hops_flux_task* tasks_dev, int32_t n_tasks, int32_t max_smem_doubles,
+                                double hbar, void* stream) {
+  if (!tasks_dev || n_tasks <= 0 || max_smem_doubles <= 0)
+    return set_err(HOPS_EINVAL, "bad flux-error launch arguments");
+  const size_t smem = (size_t)max_smem_doubles * sizeof(double);
+  if (smem > 200 * 1024) return set_err(HOPS_ENOTSUP, "flux-error scalar block too large");
+  CUDA_TRY(cudaFuncSetAttribute(k_flux_errors, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_flux_errors<<<n_tasks, 256, smem, (cudaStream_t)stream>>>(tasks_dev, hbar);
+  LAUNCH_CHECK();
+  return HOPS_OK;
 }
 
 // ======================================================= no-allocation path ==

@@ -11,6 +11,8 @@ The arrays encode the super-operators of eom/eom_hops_ksuper.py:36-230:
 """
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 import torch
 
@@ -119,23 +121,57 @@ def build_tables(system, basis, state_list=None, mode_list=None):
 
 
 class DeviceStructure:
-    """hops_structure with its arrays resident on one CUDA device."""
+    """hops_structure with its arrays resident on one CUDA device.
+
+    Every table and a device copy of the struct itself live in one packed
+    buffer uploaded with a single host->device copy (cheap enough to rebuild
+    at every adaptive basis change).
+    """
+
+    _ALIGN = 256
 
     def __init__(self, tables, device):
         self.tables = tables
         self.device = torch.device(device)
-        self._keep = []
         t = tables
-
-        def up(arr, dtype):
+        c2d, c2f = _c2d, _c2f
+        i32 = np.int32
+        fields = [
+            ("k_decay", c2d(t["k_decay"])), ("k_decay_f", c2f(t["k_decay"])),
+            ("up_ptr", t["up_ptr"].astype(i32)), ("up_aux", t["up_aux"].astype(i32)),
+            ("up_mode", t["up_mode"].astype(i32)),
+            ("dn_ptr", t["dn_ptr"].astype(i32)), ("dn_aux", t["dn_aux"].astype(i32)),
+            ("dn_mode", t["dn_mode"].astype(i32)),
+            ("dn_coef", c2d(t["dn_coef"])), ("dn_coef_f", c2f(t["dn_coef"])),
+            ("mode_lop", t["mode_lop"].astype(i32)), ("mode_g", c2d(t["mode_g"])),
+            ("mode_w", c2d(t["mode_w"])), ("mode_gw", c2d(t["mode_gw"])),
+            ("mode_gw_f", c2f(t["mode_gw"])),
+            ("first_aux", t["first_aux"].astype(i32)), ("first_mode", t["first_mode"].astype(i32)),
+            ("l_ptr", t["l_ptr"].astype(i32)), ("l_col", t["l_col"].astype(i32)),
+            ("l_val", c2d(t["l_val"])), ("l_val_f", c2f(t["l_val"])),
+            ("lh_ptr", t["lh_ptr"].astype(i32)), ("lh_col", t["lh_col"].astype(i32)),
+            ("lh_val", c2d(t["lh_val"])), ("lh_val_f", c2f(t["lh_val"])),
+            ("lop_active", t["lop_active"].astype(i32)), ("lop_site", t["lop_site"].astype(i32)),
+            ("lop_sval", c2d(t["lop_sval"])),
+            ("h_ptr", t["h_ptr"].astype(i32)), ("h_col", t["h_col"].astype(i32)),
+            ("h_val", c2d(t["h_val"])), ("h_val_f", c2f(t["h_val"])),
+            ("mode_site", t["mode_site"].astype(i32)), ("mode_gwv", c2d(t["mode_gwv"])),
+            ("mode_gwv_f", c2f(t["mode_gwv"])),
+            ("dn_coef_site", c2d(t["dn_coef_site"])), ("dn_coef_site_f", c2f(t["dn_coef_site"])),
+        ]
+        offs = {}
+        off = 0
+        for name, arr in fields:
             a = np.ascontiguousarray(arr)
             if a.size == 0:
-                a = np.zeros(2, dtype=a.dtype)
-            x = torch.from_numpy(a).to(self.device, dtype=dtype)
-            self._keep.append(x)
-            return x.data_ptr()
-
-        i32, f64, f32 = torch.int32, torch.float64, torch.float32
+                a = np.zeros(4, dtype=np.int32)
+            offs[name] = (off, a)
+            off += -(-a.nbytes // self._ALIGN) * self._ALIGN
+        struct_off = off
+        total = off + C.sizeof(HopsStructure)
+        self.buffer = torch.empty(total, dtype=torch.uint8, device=self.device)
+        base = self.buffer.data_ptr()
+        host = np.zeros(total, dtype=np.uint8)
         s = HopsStructure()
         s.n_hier, s.n_state, s.n_mode, s.n_lop = t["n_hier"], t["n_state"], t["n_mode"], t["n_lop"]
         s.n_first = len(t["first_aux"])
@@ -143,48 +179,13 @@ class DeviceStructure:
         s.n_dn = len(t["dn_aux"])
         s.site_projector = t["site_projector"]
         s.max_up, s.max_dn = t["max_up"], t["max_dn"]
-        s.k_decay = up(_c2d(t["k_decay"]), f64)
-        s.k_decay_f = up(_c2f(t["k_decay"]), f32)
-        s.up_ptr = up(t["up_ptr"], i32)
-        s.up_aux = up(t["up_aux"], i32)
-        s.up_mode = up(t["up_mode"], i32)
-        s.dn_ptr = up(t["dn_ptr"], i32)
-        s.dn_aux = up(t["dn_aux"], i32)
-        s.dn_mode = up(t["dn_mode"], i32)
-        s.dn_coef = up(_c2d(t["dn_coef"]), f64)
-        s.dn_coef_f = up(_c2f(t["dn_coef"]), f32)
-        s.mode_lop = up(t["mode_lop"], i32)
-        s.mode_g = up(_c2d(t["mode_g"]), f64)
-        s.mode_w = up(_c2d(t["mode_w"]), f64)
-        s.mode_gw = up(_c2d(t["mode_gw"]), f64)
-        s.mode_gw_f = up(_c2f(t["mode_gw"]), f32)
-        s.first_aux = up(t["first_aux"], i32)
-        s.first_mode = up(t["first_mode"], i32)
-        s.l_ptr = up(t["l_ptr"], i32)
-        s.l_col = up(t["l_col"], i32)
-        s.l_val = up(_c2d(t["l_val"]), f64)
-        s.l_val_f = up(_c2f(t["l_val"]), f32)
-        s.lh_ptr = up(t["lh_ptr"], i32)
-        s.lh_col = up(t["lh_col"], i32)
-        s.lh_val = up(_c2d(t["lh_val"]), f64)
-        s.lh_val_f = up(_c2f(t["lh_val"]), f32)
-        s.lop_active = up(t["lop_active"], i32)
-        s.lop_site = up(t["lop_site"], i32)
-        s.lop_sval = up(_c2d(t["lop_sval"]), f64)
-        s.h_ptr = up(t["h_ptr"], i32)
-        s.h_col = up(t["h_col"], i32)
-        s.h_val = up(_c2d(t["h_val"]), f64)
-        s.h_val_f = up(_c2f(t["h_val"]), f32)
-        s.mode_site = up(t["mode_site"], i32)
-        s.mode_gwv = up(_c2d(t["mode_gwv"]), f64)
-        s.mode_gwv_f = up(_c2f(t["mode_gwv"]), f32)
-        s.dn_coef_site = up(_c2d(t["dn_coef_site"]), f64)
-        s.dn_coef_site_f = up(_c2f(t["dn_coef_site"]), f32)
+        for name, (o, a) in offs.items():
+            host[o:o + a.nbytes] = a.view(np.uint8).ravel()
+            setattr(s, name, base + o)
+        host[struct_off:] = np.frombuffer(bytes(s), dtype=np.uint8)
+        self.buffer.copy_(torch.from_numpy(host))
         self.cstruct = s
-        # a device copy of the struct itself (resident tasks point at it)
-        raw = np.frombuffer(bytes(s), dtype=np.uint8).copy()
-        self._dev_struct = torch.from_numpy(raw).to(self.device)
-        self.dev_ptr = self._dev_struct.data_ptr()
+        self.dev_ptr = base + struct_off
 
     @property
     def n_elem(self):

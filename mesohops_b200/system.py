@@ -90,6 +90,15 @@ class HopsSystem:
         if len(lt) and np.any(np.asarray(lt) != 0):
             raise UnsupportedRequest("low-temperature correction (PARAM_LT_CORR)",
                                      "mesohops_b200 HopsSystem")
+        # state <-> mode maps (system_functions.py:33-39) and H couplings
+        self.states_by_lop = [np.array(self.states_of_lop(j), dtype=np.int64)
+                              for j in range(self.n_lop)]
+        self.modes_by_state = [[] for _ in range(self.n_state)]
+        for m in range(self.n_mode):
+            for st in self.states_by_lop[self.l_by_mode[m]]:
+                self.modes_by_state[st].append(m)
+        Hd = self.hamiltonian_dense()
+        self.coupled_states = [np.nonzero(Hd[i])[0] for i in range(self.n_state)]
         self.param = p
         self.param["NSTATES"] = self.n_state
         self.param["N_HMODES"] = self.n_mode

@@ -10,7 +10,8 @@ runs as CUDA kernels; the state stays on the device between calls.
 
 Options of this implementation go in the separate ``device_param`` dictionary
 (PRECISION, DEVICE, KERNEL); the reference dictionaries are validated exactly as
-MesoHOPS validates them.
+MesoHOPS validates them.  ``make_adaptive`` switches to the adaptive basis
+(adHOPS): see mesohops_b200/adaptive.py.
 """
 from __future__ import annotations
 
@@ -19,6 +20,7 @@ import time as timer
 import numpy as np
 import torch
 
+from . import adaptive as _adaptive
 from .constants import hbar, precision
 from .device import DeviceStructure, build_tables
 from .engine import ResidentRunner, ResidentTrajectory, StreamBatch
@@ -54,9 +56,8 @@ class HopsTrajectory:
         eom = self.eom_param["EQUATION_OF_MOTION"]
         if eom not in ("NORMALIZED NONLINEAR", "NONLINEAR", "LINEAR"):
             raise UnsupportedRequest("EQUATION_OF_MOTION =" + eom, "HopsEOM")
-        if self.eom_param["ADAPTIVE_H"] or self.eom_param["ADAPTIVE_S"]:
-            raise UnsupportedRequest("adaptive eom_param (use make_adaptive)", "HopsTrajectory")
-        self.eom_param["ADAPTIVE"] = False
+        self.eom_param["ADAPTIVE"] = bool(self.eom_param["ADAPTIVE_H"]
+                                          or self.eom_param["ADAPTIVE_S"])
         self.system = HopsSystem(system_param)
         self.hierarchy_param = initialize_dict(hierarchy_param or {}, HIERARCHY_DICT_DEFAULT,
                                                HIERARCHY_DICT_TYPES, "HopsHierarchy")
@@ -86,10 +87,12 @@ class HopsTrajectory:
         self.integrator_step = 0.5
         self.device_param = dict(DEVICE_DICT_DEFAULT)
         self.device_param.update(device_param or {})
-        self.storage = HopsStorage(False, storage_param)
+        self._storage_param = storage_param
+        self.storage = HopsStorage(self.eom_param["ADAPTIVE"], storage_param)
         self.__initialized__ = False
         self._t = 0.0
         self._runner = None
+        self._adhops = None
 
     # ------------------------------------------------------------------ setup
     def initialize(self, psi_0, timer_checkpoint=None):
@@ -99,6 +102,11 @@ class HopsTrajectory:
             raise LockedException("HopsTrajectory.initialize()", "HopsTrajectory")
         psi_0 = np.array(psi_0, dtype=np.complex128)
         dev = torch.device(self.device_param["DEVICE"])
+        if self.eom_param["ADAPTIVE"]:
+            self._initialize_adaptive(psi_0, dev)
+            self.storage.metadata["INITIALIZATION_TIME"] = timer.time() - t0
+            self.__initialized__ = True
+            return
         self.basis = triangular_basis(self.system.n_mode, self.hierarchy_param["MAXHIER"],
                                       self.hierarchy_param["STATIC_FILTERS"])
         self.dstruct = DeviceStructure(build_tables(self.system, self.basis), dev)
@@ -140,8 +148,54 @@ class HopsTrajectory:
 
     def make_adaptive(self, delta_a=1e-4, delta_s=1e-4, update_step=1, f_discard=0.01,
                       adaptive_noise=True):
-        raise UnsupportedRequest("make_adaptive on HopsTrajectory (use "
-                                 "mesohops_b200.adaptive.AdaptiveTrajectory)", "HopsTrajectory")
+        """Switch to an adaptive basis before initialize (hops_trajectory.py:338-400).
+
+        adaptive_noise is accepted for interface parity: the correlated noise of
+        every L-operator is generated on the device at once, and each row equals
+        the row an adaptive (per-L, on demand) generation produces."""
+        if float(f_discard) < 0 or float(f_discard) > 1:
+            raise UnsupportedRequest("f_discard not in acceptable range of [0,1]",
+                                     "make_adaptive")
+        if self.__initialized__:
+            raise TrajectoryError("Adaptive calculation cannot be turned on after "
+                                  "the trajectory is initialized")
+        ep = self.eom_param
+        if delta_a > 0:
+            ep["ADAPTIVE"] = True
+            ep["ADAPTIVE_H"] = True
+            ep["DELTA_A"] = delta_a
+            ep["UPDATE_STEP"] = update_step
+            ep["F_DISCARD"] = float(f_discard)
+        if delta_s > 0:
+            ep["ADAPTIVE"] = True
+            ep["ADAPTIVE_S"] = True
+            ep["DELTA_S"] = delta_s
+            ep["UPDATE_STEP"] = update_step
+            ep["F_DISCARD"] = float(f_discard)
+        if ep["ADAPTIVE"] and not self.storage.adaptive:
+            self.storage = HopsStorage(True, self._storage_param)
+
+    def _initialize_adaptive(self, psi_0, dev):
+        """hops_trajectory.py:282-326 with the adaptive basis on the device."""
+        self._adhops = _adaptive.AdaptiveHops(self)
+        n1 = self.noise1.prepare(dev)
+        n2 = self.noise2.prepare(dev)
+        self._n1, self._n2 = n1, n2
+        _adaptive.drive(self._adhops.initialize_gen(psi_0, n1, n2), dev)
+        self.kernel = "adaptive"
+        self.storage.n_dim = self.system.n_state
+        ad = self._adhops
+        self._t = 0.0
+        self._store_adaptive(0.0, np.zeros(self.system.n_mode, dtype=np.complex128))
+
+    def _store_adaptive(self, t, z_mem):
+        ad = self._adhops
+        b = ad.basis
+        aux_list = [np.array([(int(m), int(c[m])) for m in np.nonzero(c)[0]],
+                             dtype=int).reshape(-1, 2) for c in b.counts]
+        self.storage.store(float(t), psi=ad.phi[:b.n_state].copy(), phi=ad.phi.copy(),
+                           z_mem=z_mem.copy(), aux_list=aux_list,
+                           state_list=b.states.copy())
 
     # -------------------------------------------------------------- propagate
     def _check_tau_step(self, tau):
@@ -167,6 +221,15 @@ class HopsTrajectory:
         n_steps = int(np.ceil(t_advance / tau))
         t_axis = t0 + np.arange(1, 1 + n_steps) * tau
         if n_steps == 0:
+            return
+        if self._adhops is not None:
+            dev = torch.device(self.device_param["DEVICE"])
+            for index_t, t in enumerate(t_axis):
+                z_old = _adaptive.drive(self._adhops.step_gen(float(t), tau, index_t), dev)
+                if self.storage.check_storage_time(t):
+                    self._store_adaptive(t, z_old)
+                self._t = float(t)
+            self.storage.metadata["LIST_PROPAGATION_TIME"].append(timer.time() - t_start)
             return
         it0 = self.noise1.time_index(t0)
         di = int(round(tau * 0.5 / self.noise1.param["TAU"]))
@@ -209,6 +272,8 @@ class HopsTrajectory:
 
     # -------------------------------------------------------------- read-outs
     def _get_state(self):
+        if self._adhops is not None:
+            return self._adhops.phi.copy(), self._adhops.zmem_abs.copy()
         if self.kernel == "resident":
             return self._traj.get_state()
         phi, z = self._traj.get_state()
@@ -248,19 +313,27 @@ class HopsTrajectory:
 
     @property
     def n_hier(self):
+        if self._adhops is not None:
+            return self._adhops.basis.n_hier
         return self.basis.n_hier
 
     @property
     def n_state(self):
+        if self._adhops is not None:
+            return self._adhops.basis.n_state
         return self.system.n_state
 
     @property
     def state_list(self):
+        if self._adhops is not None:
+            return self._adhops.basis.states.copy()
         return np.arange(self.system.n_state)
 
     @property
     def auxiliary_list(self):
         """Aux vectors as dense count rows, in the reference order."""
+        if self._adhops is not None:
+            return self._adhops.basis.counts
         return self.basis.counts
 
     def normalize(self, phi):

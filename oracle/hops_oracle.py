@@ -332,6 +332,73 @@ def propagate(basis, psi0, noise1, tau_noise, t_max, dt, noise2=None,
 
 
 # ---------------------------------------------------------------------------
+# Adaptive sub-basis and the flux-error terms of the basis update
+# ---------------------------------------------------------------------------
+class OracleSubBasis(OracleBasis):
+    """One adaptive basis: a subset of states, of modes and of aux.
+
+    basis/hops_modes.py:123-171 reduces every unique L of the basis modes to the
+    state basis; the relative L list is the sorted absolute unique-L indices of
+    the basis modes (list_absindex_L2), so noise rows are noise[l_abs].
+    states / modes: sorted absolute indices; aux: count rows over ALL modes.
+    """
+
+    def __init__(self, sys_param, states, modes, aux):
+        full = expand_system(sys_param)
+        states = np.asarray(states, dtype=np.int64)
+        modes = np.asarray(modes, dtype=np.int64)
+        self.l_abs = sorted(set(int(full["L_BY_MODE"][m]) for m in modes))
+        rel = {j: i for i, j in enumerate(self.l_abs)}
+        ix = np.ix_(states, states)
+        self.sys = {"H": full["H"][ix], "G": full["G"][modes], "W": full["W"][modes],
+                    "L": [full["L"][j][ix] for j in self.l_abs],
+                    "L_BY_MODE": np.array([rel[int(full["L_BY_MODE"][m])] for m in modes],
+                                          dtype=np.int64),
+                    "NSTATE": len(states), "NMODE": len(modes)}
+        self.states, self.modes = states, modes
+        self.nstate, self.nmode = len(states), len(modes)
+        self.aux = np.asarray(aux, dtype=np.int64)[:, modes].reshape(-1, len(modes))
+        self.nhier = len(self.aux)
+        self.index = {tuple(v): i for i, v in enumerate(self.aux)}
+        self._build_super_operators()
+
+
+def flux_errors(basis, phi, zmem, z1, z2, dt, mask=None, eom="NORMALIZED NONLINEAR"):
+    """Error arrays of the adaptive update for diagonal L-operators.
+
+    e_deriv [N, S]: |dphi/dt / hbar + phi / dt|^2 of the phi restricted to the
+        aux with mask != 0 (error_deriv, basis/basis_functions_adaptive.py:10-74);
+        rows with mask == 0 are 0.
+    e_up [M, N]: |w_m|^2 (1 + k_m(a))^2 sum_s |L_m[s,s]|^2 |phi[a,s]|^2 / hbar^2
+        (error_flux_up_hier_stable, :165-266).
+    e_down [M, N]: |g_m / w_m|^2 sum_s |L_m[s,s] - <L_m>|^2 |phi[a,s]|^2 / hbar^2
+        (error_flux_down_hier_stable, :517-624; <L> of the unmasked psi_0).
+    """
+    s = basis.sys
+    S, N, M = basis.nstate, basis.nhier, basis.nmode
+    phi = np.asarray(phi, dtype=np.complex128)
+    ph = phi.copy().reshape(N, S)
+    if mask is not None:
+        ph[np.asarray(mask) == 0] = 0.0
+    dphi, _ = dsystem_dt(basis, ph.ravel(), zmem, z1, z2, eom)
+    e_deriv = np.abs(dphi / HBAR + ph.ravel() / dt).reshape(N, S) ** 2
+    if mask is not None:
+        e_deriv[np.asarray(mask) == 0] = 0.0
+    pf = phi.reshape(N, S)
+    psi0 = pf[0]
+    n2 = np.vdot(psi0, psi0)
+    avg = np.array([np.vdot(psi0, l @ psi0) / n2 for l in s["L"]])
+    m2 = np.array([np.diag(s["L"][s["L_BY_MODE"][m]]) for m in range(M)]).reshape(M, S)
+    p2 = np.abs(pf) ** 2                                   # [N, S]
+    k = basis.aux.T.astype(np.float64)                     # [M, N]
+    w2 = np.abs(s["W"]) ** 2
+    e_up = (w2[:, None] * (1.0 + k) ** 2) * ((np.abs(m2) ** 2) @ p2.T) / HBAR ** 2
+    d2 = np.abs(m2 - avg[s["L_BY_MODE"]][:, None]) ** 2
+    e_down = (np.abs(s["G"] / s["W"]) ** 2)[:, None] * (d2 @ p2.T) / HBAR ** 2
+    return e_deriv, e_up, e_down
+
+
+# ---------------------------------------------------------------------------
 # FFT-filtered noise
 # ---------------------------------------------------------------------------
 def noise_t_axis(tlen, tau):

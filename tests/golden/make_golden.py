@@ -238,5 +238,100 @@ def main():
     make_noise_fixture()
 
 
-if __name__ == "__main__":
+if __name__ == "__main__" and "--adaptive" not in sys.argv:
     main()
+
+
+def run_adaptive(name, sysp, depth, psi0, t_max, dt, delta_a, delta_s, noise_seed,
+                 update_step=1, f_discard=0.0):
+    """Adaptive propagation with PRE_CALCULATED noise; records the basis per step."""
+    tau_noise = dt / 2.0
+    tlen = t_max + dt
+    n_t = int(np.ceil(tlen / tau_noise)) + 1
+    nl = n_unique(sysp)
+    rng = np.random.default_rng(noise_seed)
+    noise = ((rng.normal(size=(nl, n_t)) + 1j * rng.normal(size=(nl, n_t))) * 20.0).astype(np.complex64)
+    tmpdir = tempfile.mkdtemp()
+    path1 = os.path.join(tmpdir, "noise1.npy")
+    np.save(path1, noise)
+    hops = HopsTrajectory(sysp, noise_param={"SEED": path1, "MODEL": "PRE_CALCULATED",
+                                             "TLEN": float(tlen), "TAU": float(tau_noise)},
+                          hierarchy_param={"MAXHIER": depth},
+                          eom_param={"EQUATION_OF_MOTION": "NORMALIZED NONLINEAR"},
+                          storage_param={})
+    # adaptive_noise=False: the reference only supports sparse noise storage for
+    # FFT_FILTER (hops_noise.py:244-245,320-323); values are the same either way
+    hops.make_adaptive(delta_a, delta_s, update_step=update_step, f_discard=f_discard,
+                       adaptive_noise=False)
+    quiet(hops.initialize, psi0)
+    quiet(hops.propagate, t_max, dt)
+    d = hops.storage.data
+    psi_full = np.array(hops.storage["psi_traj"])
+    n_mode = len(sysp["GW_SYSBATH"])
+    aux_counts = []
+    aux_ptr = [0]
+    for aux_list in d["aux_list"]:
+        for a in aux_list:
+            v = np.zeros(n_mode, dtype=np.int16)
+            for (m, k) in np.asarray(a).reshape(-1, 2):
+                v[m] = k
+            aux_counts.append(v)
+        aux_ptr.append(len(aux_counts))
+    state_ptr = [0]
+    states = []
+    for sl in d["state_list"]:
+        states.extend(list(sl))
+        state_ptr.append(len(states))
+    H = sysp["HAMILTONIAN"]
+    H = H.toarray() if sps.issparse(H) else np.asarray(H)
+    np.savez_compressed(
+        os.path.join(HERE, name + ".npz"),
+        H=np.array(H, dtype=np.complex128), G=np.array([g for g, w in sysp["GW_SYSBATH"]]),
+        W=np.array([w for g, w in sysp["GW_SYSBATH"]]), L=dense_lops(sysp), depth=depth,
+        psi0=np.array(psi0, dtype=np.complex128), t_max=t_max, dt=dt, tau_noise=tau_noise,
+        tlen=tlen, noise1=noise, delta_a=delta_a, delta_s=delta_s, update_step=update_step,
+        f_discard=f_discard, psi_traj=psi_full, t_axis=np.array(d["t_axis"]),
+        list_nhier=np.array(d["list_nhier"]), list_nstate=np.array(d["list_nstate"]),
+        aux_counts=np.array(aux_counts, dtype=np.int16).reshape(-1, n_mode),
+        aux_ptr=np.array(aux_ptr), states=np.array(states), state_ptr=np.array(state_ptr),
+        phi_end=np.array(hops.phi), n_hier_end=hops.n_hier, n_state_end=hops.n_state)
+    print(name, "adaptive steps", len(psi_full) - 1, "n_hier", list(d["list_nhier"])[:8],
+          "n_state", list(d["list_nstate"])[:8])
+
+
+def main_adaptive():
+    # dimer of dimers, tiny delta_a: the adaptive basis must equal the full one
+    hs = np.zeros((4, 4))
+    hs[0, 1] = hs[1, 0] = 40
+    hs[1, 2] = hs[2, 1] = 10
+    hs[2, 3] = hs[3, 2] = 40
+    g0, w0 = bcf_convert_dl_to_exp(20.0, 50.0, 140.0)
+    gw, lops = [], []
+    for i in range(4):
+        L = np.zeros((4, 4))
+        L[i, i] = 1.0
+        gw.append([g0, w0])
+        lops.append(sps.coo_matrix(L))
+        gw.append([-1j * np.imag(g0), 500.0])
+        lops.append(L)
+    sysp = {"HAMILTONIAN": np.array(hs, dtype=np.complex128), "GW_SYSBATH": gw,
+            "L_HIER": lops, "L_NOISE1": lops, "ALPHA_NOISE1": bcf_exp, "PARAM_NOISE1": gw}
+    psi0 = np.zeros(4, dtype=np.complex128)
+    psi0[2] = 1.0
+    run_adaptive("adaptive_dod_full", sysp, 2, psi0, 80.0, 4.0, 1e-15, 1e-100, noise_seed=31)
+    # chains with a moderate threshold (the adaptive benchmark shape, reduced)
+    for (name, n, depth, delta, seed) in [("adaptive_chain8", 8, 3, 3e-4, 32),
+                                          ("adaptive_chain12", 12, 4, 1e-3, 33)]:
+        rng = np.random.default_rng(3)
+        eps = rng.normal(0, 100, n)
+        H = np.diag(eps)
+        for i in range(n - 1):
+            H[i, i + 1] = H[i + 1, i] = 50.0
+        psi0 = np.zeros(n, dtype=np.complex128)
+        psi0[n // 2] = 1.0
+        run_adaptive(name, site_system(H, [(50, 50, 295)]), depth, psi0, 120.0, 4.0,
+                     delta, delta, noise_seed=seed)
+
+
+if __name__ == "__main__" and "--adaptive" in sys.argv:
+    main_adaptive()
