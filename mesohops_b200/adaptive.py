@@ -87,11 +87,11 @@ class Basis:
         # K2_aux_by_mode (hops_basis.py:1140-1151)
         self.k_aux = np.ascontiguousarray(self.counts[:, self.modes].T.astype(np.uint8))
         # M2_mode_from_state_diag (hops_basis.py:1031-1050), dense [mode, state]
-        ix = np.ix_(self.states, self.states)
+        self.lred = [system.lop_block(j, self.states) for j in self.tables["l_abs"]]
+        rel_l = {int(j): i for i, j in enumerate(self.tables["l_abs"])}
         self.m2 = np.zeros((self.n_mode, self.n_state), dtype=np.complex128)
         for i, m in enumerate(self.modes):
-            self.m2[i] = np.diag(system.lops[system.l_by_mode[m]][ix])
-        self.lred = [system.lops[j][ix] for j in self.tables["l_abs"]]
+            self.m2[i] = np.diag(self.lred[rel_l[int(system.l_by_mode[m])]])
         # HopsSystem.list_sc: states outside the basis coupled to it by H
         sset = set(self.states.tolist())
         sc = set()
@@ -234,6 +234,35 @@ def drive(gen, device):
             result = serve_flux([req], device)[0]
 
 
+def drive_many(gens, device):
+    """Run many coroutines in lock-step: every round serves all pending step
+    requests with one launch and all pending flux requests with one launch.
+    Returns the coroutines' return values."""
+    values = [None] * len(gens)
+    pending = {}
+    for i, g in enumerate(gens):
+        try:
+            pending[i] = g.send(None)
+        except StopIteration as stop:
+            values[i] = stop.value
+    while pending:
+        served = {}
+        steps = [i for i, r in pending.items() if isinstance(r, StepRequest)]
+        if steps:
+            served.update(zip(steps, serve_steps([pending[i] for i in steps], device)))
+        flux = [i for i, r in pending.items() if not isinstance(r, StepRequest)]
+        if flux:
+            served.update(zip(flux, serve_flux([pending[i] for i in flux], device)))
+        nxt = {}
+        for i, res in served.items():
+            try:
+                nxt[i] = gens[i].send(res)
+            except StopIteration as stop:
+                values[i] = stop.value
+        pending = nxt
+    return values
+
+
 # ------------------------------------------------------------------- driver
 class AdaptiveHops:
     """Adaptive basis state of one trajectory.
@@ -267,9 +296,8 @@ class AdaptiveHops:
         if self.eom == "LINEAR":
             raise UnsupportedRequest("LINEAR equation of motion with an adaptive basis",
                                      "HopsTrajectory")
-        for l in self.system.lops:
-            r, c = np.nonzero(l)
-            if np.any(r != c):
+        for j in range(self.system.n_lop):
+            if not self.system.lop_is_diagonal(j):
                 raise UnsupportedRequest("adaptive basis with off-diagonal L-operator couplings",
                                          "mesohops_b200 adaptive propagation")
         n1, n2 = traj.noise1, traj.noise2

@@ -64,7 +64,7 @@ def build_tables(system, basis, state_list=None, mode_list=None):
     l_rel_of_abs = {int(j): i for i, j in enumerate(l_abs)}
     mode_lop = np.array([l_rel_of_abs[int(system.l_by_mode[m])] for m in modes], dtype=np.int32)
     ix = np.ix_(states, states)
-    lops = [system.lops[j][ix] for j in l_abs]
+    lops = [system.lop_block(j, states) for j in l_abs]
     lop_active = np.array([1 if np.any(l != 0) else 0 for l in lops], dtype=np.int32)
     # site-projector form: exactly one diagonal nonzero
     site = np.zeros(L, dtype=np.int32)

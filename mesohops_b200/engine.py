@@ -246,9 +246,14 @@ class ResidentRunner:
         psi_out: optional list of device tensors [n_steps_i, S_i] complex128.
         Returns the per-trajectory status array.
         """
+        return self.collect(self.launch(trajs, it0, di, n_steps, tau_over_hbar, psi_out))
+
+    def launch(self, trajs, it0, di, n_steps, tau_over_hbar, psi_out=None):
+        """Enqueue the launch of ``run`` on the current stream and return a handle
+        for ``collect`` (nothing waits on the device here)."""
         n = len(trajs)
         if n == 0:
-            return np.zeros(0, dtype=np.int32)
+            return None
         prec = trajs[0].prec
         if any(t.prec != prec for t in trajs):
             raise ValueError("one resident launch needs one precision")
@@ -286,7 +291,16 @@ class ResidentRunner:
         rc = _lib.lib().hops_resident_propagate(tdev.data_ptr(), n, max_elems, max_sc, prec, site,
                                                 _stream(self.dev))
         _lib.check(rc, "hops_resident_propagate")
-        back = tdev.cpu().numpy().tobytes()
+        return (trajs, tdev, torch.cuda.current_stream(self.dev))
+
+    def collect(self, handle):
+        """Wait for a launch and return its per-trajectory status array."""
+        if handle is None:
+            return np.zeros(0, dtype=np.int32)
+        trajs, tdev, stream = handle
+        n = len(trajs)
+        with torch.cuda.stream(stream):
+            back = tdev.cpu().numpy().tobytes()
         out = (HopsTask * n).from_buffer_copy(back)
         status = np.array([out[i].status for i in range(n)], dtype=np.int32)
         for i, tr in enumerate(trajs):

@@ -181,16 +181,19 @@ class AuxBasis:
         """k+1 / k-1 connections along the basis modes (hops_hierarchy.py:470-523)."""
         ups_a, ups_u, ups_m = [], [], []
         below = np.nonzero(self.depth < self.maxhier)[0]
-        for rel, m in enumerate(self.modes):
-            if len(below) == 0:
-                break
-            up = self.counts[below].copy()
-            up[:, m] += 1
-            idx = self.index_of(up)
-            ok = idx >= 0
-            ups_a.append(below[ok])
-            ups_u.append(idx[ok])
-            ups_m.append(np.full(ok.sum(), rel, dtype=np.int64))
+        n_abs = self.counts.shape[1]
+        # modes per batch: keep the stacked candidate rows near 4M count entries
+        per = max(1, int(4_000_000 // max(1, len(below) * n_abs)))
+        for c0 in range(0, len(self.modes) if len(below) else 0, per):
+            rels = np.arange(c0, min(c0 + per, len(self.modes)))
+            up = np.repeat(self.counts[below][None], len(rels), axis=0)
+            up[np.arange(len(rels)), :, self.modes[rels]] += 1
+            idx = self.index_of(up.reshape(-1, n_abs)).reshape(len(rels), len(below))
+            for i, rel in enumerate(rels):
+                ok = idx[i] >= 0
+                ups_a.append(below[ok])
+                ups_u.append(idx[i][ok])
+                ups_m.append(np.full(ok.sum(), rel, dtype=np.int64))
         if ups_a:
             a = np.concatenate(ups_a)
             u = np.concatenate(ups_u)

@@ -32,13 +32,15 @@ def pattern_key(lop):
     return tuple(tuple(int(x) for x in v) for v in nz)
 
 
-def _dense(op, n):
+def _csr(op, n):
     if sps.issparse(op):
-        return np.asarray(op.toarray(), dtype=np.complex128)
-    a = np.asarray(op, dtype=np.complex128)
+        a = sps.csr_matrix(op, dtype=np.complex128)
+    else:
+        a = sps.csr_matrix(np.asarray(op, dtype=np.complex128))
     if a.shape != (n, n):
         raise UnsupportedRequest(f"operator of shape {a.shape} (expected {(n, n)})",
                                  "HopsSystem", override=True)
+    a.eliminate_zeros()
     return a
 
 
@@ -68,14 +70,16 @@ class HopsSystem:
         # unique L (system_functions.py:64-107)
         keys = [pattern_key(l) for l in p["L_HIER"]]
         self._key_index = {}
-        self.lops = []                      # dense complex [n_state, n_state]
+        self.lops_csr = []                  # sparse complex [n_state, n_state]
         self.l_by_mode = np.zeros(self.n_mode, dtype=np.int64)
         for m, k in enumerate(keys):
             if k not in self._key_index:
-                self._key_index[k] = len(self.lops)
-                self.lops.append(_dense(p["L_HIER"][m], self.n_state))
+                self._key_index[k] = len(self.lops_csr)
+                self.lops_csr.append(_csr(p["L_HIER"][m], self.n_state))
             self.l_by_mode[m] = self._key_index[k]
-        self.n_lop = len(self.lops)
+        self.n_lop = len(self.lops_csr)
+        self._lops_dense = None
+        self._coo = None
         self.modes_by_l = [np.nonzero(self.l_by_mode == j)[0] for j in range(self.n_lop)]
         # noise 1 (system_functions.py:135-150)
         self.l_by_nmode1, self.nmodes1_by_l = self._noise_map(p["L_NOISE1"], p["PARAM_NOISE1"])
@@ -130,7 +134,32 @@ class HopsSystem:
         H = self.hamiltonian
         return H.toarray() if sps.issparse(H) else np.asarray(H)
 
+    @property
+    def lops(self):
+        """Unique L-operators as dense arrays (built on first use; small systems)."""
+        if self._lops_dense is None:
+            self._lops_dense = [l.toarray() for l in self.lops_csr]
+        return self._lops_dense
+
+    def lop_block(self, j, states):
+        """Dense block L_j[states, states] (O(nnz(L_j)) via a position map)."""
+        states = np.asarray(states, dtype=np.int64)
+        if self._coo is None:
+            self._coo = [(l.tocoo().row, l.tocoo().col, l.tocoo().data) for l in self.lops_csr]
+        r, c, v = self._coo[j]
+        pos = np.full(self.n_state, -1, dtype=np.int64)
+        pos[states] = np.arange(len(states))
+        pr, pc = pos[r], pos[c]
+        keep = (pr >= 0) & (pc >= 0)
+        out = np.zeros((len(states), len(states)), dtype=np.complex128)
+        np.add.at(out, (pr[keep], pc[keep]), v[keep])
+        return out
+
+    def lop_is_diagonal(self, j):
+        r, c = self.lops_csr[j].nonzero()
+        return bool(np.all(r == c))
+
     def states_of_lop(self, j):
         """States touched by L_j (helper_functions.py:50-66)."""
-        r, c = np.nonzero(self.lops[j])
+        r, c = self.lops_csr[j].nonzero()
         return sorted(set(r.tolist()) | set(c.tolist()))

@@ -184,9 +184,16 @@ class HopsTrajectory:
         _adaptive.drive(self._adhops.initialize_gen(psi_0, n1, n2), dev)
         self.kernel = "adaptive"
         self.storage.n_dim = self.system.n_state
-        ad = self._adhops
         self._t = 0.0
         self._store_adaptive(0.0, np.zeros(self.system.n_mode, dtype=np.complex128))
+
+    def adaptive_step_gen(self, t, tau, index_t):
+        """One adaptive step as a coroutine of device requests (see
+        mesohops_b200.adaptive), with the storage of hops_trajectory.py:523-526."""
+        z_old = yield from self._adhops.step_gen(t, tau, index_t)
+        if self.storage.check_storage_time(t):
+            self._store_adaptive(t, z_old)
+        self._t = float(t)
 
     def _store_adaptive(self, t, z_mem):
         ad = self._adhops
@@ -225,10 +232,7 @@ class HopsTrajectory:
         if self._adhops is not None:
             dev = torch.device(self.device_param["DEVICE"])
             for index_t, t in enumerate(t_axis):
-                z_old = _adaptive.drive(self._adhops.step_gen(float(t), tau, index_t), dev)
-                if self.storage.check_storage_time(t):
-                    self._store_adaptive(t, z_old)
-                self._t = float(t)
+                _adaptive.drive(self.adaptive_step_gen(float(t), tau, index_t), dev)
             self.storage.metadata["LIST_PROPAGATION_TIME"].append(timer.time() - t_start)
             return
         it0 = self.noise1.time_index(t0)

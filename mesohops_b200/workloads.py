@@ -75,3 +75,65 @@ WORKLOADS = {
                   desc="2-site dimer H=[[0,50],[50,0]], DL (50,50,295 K) per site, depth 4 "
                        "(15 aux x 2 states), one trajectory, dt=4 fs, 1000 fs"),
 }
+
+
+# ----------------------------------------------------------- served stream
+def served_stream_specs(n_requests=4096, seed=4, dt=4.0, mean_gap_s=2e-3):
+    """Specs of the served request stream: Poisson arrivals (exponential gaps,
+    mean 2 ms); each request a linear chain of N_site ~ U{2..200} sites
+    (J = 50 cm^-1, eps ~ N(0, 100)), depth ~ U{3..8}, adaptive (delta = 1e-3)
+    by a fair coin, one Drude-Lorentz mode per site with lambda ~ U(20, 80),
+    gamma ~ U(30, 150) cm^-1 at 295 K, dt = 4 fs, t_max ~ U(200, 2000) fs,
+    psi_0 on a uniformly drawn site; all from one generator seeded with 4.
+    Returns a list of dicts (cheap; systems are built by ``served_request``)."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n_requests):
+        t += rng.exponential(mean_gap_s)
+        n_site = int(rng.integers(2, 201))
+        depth = int(rng.integers(3, 9))
+        adaptive = bool(rng.random() < 0.5)
+        lam = float(rng.uniform(20, 80))
+        gam = float(rng.uniform(30, 150))
+        t_max = float(rng.uniform(200, 2000))
+        eps = rng.normal(0, 100, n_site)
+        start = int(rng.integers(0, n_site))
+        out.append(dict(rid=i, arrival=t, n_site=n_site, depth=depth, adaptive=adaptive,
+                        lam=lam, gam=gam, t_max=t_max, eps=eps, start=start, dt=dt,
+                        noise_seed=i))
+    return out
+
+
+def served_request(spec, delta=1e-3):
+    """TrajectoryRequest of one stream spec (FFT-filtered noise, seed = request id)."""
+    from .serving import TrajectoryRequest
+    n = spec["n_site"]
+    sysp = chain(n, 50.0, spec["eps"], spec["lam"], spec["gam"])
+    dt = spec["dt"]
+    n_steps = int(np.ceil(spec["t_max"] / dt - 1e-12))
+    psi0 = np.zeros(n, dtype=np.complex128)
+    psi0[spec["start"]] = 1.0
+    noise = {"SEED": spec["noise_seed"], "MODEL": "FFT_FILTER", "TLEN": (n_steps + 1) * dt,
+             "TAU": dt / 2}
+    return TrajectoryRequest(spec["rid"], sysp, psi0, n_steps * dt, dt,
+                             hierarchy_param={"MAXHIER": spec["depth"]},
+                             eom_param={"EQUATION_OF_MOTION": "NORMALIZED NONLINEAR"},
+                             noise_param=noise,
+                             adaptive=(delta, delta) if spec["adaptive"] else None,
+                             arrival=spec["arrival"])
+
+
+def adaptive_chain500(n_traj=512, seed=3):
+    """500-site chain (J = 50 cm^-1, eps ~ N(0, 100) from seed 3), one DL mode
+    per site (50, 50, 295 K), depth 10, delta_a = delta_s = 1e-3, dt = 4 fs;
+    psi_0 on a site drawn from the same generator.  Returns (system_param,
+    psi_0, per-trajectory noise seeds)."""
+    n = 500
+    rng = np.random.default_rng(seed)
+    eps = rng.normal(0, 100, n)
+    start = int(rng.integers(0, n))
+    sysp = chain(n, 50.0, eps, 50.0, 50.0)
+    psi0 = np.zeros(n, dtype=np.complex128)
+    psi0[start] = 1.0
+    return sysp, psi0, list(range(n_traj))

@@ -343,8 +343,8 @@ class OracleSubBasis(OracleBasis):
     states / modes: sorted absolute indices; aux: count rows over ALL modes.
     """
 
-    def __init__(self, sys_param, states, modes, aux):
-        full = expand_system(sys_param)
+    def __init__(self, sys_param, states, modes, aux, full=None):
+        full = expand_system(sys_param) if full is None else full
         states = np.asarray(states, dtype=np.int64)
         modes = np.asarray(modes, dtype=np.int64)
         self.l_abs = sorted(set(int(full["L_BY_MODE"][m]) for m in modes))

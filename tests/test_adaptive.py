@@ -59,6 +59,7 @@ class OracleServer:
 
     def __init__(self, sysp, noise1, tau_noise):
         self.sysp = sysp
+        self.full = O.expand_system(sysp)
         self.noise1 = noise1
         self.tau_noise = tau_noise
         self.cache = {}
@@ -67,7 +68,7 @@ class OracleServer:
         key = id(basis)
         if key not in self.cache:
             self.cache[key] = (basis, O.OracleSubBasis(self.sysp, basis.states, basis.modes,
-                                                       basis.counts))
+                                                       basis.counts, full=self.full))
         return self.cache[key][1]
 
     def step(self, r):
