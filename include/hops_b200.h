@@ -104,6 +104,11 @@ typedef struct hops_structure {
   const float* mode_gwv_f;
   const double* dn_coef_site;  /* [n_dn] complex k_m(a) w_m conj(v_{l(m)}) */
   const float* dn_coef_site_f;
+  const int32_t* up_site;      /* [n_up] s_{l(m)} of the connection's mode, or -1 */
+  const int32_t* dn_site;      /* [n_dn] s_{l(m)} of the connection's mode, or -1 */
+  /* site-projector form: diagonal of -i H, kept out of the H CSR above and
+     added to the per-state diagonal coefficient; NULL otherwise */
+  const double* h_diag;        /* [n_state] complex */
 } hops_structure;
 
 /*
@@ -251,6 +256,7 @@ size_t hops_noise_filter_work_doubles(int32_t n_lop, int32_t n_t);
  * counterpart in the reference.
  */
 int hops_stage_tuning(int32_t nb, int32_t chunk_major);
+
 
 /*
  * Profiling aid: when enabled, every streaming stage-kernel launch is bracketed

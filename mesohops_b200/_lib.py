@@ -39,6 +39,7 @@ class HopsStructure(C.Structure):
         ("h_ptr", _p), ("h_col", _p), ("h_val", _p), ("h_val_f", _p),
         ("mode_site", _p), ("mode_gwv", _p), ("mode_gwv_f", _p),
         ("dn_coef_site", _p), ("dn_coef_site_f", _p),
+        ("up_site", _p), ("dn_site", _p), ("h_diag", _p),
     ]
 
 

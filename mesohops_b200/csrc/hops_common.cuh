@@ -256,13 +256,15 @@ __device__ void stage_scalars(const hops_structure& st, const StageIO& io, Get g
     }
   }
 
-  // Per-state diagonal: -nc + sum_j cz_j v_j [s == s_j] (site-projector form).
+  // Per-state diagonal (site-projector form): -nc + sum_j cz_j v_j [s == s_j]
+  // + (-iH)[s,s] (the H CSR of such a structure holds the couplings only).
   for (int s = threadIdx.x; s < S; s += blockDim.x) {
     double2 d = mk(-nc, 0.0);
     if (st.site_projector) {
       const double2* cz = reinterpret_cast<const double2*>(ws + lay.cz());
       for (int j = 0; j < L; ++j)
         if (st.lop_site[j] == s) d = cfma(cz[j], ld2(st.lop_sval, j), d);
+      if (st.h_diag) d = cadd(d, ld2(st.h_diag, s));
     }
     reinterpret_cast<double2*>(ws + lay.diagD())[s] = d;
     reinterpret_cast<float2*>(ws + lay.diagD_f())[s] = mkf((float)d.x, (float)d.y);

@@ -63,6 +63,7 @@ template <> struct Prec<double> {
   static __device__ __forceinline__ T lval(const hops_structure& st, int q) { return ld2(st.l_val, q); }
   static __device__ __forceinline__ T lhval(const hops_structure& st, int q) { return ld2(st.lh_val, q); }
   static __device__ __forceinline__ T hval(const hops_structure& st, int q) { return ld2(st.h_val, q); }
+  static __device__ __forceinline__ T hdiag(const hops_structure& st, int s) { return ld2(st.h_diag, s); }
 };
 template <> struct Prec<float> {
   using T = float2;
@@ -74,6 +75,10 @@ template <> struct Prec<float> {
   static __device__ __forceinline__ T lval(const hops_structure& st, int q) { return ld2f(st.l_val_f, q); }
   static __device__ __forceinline__ T lhval(const hops_structure& st, int q) { return ld2f(st.lh_val_f, q); }
   static __device__ __forceinline__ T hval(const hops_structure& st, int q) { return ld2f(st.h_val_f, q); }
+  static __device__ __forceinline__ T hdiag(const hops_structure& st, int s) {
+    const double2 v = ld2(st.h_diag, s);
+    return mkf((float)v.x, (float)v.y);
+  }
 };
 
 // Workspace of a batch: B per-trajectory ScalarLayout blocks followed by the
@@ -162,6 +167,9 @@ __device__ __forceinline__ typename Prec<R>::T deriv_elem(const hops_structure& 
   } else {
     T d = P::kdec(st, a);
     d.x -= cf.nc();
+    // a site-projector structure evaluated by the general path: the diagonal
+    // of -iH is not in its H CSR
+    if (st.h_diag) d = cadd(d, P::hdiag(st, s));
     k = cmul(d, y(a, s));
     const int base_s = s;
     for (int j = 0; j < st.n_lop; ++j) {
@@ -179,7 +187,7 @@ __device__ __forceinline__ typename Prec<R>::T deriv_elem(const hops_structure& 
     const int u = st.up_aux[p], m = st.up_mode[p];
     T c = cf.upc(m);
     if (SITE) {
-      if (st.mode_site[m] == s) c = csub(c, P::gwv(st, m));
+      if (st.up_site[p] == s) c = csub(c, P::gwv(st, m));
       k = cfma(c, y(u, s), k);
     } else {
       k = cfma(c, y(u, s), k);
@@ -194,10 +202,11 @@ __device__ __forceinline__ typename Prec<R>::T deriv_elem(const hops_structure& 
   }
   const int d0 = st.dn_ptr[a], d1 = st.dn_ptr[a + 1];
   for (int p = d0; p < d1; ++p) {
-    const int d = st.dn_aux[p], m = st.dn_mode[p];
+    const int d = st.dn_aux[p];
     if (SITE) {
-      if (st.mode_site[m] == s) k = cfma(P::dncs(st, p), y(d, s), k);
+      if (st.dn_site[p] == s) k = cfma(P::dncs(st, p), y(d, s), k);
     } else {
+      const int m = st.dn_mode[p];
       const int base = st.mode_lop[m] * (st.n_state + 1);
       const int q0 = st.lh_ptr[base + s], q1 = st.lh_ptr[base + s + 1];
       if (q0 != q1) {
@@ -380,6 +389,7 @@ __global__ void __launch_bounds__(256) k_wide(hops_structure st, int B, int stag
         for (; p0 + 2 <= u1; p0 += 2) {
           const int ua = __ldg(st.up_aux + p0), ma = __ldg(st.up_mode + p0);
           const int ub = __ldg(st.up_aux + p0 + 1), mb = __ldg(st.up_mode + p0 + 1);
+          const int sa = __ldg(st.up_site + p0), sb = __ldg(st.up_site + p0 + 1);
           const size_t ra = ((size_t)ua * S + s) * B + bg + lane;
           const size_t rb = ((size_t)ub * S + s) * B + bg + lane;
           ST ya[NB], yb[NB];
@@ -392,8 +402,8 @@ __global__ void __launch_bounds__(256) k_wide(hops_structure st, int B, int stag
           }
           const T* upa = upcT + (size_t)ma * B + bg + lane;
           const T* upb = upcT + (size_t)mb * B + bg + lane;
-          const T corra = __ldg(st.mode_site + ma) == s ? P::gwv(st, ma) : czero<T>();
-          const T corrb = __ldg(st.mode_site + mb) == s ? P::gwv(st, mb) : czero<T>();
+          const T corra = sa == s ? P::gwv(st, ma) : czero<T>();
+          const T corrb = sb == s ? P::gwv(st, mb) : czero<T>();
 #pragma unroll
           for (int j = 0; j < NB; ++j) {
             if (ok[j]) {
@@ -408,7 +418,7 @@ __global__ void __launch_bounds__(256) k_wide(hops_structure st, int B, int stag
         const size_t rb = ((size_t)u * S + s) * B + bg + lane;
         const T* up = upcT + (size_t)m * B + bg + lane;
         if (SITE) {
-          const bool hit = st.mode_site[m] == s;
+          const bool hit = st.up_site[p] == s;
           const T corr = hit ? P::gwv(st, m) : czero<T>();
 #pragma unroll
           for (int j = 0; j < NB; ++j)
@@ -429,15 +439,16 @@ __global__ void __launch_bounds__(256) k_wide(hops_structure st, int B, int stag
         }
       }
       for (int p = d0; p < d1; ++p) {
-        const int d = st.dn_aux[p], m = st.dn_mode[p];
         if (SITE) {
-          if (st.mode_site[m] != s) continue;
+          if (__ldg(st.dn_site + p) != s) continue;
+          const int d = __ldg(st.dn_aux + p);
           const T cf = P::dncs(st, p);
           const size_t rb = ((size_t)d * S + s) * B + bg + lane;
 #pragma unroll
           for (int j = 0; j < NB; ++j)
             if (ok[j]) k[j] = cfma(cf, cv<T>(yin[rb + 32 * j]), k[j]);
         } else {
+          const int d = st.dn_aux[p], m = st.dn_mode[p];
           const int base = st.mode_lop[m] * (S + 1);
           const int q0 = st.lh_ptr[base + s], q1 = st.lh_ptr[base + s + 1];
           for (int q = q0; q < q1; ++q) {
@@ -895,7 +906,8 @@ static void launch_wide(const hops_structure* st, int B, int stage, double h, co
 template <typename R, typename ST, typename PT, bool SITE>
 static void launch_stage(const hops_structure* st, int B, int stage, double h, const void* yin,
                          void* yout, void* phi, void* shadow, void* acc, const double* ws,
-                         cudaStream_t s) {
+                         int32_t* status, cudaStream_t s) {
+  (void)status;
   if (B >= 32) {
     const int nbmax = (B + 31) / 32;
     // auto (measured on the 20-site ring, 128 trajectories): 64 trajectories
@@ -921,7 +933,7 @@ static void launch_stage(const hops_structure* st, int B, int stage, double h, c
 template <typename R, typename ST, typename PT>
 static int run_stage(const hops_structure* st, int B, int stage, double h, const void* yin,
                      void* yout, void* phi, void* shadow, void* acc, const double* ws,
-                     cudaStream_t s) {
+                     int32_t* status, cudaStream_t s) {
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (g_timing) {
     e0 = timing_event();
@@ -929,9 +941,9 @@ static int run_stage(const hops_structure* st, int B, int stage, double h, const
     if (e0) cudaEventRecord(e0, s);
   }
   if (st->site_projector)
-    launch_stage<R, ST, PT, true>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, s);
+    launch_stage<R, ST, PT, true>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, status, s);
   else
-    launch_stage<R, ST, PT, false>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, s);
+    launch_stage<R, ST, PT, false>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, status, s);
   LAUNCH_CHECK();
   if (g_timing && e1) cudaEventRecord(e1, s);
   return HOPS_OK;
@@ -962,7 +974,8 @@ static int propagate_impl(const hops_structure* st, hops_batch* bt, int32_t it0,
       k_scalars<R, ST, PT><<<B, 128, smem, s>>>(*st, *bt, i, it, h, yin, recompute, psi_prev,
                                                 nullptr, nullptr, nullptr);
       LAUNCH_CHECK();
-      int rc = run_stage<R, ST, PT>(st, B, i, h, yin, yout, bt->phi, shadow, bt->acc, bt->work, s);
+      int rc = run_stage<R, ST, PT>(st, B, i, h, yin, yout, bt->phi, shadow, bt->acc, bt->work,
+                                    bt->status, s);
       if (rc) return rc;
     }
   }
@@ -1028,7 +1041,7 @@ static int dsys_impl(const hops_structure* st, hops_batch* bt, const float* z1, 
   // stage 4 reads the state itself (mixed mode: its complex64 copy)
   const void* yin = bt->precision == HOPS_PREC_MIXED ? bt->phi_lo : bt->phi;
   return run_stage<R, ST, PT>(st, bt->n_traj, 4, 0.0, yin, dphi, bt->phi, nullptr, bt->acc,
-                              bt->work, s);
+                              bt->work, bt->status, s);
 }
 
 extern "C" int hops_dsystem_dt(const hops_structure* st, hops_batch* bt, const float* z1_dev,

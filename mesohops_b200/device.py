@@ -82,7 +82,14 @@ def build_tables(system, basis, state_list=None, mode_list=None):
     l_ptr, l_col, l_val = _csr_of_dense(lops, S)
     lh_ptr, lh_col, lh_val = _csr_of_dense([np.conj(l.T) for l in lops], S)
     H = system.hamiltonian_dense()[ix]
-    h_ptr, h_col, h_val = _csr_of_dense([-1j * H], S)
+    if is_site:
+        # site-projector form: the diagonal of -iH joins the per-state diagonal
+        # coefficient; the CSR keeps the couplings only
+        h_diag = -1j * np.diag(H).astype(np.complex128)
+        h_ptr, h_col, h_val = _csr_of_dense([-1j * (H - np.diag(np.diag(H)))], S)
+    else:
+        h_diag = None
+        h_ptr, h_col, h_val = _csr_of_dense([-1j * H], S)
     G = system.G[modes]
     W = system.W[modes]
     counts = basis.counts
@@ -100,6 +107,8 @@ def build_tables(system, basis, state_list=None, mode_list=None):
     mode_site = site[mode_lop] if M else np.zeros(0, dtype=np.int32)
     mode_gwv = (G / W) * sval[mode_lop] if M else np.zeros(0, dtype=complex)
     dn_coef_site = dn_coef * np.conj(sval[mode_lop[dn_m]]) if len(dn_m) else np.zeros(0, complex)
+    up_site = mode_site[up_m] if len(up_m) else np.zeros(0, dtype=np.int32)
+    dn_site = mode_site[dn_m] if len(dn_m) else np.zeros(0, dtype=np.int32)
     up_counts = np.diff(basis.up_ptr)
     dn_counts = np.diff(basis.dn_ptr)
     return dict(
@@ -115,6 +124,8 @@ def build_tables(system, basis, state_list=None, mode_list=None):
         lop_active=lop_active, lop_site=site, lop_sval=sval,
         h_ptr=h_ptr, h_col=h_col, h_val=h_val, site_projector=int(is_site),
         mode_site=mode_site.astype(np.int32), mode_gwv=mode_gwv, dn_coef_site=dn_coef_site,
+        up_site=np.asarray(up_site, dtype=np.int32), dn_site=np.asarray(dn_site, dtype=np.int32),
+        h_diag=h_diag,
         max_up=int(up_counts.max()) if len(up_counts) else 0,
         max_dn=int(dn_counts.max()) if len(dn_counts) else 0,
     )
@@ -158,7 +169,10 @@ class DeviceStructure:
             ("mode_site", t["mode_site"].astype(i32)), ("mode_gwv", c2d(t["mode_gwv"])),
             ("mode_gwv_f", c2f(t["mode_gwv"])),
             ("dn_coef_site", c2d(t["dn_coef_site"])), ("dn_coef_site_f", c2f(t["dn_coef_site"])),
+            ("up_site", t["up_site"].astype(i32)), ("dn_site", t["dn_site"].astype(i32)),
         ]
+        if t["h_diag"] is not None:
+            fields.append(("h_diag", c2d(t["h_diag"])))
         offs = {}
         off = 0
         for name, arr in fields:

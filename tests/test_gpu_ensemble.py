@@ -86,3 +86,4 @@ def test_ensemble_derivative_matches_oracle(cuda_device):
         ref, rz = O.dsystem_dt(ob, phi[b], zm[b], z1[b], z2[b])
         assert np.max(np.abs(dphi[b] - ref)) <= 1e-12 * np.max(np.abs(ref))
         assert np.max(np.abs(dz[b] - rz)) <= 1e-12 * np.max(np.abs(rz))
+
