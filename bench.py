@@ -42,7 +42,14 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "complex64", "complex128"],
                     help="batched path: mixed = complex128 state with complex64 stage vectors")
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the plain/accuracy/e2e/CPU legs (profiling runs)")
+                    help="skip the plain/accuracy/e2e/CPU/served/adaptive legs (profiling runs)")
+    ap.add_argument("--no-served", action="store_true", help="skip the served-stream leg")
+    ap.add_argument("--no-adaptive", action="store_true", help="skip the adaptive-batch leg")
+    ap.add_argument("--served-requests", type=int, default=48)
+    ap.add_argument("--served-plain", type=int, default=6)
+    ap.add_argument("--served-budget-gb", type=float, default=32.0)
+    ap.add_argument("--adaptive-traj", type=int, default=512)
+    ap.add_argument("--adaptive-steps", type=int, default=6)
     return ap.parse_args()
 
 
@@ -220,9 +227,11 @@ def run_gpu(args):
     peak = peaks["hbm_gbs"] if peaks and "hbm_gbs" in peaks else 6650.0
     achieved = bytes_launch / (avg_ms / 1e3) / 1e9
     traffic = None
-    prof = os.path.join(ROOT, "profiles", f"k_stage_{args.workload}_traffic.json")
+    prof = os.path.join(ROOT, "profiles", f"k_wide_{args.workload}_{args.precision}.md")
     if os.path.exists(prof):
-        traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+        for line in open(prof):
+            if line.startswith("dram_bytes_per_launch:"):
+                traffic = int(line.split(":")[1])
     result["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                           "unit": "GB/s", "frac": round(achieved / peak, 4),
                           "traffic": traffic, "kernel": "k_stage (streaming RK4 stage)",
@@ -318,7 +327,109 @@ def extras(args, wl, sysp, ens, dev, value, K):
                   "note": "HopsEnsemble.propagate one step per call, noise window h2d "
                           "from pinned memory and psi d2h each step, host wall clock"}
     out["cpu_baseline"] = cpu_baseline(wl, sysp)
+    if not args.no_served:
+        out["served"] = served_leg(args, dev)
+    if not args.no_adaptive:
+        out["adaptive_batch"] = adaptive_leg(args, dev)
     return out
+
+
+def served_leg(args, dev):
+    """The served request stream (Poisson arrivals, mixed system and hierarchy
+    sizes, adaptive or not): its first ``--served-requests`` requests through
+    HopsServer (continuous batching, admission by HBM footprint), then the
+    first few completed ones again one at a time with the plain complex128
+    path."""
+    import torch
+    from mesohops_b200 import serving as sv
+    from mesohops_b200.trajectory import HopsTrajectory
+    from mesohops_b200.workloads import served_request, served_stream_specs
+    specs = served_stream_specs()[:args.served_requests]
+    reqs = [served_request(s) for s in specs]
+    free, _ = torch.cuda.mem_get_info(dev)
+    budget = int(min(0.6 * free, args.served_budget_gb * (1 << 30)))
+    srv = sv.HopsServer(device=dev, precision=args.precision, hbm_budget=budget,
+                        chunk_steps=32, realtime=True)
+    res = srv.serve(reqs)
+    summ = sv.summarize(res, srv.stats["makespan_s"])
+    kinds = {}
+    for r in res:
+        if r.status == "done":
+            kinds[r.kernel] = kinds.get(r.kernel, 0) + 1
+    # plain: the first completed requests one at a time, complex128, wall clock
+    n_plain, steps_plain, t_plain = 0, 0, 0.0
+    for r, q in zip(res, reqs):
+        if r.status != "done" or n_plain >= args.served_plain:
+            continue
+        h = HopsTrajectory(q.system_param, eom_param=q.eom_param, noise_param=q.noise_param,
+                           hierarchy_param=q.hierarchy_param, storage_param={},
+                           device_param={"PRECISION": "complex128", "DEVICE": str(dev)})
+        if q.adaptive is not None:
+            h.make_adaptive(q.adaptive[0], q.adaptive[1])
+        h.initialize(q.psi0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        h.propagate(q.t_max, q.dt)
+        torch.cuda.synchronize()
+        t_plain += time.perf_counter() - t0
+        steps_plain += q.n_steps
+        n_plain += 1
+    return {
+        "stream": f"first {len(reqs)} of the 4096-request stream (seed 4): Poisson arrivals "
+                  "(mean 2 ms), chains of 2-200 sites, depth 3-8, adaptive by a fair coin",
+        "precision": args.precision, "hbm_budget_bytes": budget,
+        "completed": summ["completed"], "rejected": summ["rejected"], "errors": summ["errors"],
+        "by_kernel": kinds, "traj_steps": summ["traj_steps"],
+        "traj_steps_per_s": round(summ["traj_steps_per_s"], 2),
+        "p50_ms": round(summ["p50_ms"], 1) if summ["p50_ms"] is not None else None,
+        "p99_ms": round(summ["p99_ms"], 1) if summ["p99_ms"] is not None else None,
+        "makespan_s": round(summ["makespan_s"], 2),
+        "plain_c128": {"requests": n_plain, "traj_steps_per_s":
+                       round(steps_plain / t_plain, 2) if t_plain > 0 else None,
+                       "note": "the first completed requests again, one at a time, "
+                               "HopsTrajectory complex128, propagate wall clock"},
+        "latency": "completion minus arrival, wall clock of the serving loop"}
+
+
+def adaptive_leg(args, dev):
+    """Adaptive HOPS with uneven bases: the 500-site chain, depth 10,
+    delta = 1e-3, many trajectories stepped in lock-step -- every RK4 step of
+    all of them in one persistent resident-kernel launch (each with its own
+    basis), every flux-error evaluation in one launch."""
+    import torch
+    from mesohops_b200 import adaptive as ad
+    from mesohops_b200.trajectory import HopsTrajectory
+    from mesohops_b200.workloads import adaptive_chain500
+    n, K = args.adaptive_traj, args.adaptive_steps
+    sysp, psi0, seeds = adaptive_chain500(n)
+    dt = 4.0
+    trajs = []
+    t0 = time.perf_counter()
+    for sd in seeds:
+        h = HopsTrajectory(sysp, noise_param={"SEED": sd, "MODEL": "FFT_FILTER",
+                                              "TLEN": (K + 8) * dt, "TAU": dt / 2},
+                           hierarchy_param={"MAXHIER": 10}, storage_param={},
+                           device_param={"PRECISION": args.precision, "DEVICE": str(dev)})
+        h.make_adaptive(1e-3, 1e-3, update_step=1)
+        h.initialize(psi0)
+        trajs.append(h)
+    t_init = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(K):
+        ad.drive_many([h.adaptive_step_gen((k + 1) * dt, dt, k) for h in trajs], dev)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    sizes = np.array([h.n_hier * h.n_state for h in trajs])
+    return {"workload": "500-site chain (J=50, eps~N(0,100) seed 3), DL (50,50,295 K) per "
+                        "site, depth 10, delta_a = delta_s = 1e-3, dt = 4 fs, psi_0 on a "
+                        f"seeded site; {n} trajectories (noise seeds 0..{n - 1})",
+            "steps": K, "traj_steps_per_s": round(n * K / el, 2),
+            "basis_elems": {"min": int(sizes.min()), "median": int(np.median(sizes)),
+                            "max": int(sizes.max())},
+            "init_s": round(t_init, 2), "precision": args.precision,
+            "note": f"first {K} steps (inch-worm early integrator included); host wall clock "
+                    "of lock-step stepping, one resident launch per step for all trajectories"}
 
 
 # ------------------------------------------------------------- CPU legs --

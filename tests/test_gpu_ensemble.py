@@ -87,3 +87,35 @@ def test_ensemble_derivative_matches_oracle(cuda_device):
         assert np.max(np.abs(dphi[b] - ref)) <= 1e-12 * np.max(np.abs(ref))
         assert np.max(np.abs(dz[b] - rz)) <= 1e-12 * np.max(np.abs(rz))
 
+
+
+def run_forced(f, B, precision, noise, n_steps, tuning):
+    """Ensemble run with a fixed stage-kernel shape (nb, chunk_major)."""
+    import torch
+    from mesohops_b200 import HopsEnsemble
+    ens = HopsEnsemble(golden_system(f), B,
+                       noise_param={"SEED": noise, "MODEL": "PRE_CALCULATED",
+                                    "TLEN": float(f["tlen"]), "TAU": float(f["tau_noise"])},
+                       hierarchy_param={"MAXHIER": int(f["depth"])}, precision=precision,
+                       autotune=False)
+    ens.initialize(f["psi0"])
+    ens.batch.tuning = tuning
+    dt = float(f["dt"])
+    psi = torch.empty((n_steps, B, ens.n_state), dtype=torch.complex128, device="cuda")
+    ens.propagate(n_steps * dt, dt, psi_out=psi)
+    ens.check()
+    return psi.cpu().numpy()
+
+
+
+@pytest.mark.parametrize("name", ["ring6", "chain4_2mode"])
+@pytest.mark.parametrize("B", [40, 96])
+@pytest.mark.parametrize("tuning", [(1, 0), (1, 1), (4, 0), (4, 1), (8, 1)])
+def test_stage_kernel_shapes_agree(cuda_device, name, B, tuning):
+    """Every stage-kernel shape the autotuner may pick gives the same numbers."""
+    f = load_golden(name)
+    n_steps = 8
+    noise = ensemble_noise(f, B, 11)
+    ref = run_forced(f, B, "complex128", noise, n_steps, (2, 0))
+    got = run_forced(f, B, "complex128", noise, n_steps, tuning)
+    assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref))
