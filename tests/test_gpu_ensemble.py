@@ -109,7 +109,7 @@ def run_forced(f, B, precision, noise, n_steps, tuning):
 
 
 @pytest.mark.parametrize("name", ["ring6", "chain4_2mode"])
-@pytest.mark.parametrize("B", [40, 96])
+@pytest.mark.parametrize("B", [40, 64, 96])
 @pytest.mark.parametrize("tuning", [(1, 0), (1, 1), (4, 0), (4, 1), (8, 1)])
 def test_stage_kernel_shapes_agree(cuda_device, name, B, tuning):
     """Every stage-kernel shape the autotuner may pick gives the same numbers."""
