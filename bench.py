@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--served-budget-gb", type=float, default=32.0)
     ap.add_argument("--adaptive-traj", type=int, default=512)
     ap.add_argument("--adaptive-steps", type=int, default=6)
+    ap.add_argument("--workers", type=int, default=-1,
+                    help="adaptive worker processes (-1: min(12, cores - 4))")
     return ap.parse_args()
 
 
@@ -348,9 +350,14 @@ def served_leg(args, dev):
     reqs = [served_request(s) for s in specs]
     free, _ = torch.cuda.mem_get_info(dev)
     budget = int(min(0.6 * free, args.served_budget_gb * (1 << 30)))
+    workers = args.workers if args.workers >= 0 else max(0, min(12, (os.cpu_count() or 2) - 4))
     srv = sv.HopsServer(device=dev, precision=args.precision, hbm_budget=budget,
-                        chunk_steps=32, realtime=True)
-    res = srv.serve(reqs)
+                        chunk_steps=32, realtime=True, adaptive_workers=workers)
+    start_s = srv.pool.start_s if srv.pool is not None else 0.0
+    try:
+        res = srv.serve(reqs)
+    finally:
+        srv.close()
     summ = sv.summarize(res, srv.stats["makespan_s"])
     kinds = {}
     for r in res:
@@ -378,6 +385,7 @@ def served_leg(args, dev):
         "stream": f"first {len(reqs)} of the 4096-request stream (seed 4): Poisson arrivals "
                   "(mean 2 ms), chains of 2-200 sites, depth 3-8, adaptive by a fair coin",
         "precision": args.precision, "hbm_budget_bytes": budget,
+        "adaptive_worker_processes": workers,
         "completed": summ["completed"], "rejected": summ["rejected"], "errors": summ["errors"],
         "by_kernel": kinds, "traj_steps": summ["traj_steps"],
         "traj_steps_per_s": round(summ["traj_steps_per_s"], 2),
@@ -393,43 +401,56 @@ def served_leg(args, dev):
 
 def adaptive_leg(args, dev):
     """Adaptive HOPS with uneven bases: the 500-site chain, depth 10,
-    delta = 1e-3, many trajectories stepped in lock-step -- every RK4 step of
-    all of them in one persistent resident-kernel launch (each with its own
-    basis), every flux-error evaluation in one launch."""
-    import torch
-    from mesohops_b200 import adaptive as ad
-    from mesohops_b200.trajectory import HopsTrajectory
+    delta = 1e-3, many trajectories spread over worker processes on the GPU;
+    each worker steps its share in lock-step -- every RK4 step of all of them
+    in one persistent resident-kernel launch (each with its own basis), every
+    flux-error evaluation in one launch."""
+    from mesohops_b200.adaptive_pool import AdaptiveWorkers
+    from mesohops_b200.serving import TrajectoryRequest
     from mesohops_b200.workloads import adaptive_chain500
     n, K = args.adaptive_traj, args.adaptive_steps
     sysp, psi0, seeds = adaptive_chain500(n)
     dt = 4.0
-    trajs = []
-    t0 = time.perf_counter()
-    for sd in seeds:
-        h = HopsTrajectory(sysp, noise_param={"SEED": sd, "MODEL": "FFT_FILTER",
-                                              "TLEN": (K + 8) * dt, "TAU": dt / 2},
-                           hierarchy_param={"MAXHIER": 10}, storage_param={},
-                           device_param={"PRECISION": args.precision, "DEVICE": str(dev)})
-        h.make_adaptive(1e-3, 1e-3, update_step=1)
-        h.initialize(psi0)
-        trajs.append(h)
-    t_init = time.perf_counter() - t0
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for k in range(K):
-        ad.drive_many([h.adaptive_step_gen((k + 1) * dt, dt, k) for h in trajs], dev)
-    torch.cuda.synchronize()
-    el = time.perf_counter() - t0
-    sizes = np.array([h.n_hier * h.n_state for h in trajs])
+    workers = args.workers if args.workers >= 0 else max(1, min(12, (os.cpu_count() or 2) - 4))
+    workers = max(1, workers)
+    pool = AdaptiveWorkers(workers, dev, args.precision)
+    try:
+        t0 = time.perf_counter()
+        for sd in seeds:
+            pool.submit(sd, TrajectoryRequest(
+                sd, sysp, psi0, K * dt, dt, hierarchy_param={"MAXHIER": 10},
+                eom_param={"EQUATION_OF_MOTION": "NORMALIZED NONLINEAR"},
+                noise_param={"SEED": sd, "MODEL": "FFT_FILTER", "TLEN": (K + 8) * dt,
+                             "TAU": dt / 2},
+                adaptive=(1e-3, 1e-3)))
+        errors = []
+        while any(pool.building):
+            for ev in pool.events(timeout=1.0):
+                errors.extend(ev[2])
+        t_init = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        pool.step_idle(K)
+        done = []
+        while any(pool.stepping):
+            for ev in pool.events(timeout=1.0):
+                done.extend(ev[1])
+                errors.extend(ev[2])
+        el = time.perf_counter() - t0
+    finally:
+        pool.close()
+    sizes = np.array([d[3] * d[4] for d in done]) if done else np.zeros(1)
     return {"workload": "500-site chain (J=50, eps~N(0,100) seed 3), DL (50,50,295 K) per "
                         "site, depth 10, delta_a = delta_s = 1e-3, dt = 4 fs, psi_0 on a "
                         f"seeded site; {n} trajectories (noise seeds 0..{n - 1})",
-            "steps": K, "traj_steps_per_s": round(n * K / el, 2),
-            "basis_elems": {"min": int(sizes.min()), "median": int(np.median(sizes)),
-                            "max": int(sizes.max())},
-            "init_s": round(t_init, 2), "precision": args.precision,
-            "note": f"first {K} steps (inch-worm early integrator included); host wall clock "
-                    "of lock-step stepping, one resident launch per step for all trajectories"}
+            "steps": K, "completed": len(done), "errors": len(errors),
+            "traj_steps_per_s": round(len(done) * K / el, 2),
+            "basis_elems_end": {"min": int(sizes.min()), "median": int(np.median(sizes)),
+                                "max": int(sizes.max())},
+            "worker_processes": workers, "init_s": round(t_init, 2),
+            "precision": args.precision,
+            "note": f"first {K} steps (inch-worm early integrator included), wall clock of "
+                    "the stepping; each worker process steps its trajectories in lock-step "
+                    "with one resident launch per step for all of them"}
 
 
 # ------------------------------------------------------------- CPU legs --

@@ -132,21 +132,22 @@ def serve_steps(reqs, device):
     out = [None] * len(reqs)
     res = [i for i, r in enumerate(reqs) if r.driver.kernel == "resident"]
     if res:
-        trajs, it0s, dis, hs = [], [], [], []
+        trajs, phis, zms, it0s, dis, hs = [], [], [], [], [], []
         for i in res:
             r = reqs[i]
             d = r.driver
             b = d.basis
-            d.engine.set_state(r.phi, r.zmem_abs[b.modes] if b.n_mode else None)
             trajs.append(d.engine)
+            phis.append(r.phi)
+            zms.append(r.zmem_abs[b.modes] if b.n_mode else None)
             it0s.append(d.noise_index(r.t))
             dis.append(d.noise_di(r.tau))
             hs.append(r.tau / hbar)
-        st = ResidentRunner(device).run(trajs, it0s, dis, 1, hs)
+        st, phis_o, zms_o = ResidentRunner(device).run_packed(trajs, phis, zms, it0s, dis, 1, hs)
         if np.any(st != 0):
             raise TrajectoryError("non-finite state during adaptive propagation")
-        for i in res:
-            out[i] = reqs[i].driver.engine.get_state()
+        for j, i in enumerate(res):
+            out[i] = (phis_o[j], zms_o[j])
     for i, r in enumerate(reqs):
         if out[i] is not None:
             continue
@@ -162,61 +163,80 @@ def serve_steps(reqs, device):
     return [r.driver.finish_step(r, phi, zrel) for r, (phi, zrel) in zip(reqs, out)]
 
 
+def _pack(arrays):
+    """Byte-pack numpy arrays at 16-byte aligned offsets: (buffer, offsets)."""
+    offs, total = [], 0
+    for a in arrays:
+        offs.append(total)
+        total += (a.nbytes + 15) // 16 * 16
+    buf = np.zeros(max(total, 16), dtype=np.uint8)
+    for a, o in zip(arrays, offs):
+        buf[o:o + a.nbytes] = np.ascontiguousarray(a).view(np.uint8).ravel()
+    return buf, offs
+
+
 def serve_flux(reqs, device):
-    """Every FluxRequest in ONE hops_flux_errors launch (one CTA per request)."""
+    """Every FluxRequest in ONE hops_flux_errors launch (one CTA per request);
+    all inputs go up in one copy and all error arrays come back in one."""
     n = len(reqs)
     if n == 0:
         return []
     dev = torch.device(device)
     L = _lib.lib()
-    keep = []
+    host = []
+    shapes = []
+    out_doubles = 0
+    for r in reqs:
+        b = r.driver.basis
+        N, S, M = b.n_hier, b.n_state, b.n_mode
+        host.append(np.ascontiguousarray(r.phi, dtype=np.complex128))
+        host.append(np.ascontiguousarray(r.z_step[2][b.modes] if M else np.zeros(1),
+                                         dtype=np.complex128))
+        host.append(np.ascontiguousarray(r.z_step[0], dtype=np.complex64))
+        host.append(np.ascontiguousarray(r.z_step[1], dtype=np.complex64))
+        host.append(np.ascontiguousarray(r.mask if r.mask is not None else np.zeros(1),
+                                         dtype=np.int32))
+        host.append(b.k_aux.ravel() if b.k_aux.size else np.zeros(1, np.uint8))
+        n_out = N * S + (2 * max(M * N, 1) if r.with_flux else 0)
+        shapes.append((N, S, M, out_doubles))
+        out_doubles += (n_out + 1) // 2 * 2
+    buf, offs = _pack(host)
+    dbuf = torch.from_numpy(buf).to(dev)
+    dout = torch.empty(max(out_doubles, 2), dtype=torch.float64, device=dev)
+    base, obase = dbuf.data_ptr(), dout.data_ptr()
     tasks = (HopsFluxTask * n)()
-    outs = []
     max_smem = 0
     for i, r in enumerate(reqs):
         b = r.driver.basis
-        N, S, M = b.n_hier, b.n_state, b.n_mode
-        phi_d = torch.from_numpy(np.ascontiguousarray(r.phi, dtype=np.complex128)).to(dev)
-        zm = r.z_step[2][b.modes] if M else np.zeros(1, dtype=np.complex128)
-        zm_d = torch.from_numpy(np.ascontiguousarray(zm, dtype=np.complex128)).to(dev)
-        z1_d = torch.from_numpy(np.ascontiguousarray(r.z_step[0], dtype=np.complex64)).to(dev)
-        z2_d = torch.from_numpy(np.ascontiguousarray(r.z_step[1], dtype=np.complex64)).to(dev)
-        mask_d = (torch.from_numpy(np.ascontiguousarray(r.mask, dtype=np.int32)).to(dev)
-                  if r.mask is not None else None)
-        k_d = torch.from_numpy(np.ascontiguousarray(b.k_aux).ravel()
-                               if b.k_aux.size else np.zeros(1, np.uint8)).to(dev)
-        e_deriv = torch.empty(N * S, dtype=torch.float64, device=dev)
-        e_up = torch.empty(max(M * N, 1), dtype=torch.float64, device=dev) if r.with_flux else None
-        e_dn = torch.empty(max(M * N, 1), dtype=torch.float64, device=dev) if r.with_flux else None
-        keep += [phi_d, zm_d, z1_d, z2_d, mask_d, k_d]
+        N, S, M, o = shapes[i]
         tk = tasks[i]
         tk.st = b.dstruct.dev_ptr
-        tk.phi = phi_d.data_ptr()
-        tk.zmem = zm_d.data_ptr()
-        tk.z1 = z1_d.data_ptr()
-        tk.z2 = z2_d.data_ptr()
-        tk.aux_mask = mask_d.data_ptr() if mask_d is not None else None
-        tk.e_deriv = e_deriv.data_ptr()
-        tk.e_up = e_up.data_ptr() if e_up is not None else None
-        tk.e_down = e_dn.data_ptr() if e_dn is not None else None
-        tk.k_aux = k_d.data_ptr()
+        tk.phi = base + offs[6 * i]
+        tk.zmem = base + offs[6 * i + 1]
+        tk.z1 = base + offs[6 * i + 2]
+        tk.z2 = base + offs[6 * i + 3]
+        tk.aux_mask = base + offs[6 * i + 4] if r.mask is not None else None
+        tk.k_aux = base + offs[6 * i + 5]
+        tk.e_deriv = obase + 8 * o
+        tk.e_up = obase + 8 * (o + N * S) if r.with_flux else None
+        tk.e_down = obase + 8 * (o + N * S + max(M * N, 1)) if r.with_flux else None
         tk.dt = float(r.dt)
         tk.eom = EOM_CODES[r.driver.eom]
         max_smem = max(max_smem, int(L.hops_flux_errors_smem_doubles(S, M, b.tables["n_lop"])))
-        outs.append((e_deriv, e_up, e_dn, N, S, M))
     raw = torch.from_numpy(np.frombuffer(bytes(tasks), dtype=np.uint8).copy()).to(dev)
     stream = torch.cuda.current_stream(dev).cuda_stream
     rc = L.hops_flux_errors(raw.data_ptr(), n, max_smem, hbar, stream)
     _lib.check(rc, "hops_flux_errors")
+    hout = dout.cpu().numpy()
     res = []
-    for (ed, eu, edn, N, S, M) in outs:
-        e1 = ed.cpu().numpy().reshape(N, S)
-        if eu is None:
+    for r, (N, S, M, o) in zip(reqs, shapes):
+        e1 = hout[o:o + N * S].reshape(N, S)
+        if not r.with_flux:
             res.append((e1, None, None))
-        else:
-            res.append((e1, eu.cpu().numpy()[:M * N].reshape(M, N),
-                        edn.cpu().numpy()[:M * N].reshape(M, N)))
-    del keep
+            continue
+        q = o + N * S
+        mn = max(M * N, 1)
+        res.append((e1, hout[q:q + M * N].reshape(M, N), hout[q + mn:q + mn + M * N].reshape(M, N)))
     return res
 
 
@@ -540,20 +560,24 @@ class AdaptiveHops:
         # construct_filter_state_stable_down / _up (hops_fluxfilters.py:218-302)
         F_down = np.zeros((M, N), dtype=bool)
         F_up = np.zeros((M, N), dtype=bool)
-        for v in bound_aux:
-            v = np.asarray(v, dtype=np.int16)
-            if M and int(v.sum()) < self.maxhier:
-                ups = np.repeat(v.reshape(1, -1), M, axis=0)
-                ups[np.arange(M), b.modes] += 1
-                idx = b.aux.index_of(ups)
-                ok = idx >= 0
-                F_down[np.nonzero(ok)[0], idx[ok]] = True
-            for mabs in np.nonzero(v)[0]:
-                d = v.copy()
-                d[mabs] -= 1
-                idx = int(b.aux.index_of(d.reshape(1, -1))[0])
-                if idx >= 0:
-                    F_up[b.rel_mode[int(mabs)], idx] = True
+        V = np.asarray(bound_aux, dtype=np.int16).reshape(-1, self.system.n_mode)
+        if len(V) and M:
+            # aux one step up from each boundary aux along every basis mode
+            low = V[V.sum(axis=1) < self.maxhier]
+            if len(low):
+                ups = np.repeat(low[:, None, :], M, axis=1)
+                ups[:, np.arange(M), b.modes] += 1
+                idx = b.aux.index_of(ups.reshape(-1, self.system.n_mode)).reshape(len(low), M)
+                vi, mi = np.nonzero(idx >= 0)
+                F_down[mi, idx[vi, mi]] = True
+            # aux one step down from each boundary aux along its own modes
+            vi, mabs = np.nonzero(V)
+            downs = V[vi].copy()
+            downs[np.arange(len(vi)), mabs] -= 1
+            idx = b.aux.index_of(downs)
+            ok = idx >= 0
+            rel = np.array([b.rel_mode[int(m)] for m in mabs[ok]], dtype=np.int64)
+            F_up[rel, idx[ok]] = True
         absphi2 = np.abs(phi_sn) ** 2
         if M:
             avg = self._avg_L(phi[:S])

@@ -20,19 +20,20 @@ from ._lib import HopsStructure
 
 
 def _csr_of_dense(mats, n):
-    """CSR (absolute offsets) of a list of dense n x n complex matrices."""
+    """CSR (absolute offsets) of a list of dense n x n complex matrices: block j
+    occupies ptr[j*(n+1) : (j+1)*(n+1)], entries in row-major order."""
+    if len(mats) == 0:
+        return np.zeros(0, dtype=np.int32), np.zeros(0, np.int32), np.zeros(0, np.complex128)
+    A = np.asarray(mats, dtype=np.complex128).reshape(len(mats), n, n)
+    j, r, c = np.nonzero(A)
+    counts = np.zeros(len(mats) * n, dtype=np.int64)
+    np.add.at(counts, j * n + r, 1)
+    start = np.concatenate([[0], np.cumsum(counts)])
     ptr = np.zeros(len(mats) * (n + 1), dtype=np.int32)
-    cols, vals = [], []
-    off = 0
-    for j, A in enumerate(mats):
-        for r in range(n):
-            ptr[j * (n + 1) + r] = off
-            nz = np.nonzero(A[r])[0]
-            cols.extend(nz.tolist())
-            vals.extend(A[r, nz].tolist())
-            off += len(nz)
-        ptr[j * (n + 1) + n] = off
-    return ptr, np.array(cols, dtype=np.int32), np.array(vals, dtype=np.complex128)
+    rows = np.arange(len(mats) * n)
+    ptr[(rows // n) * (n + 1) + rows % n] = start[:-1]
+    ptr[np.arange(len(mats)) * (n + 1) + n] = start[(np.arange(len(mats)) + 1) * n]
+    return ptr, c.astype(np.int32), A[j, r, c]
 
 
 def _c2d(a):

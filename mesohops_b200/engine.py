@@ -248,9 +248,11 @@ class ResidentRunner:
         """
         return self.collect(self.launch(trajs, it0, di, n_steps, tau_over_hbar, psi_out))
 
-    def launch(self, trajs, it0, di, n_steps, tau_over_hbar, psi_out=None):
+    def launch(self, trajs, it0, di, n_steps, tau_over_hbar, psi_out=None, state_ptrs=None):
         """Enqueue the launch of ``run`` on the current stream and return a handle
-        for ``collect`` (nothing waits on the device here)."""
+        for ``collect`` (nothing waits on the device here).  state_ptrs: optional
+        per-trajectory (phi, z_mem) device addresses used instead of the
+        trajectories' own buffers (which then start unscaled)."""
         n = len(trajs)
         if n == 0:
             return None
@@ -265,8 +267,11 @@ class ResidentRunner:
         for i, tr in enumerate(trajs):
             tk = tasks[i]
             tk.st = tr.st.dev_ptr
-            tk.phi = tr.phi.data_ptr()
-            tk.zmem = tr.zmem.data_ptr()
+            if state_ptrs is not None:
+                tk.phi, tk.zmem = state_ptrs[i]
+            else:
+                tk.phi = tr.phi.data_ptr()
+                tk.zmem = tr.zmem.data_ptr()
             tk.noise1 = tr.noise1.data_ptr() if tr.noise1 is not None else None
             tk.noise2 = tr.noise2.data_ptr() if tr.noise2 is not None else None
             tk.n_t1 = tr.noise1.shape[-1] if tr.noise1 is not None else 0
@@ -282,7 +287,7 @@ class ResidentRunner:
             tk.eom = tr.eom
             tk.status = 0
             tk.tau_over_hbar = float(per(tau_over_hbar, i))
-            tk.scale = tr.scale
+            tk.scale = tr.scale if state_ptrs is None else 1.0
         raw = np.frombuffer(bytes(tasks), dtype=np.uint8).copy()
         tdev = torch.from_numpy(raw).to(self.dev)
         max_elems = max(t.N * t.S for t in trajs)
@@ -292,6 +297,38 @@ class ResidentRunner:
                                                 _stream(self.dev))
         _lib.check(rc, "hops_resident_propagate")
         return (trajs, tdev, torch.cuda.current_stream(self.dev))
+
+    def run_packed(self, trajs, phis, zmems, it0, di, n_steps, tau_over_hbar):
+        """``run`` with the states on the host: every trajectory's phi and z_mem
+        travel in one host->device copy each way (packed back to back) instead
+        of one per trajectory.  Returns (status, [phi], [z_mem]) with phi
+        already renormalised by the kernel."""
+        n = len(trajs)
+        prec = trajs[0].prec
+        pdt = trajs[0].phi.dtype
+        npdt = np.complex128 if pdt == torch.complex128 else np.complex64
+        sizes = [t.N * t.S for t in trajs]
+        zs = [max(t.M, 1) for t in trajs]
+        po = np.concatenate([[0], np.cumsum(sizes)])
+        zo = np.concatenate([[0], np.cumsum(zs)])
+        hphi = np.empty(po[-1], dtype=npdt)
+        hz = np.zeros(zo[-1], dtype=np.complex128)
+        for i, t in enumerate(trajs):
+            hphi[po[i]:po[i + 1]] = phis[i]
+            if t.M:
+                hz[zo[i]:zo[i] + t.M] = zmems[i]
+        dphi = torch.from_numpy(hphi).to(self.dev)
+        dz = torch.from_numpy(hz).to(self.dev)
+        isz = 16 if pdt == torch.complex128 else 8
+        views = []
+        for i, t in enumerate(trajs):
+            views.append((dphi.data_ptr() + int(po[i]) * isz, dz.data_ptr() + int(zo[i]) * 16))
+        handle = self.launch(trajs, it0, di, n_steps, tau_over_hbar, state_ptrs=views)
+        status = self.collect(handle)
+        ophi = dphi.cpu().numpy().astype(np.complex128)
+        oz = dz.cpu().numpy()
+        return (status, [ophi[po[i]:po[i + 1]] for i in range(n)],
+                [oz[zo[i]:zo[i] + t.M] for i, t in enumerate(trajs)])
 
     def collect(self, handle):
         """Wait for a launch and return its per-trajectory status array."""

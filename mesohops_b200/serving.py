@@ -188,11 +188,14 @@ class HopsServer:
     """Continuous-batching server for HOPS trajectories on one GPU."""
 
     def __init__(self, device="cuda:0", precision="mixed", hbm_budget=None, chunk_steps=32,
-                 builders=2, realtime=True, fairness_s=1.0):
+                 builders=2, realtime=True, fairness_s=1.0, adaptive_workers=0):
         """hbm_budget: device bytes the admitted requests may hold (default 80 %
         of the free memory).  realtime: honour the arrival times (False: every
         request is present at t = 0).  fairness_s: once the oldest waiting
-        request has waited this long, later ones are not admitted ahead of it."""
+        request has waited this long, later ones are not admitted ahead of it.
+        adaptive_workers: > 0 runs the adaptive requests in that many worker
+        processes on the same GPU (adaptive_pool.AdaptiveWorkers), so their
+        host-side basis updates run in parallel; 0 steps them in this process."""
         self.device = torch.device(device)
         self.precision = precision
         if hbm_budget is None:
@@ -204,6 +207,16 @@ class HopsServer:
         self.realtime = realtime
         self.fairness_s = float(fairness_s)
         self.stats = {}
+        self.pool = None
+        if adaptive_workers > 0:
+            from .adaptive_pool import AdaptiveWorkers
+            self.pool = AdaptiveWorkers(adaptive_workers, self.device, precision)
+
+    def close(self):
+        """Stop the adaptive worker processes (if any)."""
+        if self.pool is not None:
+            self.pool.close()
+            self.pool = None
 
     # --------------------------------------------------------------- building
     def _build(self, req, kernel):
@@ -244,7 +257,7 @@ class HopsServer:
         building = []           # (future, req, fp, kernel)
         active = []
         used = 0
-        pool = ThreadPoolExecutor(max_workers=max(1, self.builders))
+        builders = ThreadPoolExecutor(max_workers=max(1, self.builders))
         runner = ResidentRunner(self.device)
         s_res = torch.cuda.Stream(self.device)
         s_ad = torch.cuda.Stream(self.device)
@@ -256,8 +269,10 @@ class HopsServer:
         arrival = {r.rid: (r.arrival if self.realtime else 0.0) for r in reqs}
         n_ticks = 0
         busy = 0.0
+        pool = self.pool
+        pooled = {}       # rid -> (request, footprint, admitted time or None)
         try:
-            while pending or queue or building or active:
+            while pending or queue or building or active or pooled:
                 now = clock()
                 while pending and arrival[pending[0].rid] <= now:
                     queue.append(pending.popleft())
@@ -271,7 +286,13 @@ class HopsServer:
                 for req, fp, kern in admit:
                     queue.remove(req)
                     used += fp
-                    building.append((pool.submit(self._build, req, kern), req, fp, kern))
+                    if kern == "adaptive" and pool is not None:
+                        pool.submit(req.rid, req)
+                        pooled[req.rid] = [req, fp, None]
+                    else:
+                        building.append((builders.submit(self._build, req, kern), req, fp, kern))
+                if pool is not None and pooled:
+                    pool.step_idle(self.chunk)
                 # builds that finished become active
                 still = []
                 for fut, req, fp, kern in building:
@@ -290,10 +311,15 @@ class HopsServer:
                     else:
                         still.append((fut, req, fp, kern))
                 building = still
+                if pooled:
+                    for ev in pool.events(timeout=0.0 if (active or building) else 0.02):
+                        self._pool_event(ev, pooled, results, clock(), arrival)
+                    used = self._used(active, building, pooled, queue)
                 if not active:
                     if building:
-                        wait([b[0] for b in building], return_when=FIRST_COMPLETED)
-                    elif pending and not queue:
+                        wait([b[0] for b in building], return_when=FIRST_COMPLETED,
+                             timeout=0.02 if pooled else None)
+                    elif pending and not queue and not pooled:
                         gap = arrival[pending[0].rid] - clock()
                         if gap > 0:
                             time.sleep(gap)
@@ -311,12 +337,37 @@ class HopsServer:
                         keep.append(a)
                 active = keep
         finally:
-            pool.shutdown(wait=True)
+            builders.shutdown(wait=True)
         self.stats = {"ticks": n_ticks, "tick_s": busy, "makespan_s": clock()}
         out = [results[r.rid] for r in sorted(requests, key=lambda r: order[r.rid])]
         for r in out:
             r.arrival = arrival[r.rid]
         return out
+
+    @staticmethod
+    def _used(active, building, pooled, queue):
+        return (sum(a.fp for a in active) + sum(b[2] for b in building)
+                + sum(v[1] for v in pooled.values()))
+
+    def _pool_event(self, ev, pooled, results, now, arrival):
+        """Book-keeping of one adaptive-worker reply."""
+        if ev[0] == "added":
+            for rid in ev[1]:
+                if rid in pooled:
+                    pooled[rid][2] = now
+            for rid, text in ev[2]:
+                req, fp, _ = pooled.pop(rid)
+                results[rid] = ServedResult(req, "error", text, footprint=fp)
+        elif ev[0] == "stepped":
+            for rid, psi, t_axis, _, _ in ev[1]:
+                req, fp, adm = pooled.pop(rid)
+                results[rid] = ServedResult(req, "done", t_axis=t_axis, psi_traj=psi,
+                                            admitted=adm, completed=now, footprint=fp,
+                                            kernel="adaptive")
+            for rid, text in ev[2]:
+                if rid in pooled:
+                    req, fp, _ = pooled.pop(rid)
+                    results[rid] = ServedResult(req, "error", text, footprint=fp)
 
     def _tick(self, active, runner, s_res, s_ad):
         res = [a for a in active if a.kernel == "resident"]

@@ -140,3 +140,21 @@ def test_rejected_requests_get_a_status():
     big = _req(7, _chain(200, 9), 8, 10)
     res = sv.HopsServer(precision="mixed", hbm_budget=1 << 30, realtime=False).serve([big])[0]
     assert res.status == "rejected" and "footprint" in res.reason
+
+
+@pytest.mark.gpu
+def test_adaptive_worker_processes_give_the_same_results():
+    """Adaptive requests stepped by worker processes equal the in-process server."""
+    mix = _mix()
+    local = sv.HopsServer(precision="complex128", hbm_budget=4 << 30, chunk_steps=16,
+                          realtime=False).serve(mix)
+    srv = sv.HopsServer(precision="complex128", hbm_budget=4 << 30, chunk_steps=16,
+                        realtime=False, adaptive_workers=2)
+    try:
+        pooled = srv.serve(_mix())
+    finally:
+        srv.close()
+    for a, b in zip(local, pooled):
+        assert a.status == b.status == "done"
+        assert a.kernel == b.kernel
+        assert np.max(np.abs(a.psi_traj - b.psi_traj)) <= 1e-12
