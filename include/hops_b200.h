@@ -228,6 +228,29 @@ int hops_flux_errors(hops_flux_task* tasks_dev, int32_t n_tasks, int32_t max_sme
                      double hbar, void* stream);
 int32_t hops_flux_errors_smem_doubles(int32_t n_state, int32_t n_mode, int32_t n_lop);
 
+/*
+ * Structure builder for a full triangular hierarchy (every aux of depth
+ * <= depth over n_mode modes, no static filters), replacing the host-side
+ * construction of the aux list, its connections (hops_hierarchy.py:340-368,
+ * 470-523) and K2_k (eom_hops_ksuper.py:36-90).  Aux g is the g-th multiset in
+ * (size, lexicographic) order.  binom_dev: int64 C(n, j) for n <= n_mode +
+ * depth + 1, j <= depth + 1, row stride depth + 2.
+ * pass1: k_decay_dev[g] = -sum_m k_m(g) w_m (complex128, w_dev [n_mode]) and
+ *        dn_count_dev[g] = number of distinct modes of g.
+ * pass2: dn_ptr_dev = exclusive prefix sum of dn_count (n_hier + 1 entries,
+ *        from the caller); writes the n_below * n_mode up connections of the
+ *        aux of depth < depth (aux g, mode m at g * n_mode + m) and, per aux,
+ *        its down connections in increasing mode order with k_m(g).
+ */
+int32_t hops_tri_max_depth(void);
+int hops_tri_pass1(int32_t n_mode, int32_t depth, const int64_t* binom_dev, int64_t n_hier,
+                   const double* w_dev, double* k_decay_dev, int32_t* dn_count_dev,
+                   void* stream);
+int hops_tri_pass2(int32_t n_mode, int32_t depth, const int64_t* binom_dev, int64_t n_hier,
+                   int64_t n_below, const int32_t* dn_ptr_dev, int32_t* up_aux_dev,
+                   int32_t* up_mode_dev, int32_t* dn_aux_dev, int32_t* dn_mode_dev,
+                   int32_t* dn_k_dev, void* stream);
+
 /* Shared-memory doubles of per-stage scalars one resident task needs. */
 int32_t hops_resident_scalar_doubles(int32_t n_state, int32_t n_mode, int32_t n_lop);
 

@@ -108,6 +108,10 @@ def lib():
                                              _i, _p, _i, _i, _i, _i, C.c_double, _p, _p, _p]
     L.hops_stage_tuning.argtypes = [_i, _i]
     L.hops_flux_errors.argtypes = [_p, _i, _i, C.c_double, _p]
+    L.hops_tri_max_depth.restype = _i
+    L.hops_tri_max_depth.argtypes = []
+    L.hops_tri_pass1.argtypes = [_i, _i, _p, C.c_int64, _p, _p, _p, _p]
+    L.hops_tri_pass2.argtypes = [_i, _i, _p, C.c_int64, C.c_int64, _p, _p, _p, _p, _p, _p, _p]
     L.hops_flux_errors_smem_doubles.restype = _i
     L.hops_flux_errors_smem_doubles.argtypes = [_i, _i, _i]
     L.hops_kernel_timing.argtypes = [C.c_int]
@@ -136,4 +140,5 @@ def exported_symbols():
             "hops_noise_filter", "hops_noise_filter_work_doubles", "hops_kernel_timing",
             "hops_kernel_timing_read", "hops_noalloc_scratch_bytes",
             "hops_rk4_propagate_noalloc", "hops_stage_tuning", "hops_flux_errors",
-            "hops_flux_errors_smem_doubles"]
+            "hops_flux_errors_smem_doubles", "hops_tri_max_depth", "hops_tri_pass1",
+            "hops_tri_pass2"]

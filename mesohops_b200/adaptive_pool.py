@@ -31,6 +31,10 @@ def _worker(conn, device, precision):
     from .trajectory import HopsTrajectory
     torch.set_num_threads(1)
     torch.cuda.set_device(torch.device(device))
+    torch.zeros(1, device=device)          # create the CUDA context before reporting ready
+    from . import _lib
+    _lib.lib()
+    conn.send(("ready",))
     live = {}   # key -> [traj, request, steps done]
     while True:
         msg = conn.recv()
@@ -98,6 +102,9 @@ class AdaptiveWorkers:
             p.start()
             self.conns.append(a)
             self.procs.append(p)
+        for c in self.conns:                    # every worker has its CUDA context
+            if c.recv()[0] != "ready":
+                raise RuntimeError("adaptive worker failed to start")
         self.load = [0] * len(self.conns)      # trajectories owned
         self.building = [0] * len(self.conns)  # add messages not yet answered
         self.stepping = [False] * len(self.conns)

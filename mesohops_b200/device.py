@@ -12,6 +12,7 @@ The arrays encode the super-operators of eom/eom_hops_ksuper.py:36-230:
 from __future__ import annotations
 
 import ctypes as C
+from math import comb
 
 import numpy as np
 import torch
@@ -47,6 +48,24 @@ def _c2f(a):
     return a.view(np.float32).copy() if a.size else np.zeros(2, dtype=np.float32)
 
 
+def _c2d_any(a):
+    if isinstance(a, torch.Tensor):
+        return torch.view_as_real(a.to(torch.complex128).contiguous()).reshape(-1)
+    return _c2d(a)
+
+
+def _c2f_any(a):
+    if isinstance(a, torch.Tensor):
+        return torch.view_as_real(a.to(torch.complex64).contiguous()).reshape(-1)
+    return _c2f(a)
+
+
+def _i32_any(a):
+    if isinstance(a, torch.Tensor):
+        return a.to(torch.int32)
+    return np.asarray(a).astype(np.int32)
+
+
 def build_tables(system, basis, state_list=None, mode_list=None):
     """Host arrays of one basis.
 
@@ -57,6 +76,45 @@ def build_tables(system, basis, state_list=None, mode_list=None):
     S_abs = system.n_state
     states = np.arange(S_abs) if state_list is None else np.asarray(state_list, dtype=np.int64)
     modes = basis.modes if mode_list is None else np.asarray(mode_list, dtype=np.int64)
+    small = _state_mode_tables(system, states, modes)
+    M = small["n_mode"]
+    mode_lop, sval = small["mode_lop"], small["lop_sval"]
+    W = small["mode_w"]
+    counts = basis.counts
+    # K2_k diagonal (eom_hops_ksuper.py:78-87): -aux . W over the aux's own modes
+    k_decay = -(counts[:, modes].astype(np.float64) @ W) if M else np.zeros(basis.n_hier)
+    # connections are along basis.modes; remap to the relative mode list
+    rel_of_basis_mode = {int(m): i for i, m in enumerate(modes)}
+    up_m = np.array([rel_of_basis_mode[int(basis.modes[m])] for m in basis.up_m], dtype=np.int32)
+    dn_m = np.array([rel_of_basis_mode[int(basis.modes[m])] for m in basis.dn_m], dtype=np.int32)
+    dn_coef = basis.dn_k.astype(np.float64) * W[dn_m] if len(dn_m) else np.zeros(0, complex)
+    first = [(a, rel_of_basis_mode[int(basis.modes[m])]) for (a, m) in basis.first_level()]
+    first_aux = np.array([a for a, _ in first], dtype=np.int32)
+    first_mode = np.array([m for _, m in first], dtype=np.int32)
+    mode_site = small["mode_site"]
+    dn_coef_site = dn_coef * np.conj(sval[mode_lop[dn_m]]) if len(dn_m) else np.zeros(0, complex)
+    up_site = mode_site[up_m] if len(up_m) else np.zeros(0, dtype=np.int32)
+    dn_site = mode_site[dn_m] if len(dn_m) else np.zeros(0, dtype=np.int32)
+    up_counts = np.diff(basis.up_ptr)
+    dn_counts = np.diff(basis.dn_ptr)
+    small.update(
+        n_hier=basis.n_hier,
+        k_decay=k_decay, up_ptr=basis.up_ptr.astype(np.int32),
+        up_aux=basis.up_u.astype(np.int32), up_mode=up_m,
+        dn_ptr=basis.dn_ptr.astype(np.int32), dn_aux=basis.dn_d.astype(np.int32),
+        dn_mode=dn_m, dn_coef=dn_coef,
+        first_aux=first_aux, first_mode=first_mode,
+        dn_coef_site=dn_coef_site,
+        up_site=np.asarray(up_site, dtype=np.int32), dn_site=np.asarray(dn_site, dtype=np.int32),
+        max_up=int(up_counts.max()) if len(up_counts) else 0,
+        max_dn=int(dn_counts.max()) if len(dn_counts) else 0,
+    )
+    return small
+
+
+def _state_mode_tables(system, states, modes):
+    """Tables that depend only on the state and mode bases: the relative L list
+    and its CSR forms, -iH, per-mode coefficients, the site-projector form."""
     S = len(states)
     M = len(modes)
     # relative L list: unique L of the basis modes, sorted (hops_modes.py:123-136)
@@ -93,43 +151,80 @@ def build_tables(system, basis, state_list=None, mode_list=None):
         h_ptr, h_col, h_val = _csr_of_dense([-1j * H], S)
     G = system.G[modes]
     W = system.W[modes]
-    counts = basis.counts
-    # K2_k diagonal (eom_hops_ksuper.py:78-87): -aux . W over the aux's own modes
-    k_decay = -(counts[:, modes].astype(np.float64) @ W) if M else np.zeros(basis.n_hier)
-    # connections are along basis.modes; remap to the relative mode list
-    rel_of_basis_mode = {int(m): i for i, m in enumerate(modes)}
-    up_m = np.array([rel_of_basis_mode[int(basis.modes[m])] for m in basis.up_m], dtype=np.int32)
-    dn_m = np.array([rel_of_basis_mode[int(basis.modes[m])] for m in basis.dn_m], dtype=np.int32)
-    dn_coef = basis.dn_k.astype(np.float64) * W[dn_m] if len(dn_m) else np.zeros(0, complex)
-    first = [(a, rel_of_basis_mode[int(basis.modes[m])]) for (a, m) in basis.first_level()]
-    first_aux = np.array([a for a, _ in first], dtype=np.int32)
-    first_mode = np.array([m for _, m in first], dtype=np.int32)
-    # site-projector coefficients per mode and per down connection
+    # site-projector coefficients per mode
     mode_site = site[mode_lop] if M else np.zeros(0, dtype=np.int32)
     mode_gwv = (G / W) * sval[mode_lop] if M else np.zeros(0, dtype=complex)
-    dn_coef_site = dn_coef * np.conj(sval[mode_lop[dn_m]]) if len(dn_m) else np.zeros(0, complex)
-    up_site = mode_site[up_m] if len(up_m) else np.zeros(0, dtype=np.int32)
-    dn_site = mode_site[dn_m] if len(dn_m) else np.zeros(0, dtype=np.int32)
-    up_counts = np.diff(basis.up_ptr)
-    dn_counts = np.diff(basis.dn_ptr)
     return dict(
-        n_hier=basis.n_hier, n_state=S, n_mode=M, n_lop=L,
-        states=states, modes=modes, l_abs=l_abs,
-        k_decay=k_decay, up_ptr=basis.up_ptr.astype(np.int32),
-        up_aux=basis.up_u.astype(np.int32), up_mode=up_m,
-        dn_ptr=basis.dn_ptr.astype(np.int32), dn_aux=basis.dn_d.astype(np.int32),
-        dn_mode=dn_m, dn_coef=dn_coef,
+        n_state=S, n_mode=M, n_lop=L, states=states, modes=modes, l_abs=l_abs,
         mode_lop=mode_lop, mode_g=G, mode_w=W, mode_gw=G / W if M else G,
-        first_aux=first_aux, first_mode=first_mode,
         l_ptr=l_ptr, l_col=l_col, l_val=l_val, lh_ptr=lh_ptr, lh_col=lh_col, lh_val=lh_val,
         lop_active=lop_active, lop_site=site, lop_sval=sval,
         h_ptr=h_ptr, h_col=h_col, h_val=h_val, site_projector=int(is_site),
-        mode_site=mode_site.astype(np.int32), mode_gwv=mode_gwv, dn_coef_site=dn_coef_site,
-        up_site=np.asarray(up_site, dtype=np.int32), dn_site=np.asarray(dn_site, dtype=np.int32),
-        h_diag=h_diag,
-        max_up=int(up_counts.max()) if len(up_counts) else 0,
-        max_dn=int(dn_counts.max()) if len(dn_counts) else 0,
+        mode_site=mode_site.astype(np.int32), mode_gwv=mode_gwv, h_diag=h_diag,
     )
+
+
+def _binomials(n_max, k_max):
+    """int64 table C(n, j), n <= n_max, j <= k_max (row stride k_max + 1)."""
+    t = np.zeros((n_max + 1, k_max + 1), dtype=np.int64)
+    for n in range(n_max + 1):
+        for j in range(min(n, k_max) + 1):
+            t[n, j] = comb(n, j)
+    return t
+
+
+def build_tables_triangular(system, depth, device):
+    """``build_tables`` for the full triangular hierarchy over every mode and
+    state, with the aux-indexed arrays built on the GPU (hops_tri_pass1/2)
+    and left there as torch tensors; the state/mode tables stay on the host."""
+    from . import _lib
+    from .exceptions import UnsupportedRequest
+    dev = torch.device(device)
+    M, D = system.n_mode, int(depth)
+    N = comb(M + D, D)
+    n_below = comb(M + D - 1, D - 1) if D > 0 else 0
+    if N >= 2 ** 31:
+        raise UnsupportedRequest(f"hierarchy of {N} aux (>= 2^31)", "mesohops_b200 build_tables")
+    small = _state_mode_tables(system, np.arange(system.n_state), np.arange(M))
+    L = _lib.lib()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    binom = torch.from_numpy(_binomials(M + D + 1, D + 1)).to(dev)
+    w = torch.from_numpy(np.ascontiguousarray(system.W, dtype=np.complex128)).to(dev)
+    k_decay = torch.empty(N, dtype=torch.complex128, device=dev)
+    dn_count = torch.empty(N, dtype=torch.int32, device=dev)
+    _lib.check(L.hops_tri_pass1(M, D, binom.data_ptr(), N, w.data_ptr(), k_decay.data_ptr(),
+                                dn_count.data_ptr(), stream), "hops_tri_pass1")
+    dn_ptr = torch.zeros(N + 1, dtype=torch.int64, device=dev)
+    dn_ptr[1:] = torch.cumsum(dn_count, 0)
+    n_dn = int(dn_ptr[-1])
+    dn_ptr = dn_ptr.to(torch.int32)
+    up_aux = torch.empty(n_below * M, dtype=torch.int32, device=dev)
+    up_mode = torch.empty(n_below * M, dtype=torch.int32, device=dev)
+    dn_aux = torch.empty(max(n_dn, 1), dtype=torch.int32, device=dev)
+    dn_mode = torch.empty(max(n_dn, 1), dtype=torch.int32, device=dev)
+    dn_k = torch.empty(max(n_dn, 1), dtype=torch.int32, device=dev)
+    _lib.check(L.hops_tri_pass2(M, D, binom.data_ptr(), N, n_below, dn_ptr.data_ptr(),
+                                up_aux.data_ptr(), up_mode.data_ptr(), dn_aux.data_ptr(),
+                                dn_mode.data_ptr(), dn_k.data_ptr(), stream), "hops_tri_pass2")
+    dn_aux, dn_mode, dn_k = dn_aux[:n_dn], dn_mode[:n_dn], dn_k[:n_dn]
+    up_ptr = (torch.clamp(torch.arange(N + 1, device=dev), max=n_below) * M).to(torch.int32)
+    sval = torch.from_numpy(small["lop_sval"]).to(dev)
+    mode_lop = torch.from_numpy(small["mode_lop"].astype(np.int64)).to(dev)
+    mode_site = torch.from_numpy(small["mode_site"].astype(np.int64)).to(dev)
+    dnm = dn_mode.to(torch.int64)
+    dn_coef = dn_k.to(torch.float64) * w[dnm]
+    dn_coef_site = dn_coef * torch.conj(sval[mode_lop[dnm]])
+    first_aux = np.arange(1, M + 1, dtype=np.int32) if D >= 1 else np.zeros(0, np.int32)
+    first_mode = np.arange(M, dtype=np.int32) if D >= 1 else np.zeros(0, np.int32)
+    small.update(
+        n_hier=int(N), k_decay=k_decay, up_ptr=up_ptr, up_aux=up_aux, up_mode=up_mode,
+        dn_ptr=dn_ptr, dn_aux=dn_aux, dn_mode=dn_mode, dn_coef=dn_coef,
+        first_aux=first_aux, first_mode=first_mode, dn_coef_site=dn_coef_site,
+        up_site=mode_site[up_mode.to(torch.int64)].to(torch.int32),
+        dn_site=mode_site[dnm].to(torch.int32),
+        max_up=M if n_below > 0 else 0, max_dn=min(D, M) if N > 1 else 0,
+    )
+    return small
 
 
 class DeviceStructure:
@@ -146,14 +241,14 @@ class DeviceStructure:
         self.tables = tables
         self.device = torch.device(device)
         t = tables
-        c2d, c2f = _c2d, _c2f
+        c2d, c2f = _c2d_any, _c2f_any
         i32 = np.int32
         fields = [
             ("k_decay", c2d(t["k_decay"])), ("k_decay_f", c2f(t["k_decay"])),
-            ("up_ptr", t["up_ptr"].astype(i32)), ("up_aux", t["up_aux"].astype(i32)),
-            ("up_mode", t["up_mode"].astype(i32)),
-            ("dn_ptr", t["dn_ptr"].astype(i32)), ("dn_aux", t["dn_aux"].astype(i32)),
-            ("dn_mode", t["dn_mode"].astype(i32)),
+            ("up_ptr", _i32_any(t["up_ptr"])), ("up_aux", _i32_any(t["up_aux"])),
+            ("up_mode", _i32_any(t["up_mode"])),
+            ("dn_ptr", _i32_any(t["dn_ptr"])), ("dn_aux", _i32_any(t["dn_aux"])),
+            ("dn_mode", _i32_any(t["dn_mode"])),
             ("dn_coef", c2d(t["dn_coef"])), ("dn_coef_f", c2f(t["dn_coef"])),
             ("mode_lop", t["mode_lop"].astype(i32)), ("mode_g", c2d(t["mode_g"])),
             ("mode_w", c2d(t["mode_w"])), ("mode_gw", c2d(t["mode_gw"])),
@@ -170,18 +265,25 @@ class DeviceStructure:
             ("mode_site", t["mode_site"].astype(i32)), ("mode_gwv", c2d(t["mode_gwv"])),
             ("mode_gwv_f", c2f(t["mode_gwv"])),
             ("dn_coef_site", c2d(t["dn_coef_site"])), ("dn_coef_site_f", c2f(t["dn_coef_site"])),
-            ("up_site", t["up_site"].astype(i32)), ("dn_site", t["dn_site"].astype(i32)),
+            ("up_site", _i32_any(t["up_site"])), ("dn_site", _i32_any(t["dn_site"])),
         ]
         if t["h_diag"] is not None:
             fields.append(("h_diag", c2d(t["h_diag"])))
         offs = {}
         off = 0
         for name, arr in fields:
-            a = np.ascontiguousarray(arr)
-            if a.size == 0:
-                a = np.zeros(4, dtype=np.int32)
-            offs[name] = (off, a)
-            off += -(-a.nbytes // self._ALIGN) * self._ALIGN
+            if isinstance(arr, torch.Tensor):
+                a = arr.contiguous()
+                if a.numel() == 0:
+                    a = torch.zeros(4, dtype=torch.int32, device=self.device)
+                nbytes = a.numel() * a.element_size()
+            else:
+                a = np.ascontiguousarray(arr)
+                if a.size == 0:
+                    a = np.zeros(4, dtype=np.int32)
+                nbytes = a.nbytes
+            offs[name] = (off, a, nbytes)
+            off += -(-nbytes // self._ALIGN) * self._ALIGN
         struct_off = off
         total = off + C.sizeof(HopsStructure)
         self.buffer = torch.empty(total, dtype=torch.uint8, device=self.device)
@@ -194,14 +296,42 @@ class DeviceStructure:
         s.n_dn = len(t["dn_aux"])
         s.site_projector = t["site_projector"]
         s.max_up, s.max_dn = t["max_up"], t["max_dn"]
-        for name, (o, a) in offs.items():
-            host[o:o + a.nbytes] = a.view(np.uint8).ravel()
+        dev_parts = []
+        for name, (o, a, nbytes) in offs.items():
+            if isinstance(a, torch.Tensor):
+                dev_parts.append((o, a, nbytes))
+            else:
+                host[o:o + nbytes] = a.view(np.uint8).ravel()
             setattr(s, name, base + o)
         host[struct_off:] = np.frombuffer(bytes(s), dtype=np.uint8)
         self.buffer.copy_(torch.from_numpy(host))
+        for o, a, nbytes in dev_parts:
+            self.buffer[o:o + nbytes].copy_(a.view(torch.uint8).reshape(-1))
         self.cstruct = s
         self.dev_ptr = base + struct_off
 
     @property
     def n_elem(self):
         return self.tables["n_hier"] * self.tables["n_state"]
+
+
+# Hierarchies at least this large are built on the GPU when they have no
+# static filters (build_tables_triangular); smaller ones on the host.
+GPU_BUILD_MIN_AUX = 4096
+
+
+def hierarchy_structure(system, hierarchy_param, device):
+    """(hierarchy, DeviceStructure) of the non-adaptive basis of a trajectory or
+    ensemble: all states, all modes, the triangular hierarchy with the static
+    filters of hierarchy_param."""
+    from .hierarchy import TriangularHierarchy, triangular_basis
+    from . import _lib
+    dev = torch.device(device)
+    depth = int(hierarchy_param["MAXHIER"])
+    filters = hierarchy_param.get("STATIC_FILTERS", [])
+    if (dev.type == "cuda" and not filters and depth <= int(_lib.lib().hops_tri_max_depth())
+            and comb(system.n_mode + depth, depth) >= GPU_BUILD_MIN_AUX):
+        h = TriangularHierarchy(system.n_mode, depth)
+        return h, DeviceStructure(build_tables_triangular(system, depth, dev), dev)
+    basis = triangular_basis(system.n_mode, depth, filters)
+    return basis, DeviceStructure(build_tables(system, basis), dev)

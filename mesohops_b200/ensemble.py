@@ -12,10 +12,9 @@ import numpy as np
 import torch
 
 from .constants import hbar, precision
-from .device import DeviceStructure, build_tables
+from .device import hierarchy_structure
 from .engine import StreamBatch
 from .exceptions import TrajectoryError, UnsupportedRequest
-from .hierarchy import triangular_basis
 from .noise import HopsNoise, filter_on_device, raw_white_noise
 from .params import (EOM_DICT_DEFAULT, EOM_DICT_TYPES, HIERARCHY_DICT_DEFAULT,
                      HIERARCHY_DICT_TYPES, NOISE_DICT_DEFAULT, NOISE_DICT_TYPES,
@@ -44,9 +43,8 @@ class HopsEnsemble:
         self.noise_param = initialize_dict(np_, NOISE_DICT_DEFAULT, NOISE_DICT_TYPES, "HopsNoise")
         self.seeds = seeds
         self.n_t = int(np.ceil(self.noise_param["TLEN"] / self.noise_param["TAU"])) + 1
-        self.basis = triangular_basis(self.system.n_mode, self.hierarchy_param["MAXHIER"],
-                                      self.hierarchy_param["STATIC_FILTERS"])
-        self.dstruct = DeviceStructure(build_tables(self.system, self.basis), self.device)
+        self.basis, self.dstruct = hierarchy_structure(self.system, self.hierarchy_param,
+                                                       self.device)
         self.batch = StreamBatch(self.dstruct, self.B, precision,
                                  self.eom_param["EQUATION_OF_MOTION"])
         self.t = 0.0

@@ -231,3 +231,23 @@ def triangular_basis(n_mode, maxhier, static_filters=()):
     if static_filters:
         counts = apply_static_filters(counts, static_filters, n_mode)
     return AuxBasis(counts, keyer, maxhier)
+
+
+class TriangularHierarchy:
+    """The full triangular hierarchy over ``n_mode`` modes to depth
+    ``maxhier`` when its tables are built on the GPU
+    (device.build_tables_triangular); the host count matrix is produced only
+    when asked for (``counts``)."""
+
+    def __init__(self, n_mode, maxhier):
+        self.maxhier = int(maxhier)
+        self.n_mode = int(n_mode)
+        self.n_hier = comb(self.n_mode + self.maxhier, self.maxhier)
+        self.modes = np.arange(self.n_mode)
+        self._counts = None
+
+    @property
+    def counts(self):
+        if self._counts is None:
+            self._counts = triangular_counts(self.n_mode, self.maxhier)
+        return self._counts

@@ -22,10 +22,9 @@ import torch
 
 from . import adaptive as _adaptive
 from .constants import hbar, precision
-from .device import DeviceStructure, build_tables
+from .device import hierarchy_structure
 from .engine import ResidentRunner, ResidentTrajectory, StreamBatch
 from .exceptions import LockedException, TrajectoryError, UnsupportedRequest
-from .hierarchy import triangular_basis
 from .noise import HopsNoise
 from .params import (DEVICE_DICT_DEFAULT, EOM_DICT_DEFAULT, EOM_DICT_TYPES,
                      HIERARCHY_DICT_DEFAULT, HIERARCHY_DICT_TYPES, INTEGRATION_DICT_DEFAULT,
@@ -107,9 +106,7 @@ class HopsTrajectory:
             self.storage.metadata["INITIALIZATION_TIME"] = timer.time() - t0
             self.__initialized__ = True
             return
-        self.basis = triangular_basis(self.system.n_mode, self.hierarchy_param["MAXHIER"],
-                                      self.hierarchy_param["STATIC_FILTERS"])
-        self.dstruct = DeviceStructure(build_tables(self.system, self.basis), dev)
+        self.basis, self.dstruct = hierarchy_structure(self.system, self.hierarchy_param, dev)
         prec = self.device_param["PRECISION"]
         prec_bytes = 16 if prec in ("complex128", "c128", "mixed") else 8
         n_elem = self.dstruct.n_elem
