@@ -144,13 +144,15 @@ def footprint(req, precision):
     return vec + table + noise + psi, kern
 
 
-def plan_admission(queue, arrival, used, budget, now, fairness_s, precision):
+def plan_admission(queue, arrival, used, budget, now, fairness_s, precision, small_frac=0.02):
     """Admission decisions for the waiting requests (in arrival order).
 
     Returns (admit [(req, bytes, kernel)], reject [(req, bytes)]): a request whose
     footprint exceeds the whole budget is rejected; the others are admitted
-    first-fit while the budget lasts, except that once the oldest waiting
-    request has waited longer than fairness_s nothing is admitted ahead of it."""
+    first-fit while the budget lasts.  Once the oldest waiting request has
+    waited longer than fairness_s, later requests overtake it only if they are
+    small (at most small_frac of the budget), so a large request is not starved
+    and small ones do not queue behind it."""
     admit, reject = [], []
     blocked = False
     head_seen = False
@@ -159,7 +161,7 @@ def plan_admission(queue, arrival, used, budget, now, fairness_s, precision):
         if fp > budget:
             reject.append((req, fp))
             continue
-        if blocked:
+        if blocked and fp > small_frac * budget:
             continue
         if used + fp <= budget:
             admit.append((req, fp, kern))
@@ -287,7 +289,12 @@ class HopsServer:
                     queue.remove(req)
                     used += fp
                     if kern == "adaptive" and pool is not None:
-                        pool.submit(req.rid, req)
+                        try:
+                            pool.submit(req.rid, req)
+                        except (UnsupportedRequest, TrajectoryError, ValueError) as exc:
+                            used -= fp
+                            results[req.rid] = ServedResult(req, "error", str(exc), footprint=fp)
+                            continue
                         pooled[req.rid] = [req, fp, None]
                     else:
                         building.append((builders.submit(self._build, req, kern), req, fp, kern))

@@ -62,10 +62,14 @@ def test_admission_first_fit_reject_and_fairness():
                                       fairness_s=1.0, precision="mixed")
     assert [r.rid for r, _, _ in admit] == [1]
     assert [r.rid for r, _ in reject] == [2]
-    # a has waited past the fairness limit: b may not overtake it
+    # a has waited past the fairness limit: b may overtake it only while b is
+    # small against the budget
     admit, reject = sv.plan_admission([a, b], arrival, used=fb, budget=budget, now=5.0,
-                                      fairness_s=1.0, precision="mixed")
+                                      fairness_s=1.0, precision="mixed", small_frac=0.0)
     assert admit == [] and reject == []
+    admit, _ = sv.plan_admission([a, b], arrival, used=fb, budget=budget, now=5.0,
+                                 fairness_s=1.0, precision="mixed", small_frac=0.5)
+    assert [r.rid for r, _, _ in admit] == [1]
     admit, _ = sv.plan_admission([a, b], arrival, used=0, budget=budget, now=5.0,
                                  fairness_s=1.0, precision="mixed")
     assert [r.rid for r, _, _ in admit] == [0]
