@@ -26,7 +26,7 @@ from .device import hierarchy_structure
 from .engine import ResidentRunner, ResidentTrajectory, StreamBatch
 from .exceptions import LockedException, TrajectoryError, UnsupportedRequest
 from .noise import HopsNoise
-from .params import (DEVICE_DICT_DEFAULT, EOM_DICT_DEFAULT, EOM_DICT_TYPES,
+from .params import (DEVICE_DICT_DEFAULT, EOM_DICT_DEFAULT, EOM_DICT_TYPES, NOISE_DICT_DEFAULT,
                      HIERARCHY_DICT_DEFAULT, HIERARCHY_DICT_TYPES, INTEGRATION_DICT_DEFAULT,
                      INTEGRATION_DICT_TYPES, initialize_dict)
 from .storage import HopsStorage
@@ -336,6 +336,112 @@ class HopsTrajectory:
         if self._adhops is not None:
             return self._adhops.basis.counts
         return self.basis.counts
+
+    # ------------------------------------------------------------ checkpoints
+    _SYSTEM_KEYS = ("HAMILTONIAN", "GW_SYSBATH", "L_HIER", "L_NOISE1", "ALPHA_NOISE1",
+                    "PARAM_NOISE1", "L_NOISE2", "ALPHA_NOISE2", "PARAM_NOISE2", "L_LT_CORR",
+                    "PARAM_LT_CORR")
+
+    def save_checkpoint(self, filepath, compress=True, drop_seed=False):
+        """Save parameters, state and storage to an .npz file with the keys of
+        hops_trajectory.py:853-937 (phi, z_mem, t, state_list, aux_list,
+        early_counter, storage_data, storage_meta, params); params also holds
+        this implementation's device_param.  drop_seed leaves out the noise
+        seeds (to be given again to load_checkpoint)."""
+        if not self.__initialized__:
+            raise TrajectoryError("save_checkpoint called before initialize")
+        eom_param = {k: v for k, v in self.eom_param.items() if k != "ADAPTIVE"}
+        for key in ("DELTA_A", "DELTA_S", "F_DISCARD"):
+            if key in eom_param:
+                eom_param[key] = float(eom_param[key])
+        if eom_param.get("UPDATE_STEP") is None:
+            eom_param.pop("UPDATE_STEP", None)
+
+        def noise_dict(nz):
+            return {k: nz.param[k] for k in NOISE_DICT_DEFAULT
+                    if k in nz.param and not (k == "SEED" and drop_seed)}
+
+        storage_param = dict(self.storage.storage_dic)
+        storage_param["STORAGE_TIME"] = self.storage.storage_time
+        params = {
+            "system_param": {k: self.system.param[k] for k in self._SYSTEM_KEYS
+                             if k in self.system.param},
+            "hierarchy_param": {k: self.hierarchy_param[k] for k in HIERARCHY_DICT_DEFAULT},
+            "eom_param": eom_param,
+            "noise1_param": noise_dict(self.noise1),
+            "noise2_param": noise_dict(self.noise2),
+            "integration_param": dict(self.integration_param),
+            "storage_param": storage_param,
+            "device_param": dict(self.device_param),
+        }
+        phi, z_mem = self._get_state()
+        counts = self.auxiliary_list
+        aux_list = np.empty(len(counts), dtype=object)
+        for i, c in enumerate(counts):
+            nz = np.nonzero(c)[0]
+            aux_list[i] = np.array([(int(m), int(c[m])) for m in nz], dtype=int).reshape(-1, 2)
+        checkpoint = {
+            "phi": phi, "z_mem": z_mem, "t": self.t,
+            "state_list": np.array(self.state_list, dtype=int), "aux_list": aux_list,
+            "early_counter": self._adhops.early_counter if self._adhops is not None else 0,
+            "storage_data": self.storage.data, "storage_meta": self.storage.metadata,
+            "params": params,
+        }
+        (np.savez_compressed if compress else np.savez)(filepath, **checkpoint)
+
+    @classmethod
+    def load_checkpoint(cls, filename, add_seed1=None, add_seed2=None, add_system_param=None,
+                        device_param=None):
+        """A trajectory restored from save_checkpoint (hops_trajectory.py:938-1034):
+        same parameters, basis, state, noise memory, time and storage; the
+        device_param stored with it unless another is given."""
+        data = np.load(filename, allow_pickle=True)
+        params = data["params"].item()
+        if add_seed1 is not None:
+            params["noise1_param"]["SEED"] = add_seed1
+        if add_seed2 is not None:
+            params["noise2_param"]["SEED"] = add_seed2
+        if add_system_param is not None:
+            params["system_param"] = add_system_param
+        traj = cls(params["system_param"], eom_param=params["eom_param"],
+                   noise_param=params["noise1_param"], noise2_param=params["noise2_param"],
+                   hierarchy_param=params["hierarchy_param"],
+                   storage_param=params["storage_param"],
+                   integration_param=params["integration_param"],
+                   device_param=device_param or params.get("device_param"))
+        states = np.asarray(data["state_list"], dtype=np.int64)
+        phi = np.asarray(data["phi"], dtype=np.complex128)
+        z_mem = data["z_mem"]
+        if z_mem.dtype == object:                      # a sparse matrix
+            z_mem = z_mem.item()
+            z_mem = np.asarray(z_mem.toarray() if hasattr(z_mem, "toarray") else z_mem)
+        z_mem = np.asarray(z_mem, dtype=np.complex128).ravel()
+        if len(z_mem) < traj.system.n_mode:
+            z_mem = np.concatenate([z_mem, np.zeros(traj.system.n_mode - len(z_mem), complex)])
+        psi_0 = np.zeros(traj.system.n_state, dtype=np.complex128)
+        psi_0[states] = phi[:len(states)]
+        traj.initialize(psi_0)
+        if traj._adhops is not None:
+            ad = traj._adhops
+            counts = np.zeros((len(data["aux_list"]), traj.system.n_mode), dtype=np.int16)
+            for i, a in enumerate(data["aux_list"]):
+                for (m, k) in np.asarray(a).reshape(-1, 2):
+                    counts[i, int(m)] = int(k)
+            ad.update_basis(ad.phi, states, counts)
+            if len(phi) != ad.basis.n_hier * ad.basis.n_state:
+                raise TrajectoryError("checkpoint state does not match its basis")
+            ad.phi = phi.copy()
+            ad.zmem_abs = z_mem[:traj.system.n_mode].copy()
+            ad.t = float(data["t"])
+            ad.early_counter = int(data["early_counter"])
+        else:
+            if len(phi) != traj.n_hier * traj.n_state:
+                raise TrajectoryError("checkpoint state does not match the hierarchy")
+            traj._set_state(phi, z_mem[:traj.system.n_mode])
+        traj._t = float(data["t"])
+        traj.storage.data = data["storage_data"].item()
+        traj.storage.metadata = data["storage_meta"].item()
+        return traj
 
     def normalize(self, phi):
         """hops_trajectory.py:616-634 (host helper for callers)."""
