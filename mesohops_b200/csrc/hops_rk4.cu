@@ -266,9 +266,12 @@ __device__ __forceinline__ void acc_store(ST* p, ST v) {
   else *p = v;
 }
 
+// rk_finish: the same update with the accumulated slope acc[e] already loaded
+// (accv; read at stages 1-3 only), so that a caller can load the operands of
+// several elements before it stores any of them.
 template <bool GHINT, typename T, typename ST, typename PT>
-__device__ __forceinline__ void rk_update(int stage, double h, T k, PT ph, ST* acc, ST* yout,
-                                          PT* phi, ST* shadow, size_t e) {
+__device__ __forceinline__ void rk_finish(int stage, double h, T k, PT ph, ST accv, ST* acc,
+                                          ST* yout, PT* phi, ST* shadow, size_t e) {
   using RP = decltype(ph.x);
   const RP hh = (RP)h;
   switch (stage) {
@@ -278,13 +281,13 @@ __device__ __forceinline__ void rk_update(int stage, double h, T k, PT ph, ST* a
     } break;
     case 1:
     case 2: {
-      const T a0 = cv<T>(acc_load<GHINT>(acc + e));
+      const T a0 = cv<T>(accv);
       acc_store<GHINT>(acc + e, cv<ST>(cadd(a0, cscale(k, (decltype(k.x))2))));
       const RP c = stage == 1 ? hh * (RP)0.5 : hh;
       yout[e] = cv<ST>(cadd(ph, cscale(cv<PT>(k), c)));
     } break;
     case 3: {
-      PT sum = cv<PT>(cadd(cv<T>(acc_load<GHINT>(acc + e)), k));
+      PT sum = cv<PT>(cadd(cv<T>(accv), k));
       PT hs = cscale(sum, hh);
       hs.x = hs.x / (RP)6;
       hs.y = hs.y / (RP)6;
@@ -297,6 +300,13 @@ __device__ __forceinline__ void rk_update(int stage, double h, T k, PT ph, ST* a
   }
 }
 
+template <bool GHINT, typename T, typename ST, typename PT>
+__device__ __forceinline__ void rk_update(int stage, double h, T k, PT ph, ST* acc, ST* yout,
+                                          PT* phi, ST* shadow, size_t e) {
+  const ST accv = (stage >= 1 && stage <= 3) ? acc_load<GHINT>(acc + e) : ST{};
+  rk_finish<GHINT, T, ST, PT>(stage, h, k, ph, accv, acc, yout, phi, shadow, e);
+}
+
 // ---------------------------------------------------- wide stage kernel ----
 // B >= 32 trajectories: one warp per (aux a, state s, chunk of 32*NB
 // trajectories); lane l owns the trajectories bg + l + 32 j, j < NB.
@@ -307,8 +317,12 @@ __device__ __forceinline__ void rk_update(int stage, double h, T k, PT ph, ST* a
 // all gather from one chunk's slice of Y, which stays resident in L2 (a slice
 // of 32 trajectories of the 20-site ring is 54 MB in complex64); otherwise each
 // warp walks every chunk of its (a, s).
+// The stage is bound by load latency at the occupancy registers allow: with
+// NB <= 2 the kernel is held to 64 registers (4 CTAs, 32 warps per SM), which
+// measured faster than the extra registers it would otherwise take; NB >= 4
+// keeps every segment's loads in flight in registers and is left uncapped.
 template <typename R, typename ST, typename PT, bool SITE, int NB>
-__global__ void __launch_bounds__(256) k_wide(hops_structure st, int B, int stage, double h,
+__global__ void __launch_bounds__(256, NB <= 2 ? 4 : 1) k_wide(hops_structure st, int B, int stage, double h,
                                               const ST* __restrict__ yin, ST* __restrict__ yout,
                                               PT* phi, ST* shadow, ST* acc,
                                               const double* __restrict__ ws, FastDiv divS,
@@ -460,18 +474,34 @@ __global__ void __launch_bounds__(256) k_wide(hops_structure st, int B, int stag
           }
         }
       }
+      // Every load of the RK update (phi, the accumulated slope, the pending
+      // scale) of all NB elements is issued before the first store: phi, acc
+      // and the outputs may alias as far as the compiler knows, so otherwise
+      // each element would wait for a DRAM round trip of its own.
+      PT ph[NB];
+      ST accv[NB];
+      double sc[NB];
 #pragma unroll
       for (int j = 0; j < NB; ++j) {
+        ph[j] = PT{};
+        accv[j] = ST{};
+        sc[j] = 1.0;
         if (!ok[j]) continue;
         const int b = bg + lane + 32 * j;
         const size_t e = rowa + b;
-        const double sc = scaleB[b];
-        T kk = k[j];
-        if (stage == 0 || stage == 4) kk = cscale(kk, (R)sc);
+        sc[j] = scaleB[b];
         // stages 1-3 read phi once (pure stream); stage 0 also gathers phi
-        PT ph = PT{};
-        if (stage != 4) ph = cscale(stage == 0 ? phi[e] : __ldcs(phi + e), (decltype(PT{}.x))sc);
-        rk_update<true, T, ST, PT>(stage, h, kk, ph, acc, yout, phi, shadow, e);
+        if (stage != 4) ph[j] = stage == 0 ? phi[e] : __ldcs(phi + e);
+        if (stage >= 1 && stage <= 3) accv[j] = acc_load<true>(acc + e);
+      }
+#pragma unroll
+      for (int j = 0; j < NB; ++j) {
+        if (!ok[j]) continue;
+        const size_t e = rowa + bg + lane + 32 * j;
+        T kk = k[j];
+        if (stage == 0 || stage == 4) kk = cscale(kk, (R)sc[j]);
+        const PT p = stage == 4 ? PT{} : cscale(ph[j], (decltype(PT{}.x))sc[j]);
+        rk_finish<true, T, ST, PT>(stage, h, kk, p, accv[j], acc, yout, phi, shadow, e);
       }
     }
   }
@@ -910,12 +940,12 @@ static void launch_stage(const hops_structure* st, int B, int stage, double h, c
   (void)status;
   if (B >= 32) {
     const int nbmax = (B + 31) / 32;
-    // auto (measured on the 20-site ring, 128 trajectories): 64 trajectories
-    // per warp task with FP32 arithmetic, 128 with FP64 arithmetic, natural
+    // auto (measured on the 20-site ring, 128 trajectories): 128 trajectories
+    // per warp task with FP32 arithmetic, 64 with FP64 arithmetic, natural
     // task order; the autotuner overrides this per problem class
     int cm = g_tune_cm >= 0 ? g_tune_cm : 0;
     int nb = g_tune_nb;
-    if (nb == 0) nb = sizeof(typename Prec<R>::T) == 8 ? 2 : 4;
+    if (nb == 0) nb = sizeof(typename Prec<R>::T) == 8 ? 4 : 2;
     if (nb > nbmax) nb = nbmax >= 4 ? 4 : (nbmax >= 2 ? 2 : 1);
     if (nb > 8) nb = 8;
     if (nb == 1) launch_wide<R, ST, PT, SITE, 1>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, cm, s);
