@@ -321,12 +321,36 @@ __device__ __forceinline__ void rk_update(int stage, double h, T k, PT ph, ST* a
 // NB <= 2 the kernel is held to 64 registers (4 CTAs, 32 warps per SM), which
 // measured faster than the extra registers it would otherwise take; NB >= 4
 // keeps every segment's loads in flight in registers and is left uncapped.
+// Asynchronous global -> shared copies (cp.async, no register staging).
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* sdst, const void* gsrc) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(gsrc), "n"(BYTES)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Shared memory of k_wide: per warp, two buffers of one work item's streamed
+// operands (phi, acc and the item's own row of Y; 32*NB trajectories each).
+template <typename ST, typename PT, int NB>
+constexpr size_t wide_smem_bytes(int warps) {
+  return (size_t)warps * 2 * 32 * NB * (sizeof(PT) + 2 * sizeof(ST));
+}
+
 template <typename R, typename ST, typename PT, bool SITE, int NB>
-__global__ void __launch_bounds__(256, NB <= 2 ? 4 : 1) k_wide(hops_structure st, int B, int stage, double h,
-                                              const ST* __restrict__ yin, ST* __restrict__ yout,
-                                              PT* phi, ST* shadow, ST* acc,
-                                              const double* __restrict__ ws, FastDiv divS,
-                                              FastDiv divAS, int chunk_major) {
+__global__ void __launch_bounds__(256, NB <= 2 ? 4 : (NB == 4 ? 2 : 1))
+    k_wide(hops_structure st, int B, int stage, double h, const ST* __restrict__ yin,
+           ST* __restrict__ yout, PT* phi, ST* shadow, ST* acc, const double* __restrict__ ws,
+           FastDiv divS, FastDiv divAS, int chunk_major) {
   using P = Prec<R>;
   using T = typename P::T;
   const int S = st.n_state;
@@ -342,169 +366,203 @@ __global__ void __launch_bounds__(256, NB <= 2 ? 4 : 1) k_wide(hops_structure st
   const unsigned nchunk = (unsigned)((B + CH - 1) / CH);
   const unsigned ntask = chunk_major ? n_as * nchunk : n_as;
   const unsigned nw = (gridDim.x * blockDim.x) >> 5;
-  for (unsigned t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntask; t += nw) {
-    unsigned as = t, c0 = 0, c1 = nchunk;
-    if (chunk_major) {
-      c0 = divAS.div(t);
-      as = t - c0 * n_as;
-      c1 = c0 + 1;
+
+  // A work item is one (task, chunk).  The streamed operands of the warp's
+  // next item are copied into shared memory while the current item gathers
+  // its neighbours, so no item waits for its own DRAM reads.
+  extern __shared__ __align__(16) unsigned char wide_smem[];
+  const int nwb = blockDim.x >> 5;
+  const int wib = threadIdx.x >> 5;
+  PT* ph_s = reinterpret_cast<PT*>(wide_smem) + (size_t)wib * 2 * CH;
+  ST* ac_s = reinterpret_cast<ST*>(wide_smem + (size_t)nwb * 2 * CH * sizeof(PT)) +
+             (size_t)wib * 2 * CH;
+  ST* ys_s = reinterpret_cast<ST*>(wide_smem + (size_t)nwb * 2 * CH * (sizeof(PT) + sizeof(ST))) +
+             (size_t)wib * 2 * CH;
+  const bool want_phi = stage != 4;
+  const bool want_acc = stage >= 1 && stage <= 3;
+  auto prefetch = [&](unsigned t, unsigned ci, int buf) {
+    const unsigned as = chunk_major ? t - ci * n_as : t;
+    const size_t row = (size_t)as * B;
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+      const int b = (int)ci * CH + lane + 32 * j;
+      if (b < B) {
+        const int o = buf * CH + lane + 32 * j;
+        cp_async<sizeof(ST)>(ys_s + o, yin + row + b);
+        if (want_phi) cp_async<sizeof(PT)>(ph_s + o, phi + row + b);
+        if (want_acc) cp_async<sizeof(ST)>(ac_s + o, acc + row + b);
+      }
     }
+  };
+
+  unsigned t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  unsigned ci = (t < ntask && chunk_major) ? divAS.div(t) : 0u;
+  if (t < ntask) prefetch(t, ci, 0);
+  cp_async_commit();
+  int buf = 0;
+  while (t < ntask) {
+    unsigned tn = t, cn = ci + 1;
+    if (chunk_major || cn >= nchunk) {
+      tn = t + nw;
+      cn = (tn < ntask && chunk_major) ? divAS.div(tn) : 0u;
+    }
+    if (tn < ntask) prefetch(tn, cn, buf ^ 1);
+    cp_async_commit();  // one group per item, empty past the last one
+
+    const unsigned as = chunk_major ? t - ci * n_as : t;
     const int a = (int)divS.div(as);
     const int s = (int)as - a * S;
-    const size_t rowa = ((size_t)a * S + s) * B;
+    const size_t rowa = (size_t)as * B;
     const T kd = P::kdec(st, a);
     const int u0 = st.up_ptr[a], u1 = st.up_ptr[a + 1];
     const int d0 = st.dn_ptr[a], d1 = st.dn_ptr[a + 1];
     const int h0 = st.h_ptr[s], h1 = st.h_ptr[s + 1];
-    for (unsigned ci = c0; ci < c1; ++ci) {
-      const int bg = (int)ci * CH;
-      T k[NB];
-      bool ok[NB];
+    const int bg = (int)ci * CH;
+    cp_async_wait<1>();  // this item's copies have landed (each lane reads only its own)
+    T k[NB];
+    bool ok[NB];
 #pragma unroll
-      for (int j = 0; j < NB; ++j) {
-        const int b = bg + lane + 32 * j;
-        ok[j] = b < B;
-        k[j] = czero<T>();
-        if (ok[j]) {
-          T c = kd;
-          if (SITE) {
-            c = cadd(c, diagT[(size_t)s * B + b]);
-          } else {
-            c.x -= (R)ncB[b];
-          }
-          k[j] = cmul(c, cv<T>(yin[rowa + b]));
+    for (int j = 0; j < NB; ++j) {
+      const int b = bg + lane + 32 * j;
+      ok[j] = b < B;
+      k[j] = czero<T>();
+      if (ok[j]) {
+        T c = kd;
+        if (SITE) {
+          c = cadd(c, diagT[(size_t)s * B + b]);
+        } else {
+          c.x -= (R)ncB[b];
+        }
+        k[j] = cmul(c, cv<T>(ys_s[buf * CH + lane + 32 * j]));
+      }
+    }
+    if (!SITE) {
+      for (int jl = 0; jl < st.n_lop; ++jl) {
+        const int base = jl * (S + 1);
+        const int q0 = st.l_ptr[base + s], q1 = st.l_ptr[base + s + 1];
+        for (int q = q0; q < q1; ++q) {
+          const T lv = P::lval(st, q);
+          const size_t rb = ((size_t)a * S + st.l_col[q]) * B + bg + lane;
+#pragma unroll
+          for (int j = 0; j < NB; ++j)
+            if (ok[j])
+              k[j] = cfma(cmul(czT[(size_t)jl * B + bg + lane + 32 * j], lv), cv<T>(yin[rb + 32 * j]), k[j]);
         }
       }
-      if (!SITE) {
-        for (int jl = 0; jl < st.n_lop; ++jl) {
-          const int base = jl * (S + 1);
-          const int q0 = st.l_ptr[base + s], q1 = st.l_ptr[base + s + 1];
-          for (int q = q0; q < q1; ++q) {
-            const T lv = P::lval(st, q);
-            const size_t rb = ((size_t)a * S + st.l_col[q]) * B + bg + lane;
+    }
+    for (int q = h0; q < h1; ++q) {
+      const T hv = P::hval(st, q);
+      const size_t rb = ((size_t)a * S + st.h_col[q]) * B + bg + lane;
 #pragma unroll
-            for (int j = 0; j < NB; ++j)
-              if (ok[j])
-                k[j] = cfma(cmul(czT[(size_t)jl * B + bg + lane + 32 * j], lv), cv<T>(yin[rb + 32 * j]), k[j]);
+      for (int j = 0; j < NB; ++j)
+        if (ok[j]) k[j] = cfma(hv, cv<T>(yin[rb + 32 * j]), k[j]);
+    }
+    int p0 = u0;
+    if (SITE) {
+      // two neighbours per iteration: their 2 x NB row segments are loaded
+      // before either is consumed, so twice as many loads are in flight
+      for (; p0 + 2 <= u1; p0 += 2) {
+        const int ua = __ldg(st.up_aux + p0), ma = __ldg(st.up_mode + p0);
+        const int ub = __ldg(st.up_aux + p0 + 1), mb = __ldg(st.up_mode + p0 + 1);
+        const int sa = __ldg(st.up_site + p0), sb = __ldg(st.up_site + p0 + 1);
+        const size_t ra = ((size_t)ua * S + s) * B + bg + lane;
+        const size_t rb = ((size_t)ub * S + s) * B + bg + lane;
+        ST ya[NB], yb[NB];
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+          if (ok[j]) {
+            ya[j] = yin[ra + 32 * j];
+            yb[j] = yin[rb + 32 * j];
+          }
+        }
+        const T* upa = upcT + (size_t)ma * B + bg + lane;
+        const T* upb = upcT + (size_t)mb * B + bg + lane;
+        const T corra = sa == s ? P::gwv(st, ma) : czero<T>();
+        const T corrb = sb == s ? P::gwv(st, mb) : czero<T>();
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+          if (ok[j]) {
+            k[j] = cfma(csub(upa[32 * j], corra), cv<T>(ya[j]), k[j]);
+            k[j] = cfma(csub(upb[32 * j], corrb), cv<T>(yb[j]), k[j]);
           }
         }
       }
-      for (int q = h0; q < h1; ++q) {
-        const T hv = P::hval(st, q);
-        const size_t rb = ((size_t)a * S + st.h_col[q]) * B + bg + lane;
+    }
+    for (int p = p0; p < u1; ++p) {
+      const int u = st.up_aux[p], m = st.up_mode[p];
+      const size_t rb = ((size_t)u * S + s) * B + bg + lane;
+      const T* up = upcT + (size_t)m * B + bg + lane;
+      if (SITE) {
+        const bool hit = st.up_site[p] == s;
+        const T corr = hit ? P::gwv(st, m) : czero<T>();
 #pragma unroll
         for (int j = 0; j < NB; ++j)
-          if (ok[j]) k[j] = cfma(hv, cv<T>(yin[rb + 32 * j]), k[j]);
+          if (ok[j]) k[j] = cfma(csub(up[32 * j], corr), cv<T>(yin[rb + 32 * j]), k[j]);
+      } else {
+#pragma unroll
+        for (int j = 0; j < NB; ++j)
+          if (ok[j]) k[j] = cfma(up[32 * j], cv<T>(yin[rb + 32 * j]), k[j]);
+        const int base = st.mode_lop[m] * (S + 1);
+        const int q0 = st.l_ptr[base + s], q1 = st.l_ptr[base + s + 1];
+        for (int q = q0; q < q1; ++q) {
+          const T lv = cmul(P::gw(st, m), P::lval(st, q));
+          const size_t rb2 = ((size_t)u * S + st.l_col[q]) * B + bg + lane;
+#pragma unroll
+          for (int j = 0; j < NB; ++j)
+            if (ok[j]) k[j] = csub(k[j], cmul(lv, cv<T>(yin[rb2 + 32 * j])));
+        }
       }
-      int p0 = u0;
+    }
+    for (int p = d0; p < d1; ++p) {
       if (SITE) {
-        // two neighbours per iteration: their 2 x NB row segments are loaded
-        // before either is consumed, so twice as many loads are in flight
-        for (; p0 + 2 <= u1; p0 += 2) {
-          const int ua = __ldg(st.up_aux + p0), ma = __ldg(st.up_mode + p0);
-          const int ub = __ldg(st.up_aux + p0 + 1), mb = __ldg(st.up_mode + p0 + 1);
-          const int sa = __ldg(st.up_site + p0), sb = __ldg(st.up_site + p0 + 1);
-          const size_t ra = ((size_t)ua * S + s) * B + bg + lane;
-          const size_t rb = ((size_t)ub * S + s) * B + bg + lane;
-          ST ya[NB], yb[NB];
+        if (__ldg(st.dn_site + p) != s) continue;
+        const int d = __ldg(st.dn_aux + p);
+        const T cf = P::dncs(st, p);
+        const size_t rb = ((size_t)d * S + s) * B + bg + lane;
 #pragma unroll
-          for (int j = 0; j < NB; ++j) {
-            if (ok[j]) {
-              ya[j] = yin[ra + 32 * j];
-              yb[j] = yin[rb + 32 * j];
-            }
-          }
-          const T* upa = upcT + (size_t)ma * B + bg + lane;
-          const T* upb = upcT + (size_t)mb * B + bg + lane;
-          const T corra = sa == s ? P::gwv(st, ma) : czero<T>();
-          const T corrb = sb == s ? P::gwv(st, mb) : czero<T>();
-#pragma unroll
-          for (int j = 0; j < NB; ++j) {
-            if (ok[j]) {
-              k[j] = cfma(csub(upa[32 * j], corra), cv<T>(ya[j]), k[j]);
-              k[j] = cfma(csub(upb[32 * j], corrb), cv<T>(yb[j]), k[j]);
-            }
-          }
-        }
-      }
-      for (int p = p0; p < u1; ++p) {
-        const int u = st.up_aux[p], m = st.up_mode[p];
-        const size_t rb = ((size_t)u * S + s) * B + bg + lane;
-        const T* up = upcT + (size_t)m * B + bg + lane;
-        if (SITE) {
-          const bool hit = st.up_site[p] == s;
-          const T corr = hit ? P::gwv(st, m) : czero<T>();
-#pragma unroll
-          for (int j = 0; j < NB; ++j)
-            if (ok[j]) k[j] = cfma(csub(up[32 * j], corr), cv<T>(yin[rb + 32 * j]), k[j]);
-        } else {
-#pragma unroll
-          for (int j = 0; j < NB; ++j)
-            if (ok[j]) k[j] = cfma(up[32 * j], cv<T>(yin[rb + 32 * j]), k[j]);
-          const int base = st.mode_lop[m] * (S + 1);
-          const int q0 = st.l_ptr[base + s], q1 = st.l_ptr[base + s + 1];
-          for (int q = q0; q < q1; ++q) {
-            const T lv = cmul(P::gw(st, m), P::lval(st, q));
-            const size_t rb2 = ((size_t)u * S + st.l_col[q]) * B + bg + lane;
-#pragma unroll
-            for (int j = 0; j < NB; ++j)
-              if (ok[j]) k[j] = csub(k[j], cmul(lv, cv<T>(yin[rb2 + 32 * j])));
-          }
-        }
-      }
-      for (int p = d0; p < d1; ++p) {
-        if (SITE) {
-          if (__ldg(st.dn_site + p) != s) continue;
-          const int d = __ldg(st.dn_aux + p);
-          const T cf = P::dncs(st, p);
-          const size_t rb = ((size_t)d * S + s) * B + bg + lane;
+        for (int j = 0; j < NB; ++j)
+          if (ok[j]) k[j] = cfma(cf, cv<T>(yin[rb + 32 * j]), k[j]);
+      } else {
+        const int d = st.dn_aux[p], m = st.dn_mode[p];
+        const int base = st.mode_lop[m] * (S + 1);
+        const int q0 = st.lh_ptr[base + s], q1 = st.lh_ptr[base + s + 1];
+        for (int q = q0; q < q1; ++q) {
+          const T cf = cmul(P::dncoef(st, p), P::lhval(st, q));
+          const size_t rb = ((size_t)d * S + st.lh_col[q]) * B + bg + lane;
 #pragma unroll
           for (int j = 0; j < NB; ++j)
             if (ok[j]) k[j] = cfma(cf, cv<T>(yin[rb + 32 * j]), k[j]);
-        } else {
-          const int d = st.dn_aux[p], m = st.dn_mode[p];
-          const int base = st.mode_lop[m] * (S + 1);
-          const int q0 = st.lh_ptr[base + s], q1 = st.lh_ptr[base + s + 1];
-          for (int q = q0; q < q1; ++q) {
-            const T cf = cmul(P::dncoef(st, p), P::lhval(st, q));
-            const size_t rb = ((size_t)d * S + st.lh_col[q]) * B + bg + lane;
-#pragma unroll
-            for (int j = 0; j < NB; ++j)
-              if (ok[j]) k[j] = cfma(cf, cv<T>(yin[rb + 32 * j]), k[j]);
-          }
         }
       }
-      // Every load of the RK update (phi, the accumulated slope, the pending
-      // scale) of all NB elements is issued before the first store: phi, acc
-      // and the outputs may alias as far as the compiler knows, so otherwise
-      // each element would wait for a DRAM round trip of its own.
-      PT ph[NB];
-      ST accv[NB];
-      double sc[NB];
-#pragma unroll
-      for (int j = 0; j < NB; ++j) {
-        ph[j] = PT{};
-        accv[j] = ST{};
-        sc[j] = 1.0;
-        if (!ok[j]) continue;
-        const int b = bg + lane + 32 * j;
-        const size_t e = rowa + b;
-        sc[j] = scaleB[b];
-        // stages 1-3 read phi once (pure stream); stage 0 also gathers phi
-        if (stage != 4) ph[j] = stage == 0 ? phi[e] : __ldcs(phi + e);
-        if (stage >= 1 && stage <= 3) accv[j] = acc_load<true>(acc + e);
-      }
-#pragma unroll
-      for (int j = 0; j < NB; ++j) {
-        if (!ok[j]) continue;
-        const size_t e = rowa + bg + lane + 32 * j;
-        T kk = k[j];
-        if (stage == 0 || stage == 4) kk = cscale(kk, (R)sc[j]);
-        const PT p = stage == 4 ? PT{} : cscale(ph[j], (decltype(PT{}.x))sc[j]);
-        rk_finish<true, T, ST, PT>(stage, h, kk, p, accv[j], acc, yout, phi, shadow, e);
-      }
     }
+    PT ph[NB];
+    ST accv[NB];
+    double sc[NB];
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+      const int o = buf * CH + lane + 32 * j;
+      ph[j] = PT{};
+      accv[j] = ST{};
+      sc[j] = 1.0;
+      if (!ok[j]) continue;
+      sc[j] = scaleB[bg + lane + 32 * j];
+      if (want_phi) ph[j] = ph_s[o];
+      if (want_acc) accv[j] = ac_s[o];
+    }
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+      if (!ok[j]) continue;
+      const size_t e = rowa + bg + lane + 32 * j;
+      T kk = k[j];
+      if (stage == 0 || stage == 4) kk = cscale(kk, (R)sc[j]);
+      const PT p = stage == 4 ? PT{} : cscale(ph[j], (decltype(PT{}.x))sc[j]);
+      rk_finish<true, T, ST, PT>(stage, h, kk, p, accv[j], acc, yout, phi, shadow, e);
+    }
+    t = tn;
+    ci = cn;
+    buf ^= 1;
   }
+  cp_async_wait<0>();
 }
 
 // -------------------------------------------------- narrow stage kernel ----
@@ -927,7 +985,19 @@ static void launch_wide(const hops_structure* st, int B, int stage, double h, co
   const unsigned n_as = (unsigned)st->n_hier * st->n_state;
   const long nchunk = (B + 32 * NB - 1) / (32 * NB);
   const int grid = grid_for_warps(chunk_major ? (long)n_as * nchunk : (long)n_as);
-  k_wide<R, ST, PT, SITE, NB><<<grid, 256, 0, s>>>(*st, B, stage, h, (const ST*)yin, (ST*)yout,
+  constexpr size_t smem = wide_smem_bytes<ST, PT, NB>(256 / 32);
+  if (smem > 48 * 1024) {
+    // opt in to the large shared-memory carve-out once per device
+    static int set_for = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (set_for != dev) {
+      cudaFuncSetAttribute(k_wide<R, ST, PT, SITE, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      set_for = dev;
+    }
+  }
+  k_wide<R, ST, PT, SITE, NB><<<grid, 256, smem, s>>>(*st, B, stage, h, (const ST*)yin, (ST*)yout,
                                                    (PT*)phi, (ST*)shadow, (ST*)acc, ws,
                                                    FastDiv((unsigned)st->n_state), FastDiv(n_as),
                                                    chunk_major);
