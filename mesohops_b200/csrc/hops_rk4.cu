@@ -307,20 +307,6 @@ __device__ __forceinline__ void rk_update(int stage, double h, T k, PT ph, ST* a
   rk_finish<GHINT, T, ST, PT>(stage, h, k, ph, accv, acc, yout, phi, shadow, e);
 }
 
-// ---------------------------------------------------- wide stage kernel ----
-// B >= 32 trajectories: one warp per (aux a, state s, chunk of 32*NB
-// trajectories); lane l owns the trajectories bg + l + 32 j, j < NB.
-// Connection lists, coefficients and the site test are warp-uniform and loaded
-// once per neighbour for the whole chunk; every Y load is a coalesced
-// 32-trajectory segment and the NB loads per neighbour are in flight together.
-// chunk_major: the chunk is the outermost task index, so the warps in flight
-// all gather from one chunk's slice of Y, which stays resident in L2 (a slice
-// of 32 trajectories of the 20-site ring is 54 MB in complex64); otherwise each
-// warp walks every chunk of its (a, s).
-// The stage is bound by load latency at the occupancy registers allow: with
-// NB <= 2 the kernel is held to 64 registers (4 CTAs, 32 warps per SM), which
-// measured faster than the extra registers it would otherwise take; NB >= 4
-// keeps every segment's loads in flight in registers and is left uncapped.
 // Asynchronous global -> shared copies (cp.async, no register staging).
 template <int BYTES>
 __device__ __forceinline__ void cp_async(void* sdst, const void* gsrc) {
@@ -346,8 +332,26 @@ constexpr size_t wide_smem_bytes(int warps) {
   return (size_t)warps * 2 * 32 * NB * (sizeof(PT) + 2 * sizeof(ST));
 }
 
+// ---------------------------------------------------- wide stage kernel ----
+// B >= 32 trajectories: one warp per (aux a, state s, chunk of 32*NB
+// trajectories); lane l owns the trajectories bg + l + 32 j, j < NB.
+// Connection lists, coefficients and the site test are warp-uniform and loaded
+// once per neighbour for the whole chunk; every Y load is a coalesced
+// 32-trajectory segment and the NB loads per neighbour are in flight together.
+// chunk_major: the chunk is the outermost task index, so the warps in flight
+// all gather from one chunk's slice of Y, which stays resident in L2 (a slice
+// of 32 trajectories of the 20-site ring is 54 MB in complex64); otherwise each
+// warp walks every chunk of its (a, s).
+// The stage is bound by load latency at the occupancy registers allow.  NB <= 2
+// is held to 64 registers (4 CTAs of 256 threads, 32 warps per SM), NB = 4 to
+// 128 (4 CTAs of 128 threads); both measured faster than the registers the
+// compiler would otherwise take.  NB = 8 is left nearly uncapped.
+// CTA size of k_wide: 256 threads for NB <= 2, else 128 (finer occupancy
+// steps at the register counts the wider tasks take).
+constexpr int wide_threads(int nb) { return nb <= 2 ? 256 : 128; }
+
 template <typename R, typename ST, typename PT, bool SITE, int NB>
-__global__ void __launch_bounds__(256, NB <= 2 ? 4 : (NB == 4 ? 2 : 1))
+__global__ void __launch_bounds__(wide_threads(NB), NB <= 2 ? 4 : (NB == 4 ? 4 : 2))
     k_wide(hops_structure st, int B, int stage, double h, const ST* __restrict__ yin,
            ST* __restrict__ yout, PT* phi, ST* shadow, ST* acc, const double* __restrict__ ws,
            FastDiv divS, FastDiv divAS, int chunk_major) {
@@ -984,8 +988,9 @@ static void launch_wide(const hops_structure* st, int B, int stage, double h, co
                         int chunk_major, cudaStream_t s) {
   const unsigned n_as = (unsigned)st->n_hier * st->n_state;
   const long nchunk = (B + 32 * NB - 1) / (32 * NB);
-  const int grid = grid_for_warps(chunk_major ? (long)n_as * nchunk : (long)n_as);
-  constexpr size_t smem = wide_smem_bytes<ST, PT, NB>(256 / 32);
+  constexpr int threads = wide_threads(NB);
+  const int grid = (256 / threads) * grid_for_warps(chunk_major ? (long)n_as * nchunk : (long)n_as);
+  constexpr size_t smem = wide_smem_bytes<ST, PT, NB>(threads / 32);
   if (smem > 48 * 1024) {
     // opt in to the large shared-memory carve-out once per device
     static int set_for = -1;
@@ -997,7 +1002,7 @@ static void launch_wide(const hops_structure* st, int B, int stage, double h, co
       set_for = dev;
     }
   }
-  k_wide<R, ST, PT, SITE, NB><<<grid, 256, smem, s>>>(*st, B, stage, h, (const ST*)yin, (ST*)yout,
+  k_wide<R, ST, PT, SITE, NB><<<grid, threads, smem, s>>>(*st, B, stage, h, (const ST*)yin, (ST*)yout,
                                                    (PT*)phi, (ST*)shadow, (ST*)acc, ws,
                                                    FastDiv((unsigned)st->n_state), FastDiv(n_as),
                                                    chunk_major);
