@@ -236,7 +236,7 @@ def run_gpu(args):
                 traffic = int(line.split(":")[1])
     result["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                           "unit": "GB/s", "frac": round(achieved / peak, 4),
-                          "traffic": traffic, "kernel": "k_stage (streaming RK4 stage)",
+                          "traffic": traffic, "kernel": "k_wide (streaming RK4 stage)",
                           "algorithmic_bytes_per_launch": int(bytes_launch),
                           "avg_launch_ms": round(avg_ms, 5),
                           "stage_share_of_step": round(tot.value / kr / (ms / K), 3),
