@@ -132,10 +132,11 @@ struct StageIO {
 // coefficients for one trajectory.  Restates eom/eom_functions.py:11-213 and
 // the z_mem half of integrator/integrator_rk.py:10-75.
 //   get(a, s): stage-input element (aux a, state s) of this trajectory as double2.
+//   getf(f, s): the same for the f-th first-order aux (st.first_aux[f]).
 // All threads of the block must call it; red / sh are shared scratch
 // (red >= 32 doubles, sh >= 4*L + 2 doubles).
-template <class Get>
-__device__ void stage_scalars(const hops_structure& st, const StageIO& io, Get get,
+template <class Get, class GetF>
+__device__ void stage_scalars(const hops_structure& st, const StageIO& io, Get get, GetF getf,
                               double* red, double* sh) {
   const int S = st.n_state, M = st.n_mode, L = st.n_lop;
   ScalarLayout lay(S, M, L);
@@ -202,17 +203,17 @@ __device__ void stage_scalars(const hops_structure& st, const StageIO& io, Get g
       part_re = d.x;
     }
     for (int f = threadIdx.x; f < st.n_first; f += blockDim.x) {
-      const int a = st.first_aux[f], m = st.first_mode[f], j = st.mode_lop[m];
+      const int m = st.first_mode[f], j = st.mode_lop[m];
       if (!st.lop_active[j]) continue;
       const int base = j * (S + 1);
       double2 t1 = mk(0.0, 0.0), t2 = mk(0.0, 0.0);
       for (int r = 0; r < S; ++r) {
         double2 p0 = get(0, r);
-        t2 = cadd(t2, cconjmul(p0, get(a, r)));
+        t2 = cadd(t2, cconjmul(p0, getf(f, r)));
         int q0 = st.l_ptr[base + r], q1 = st.l_ptr[base + r + 1];
         if (q0 == q1) continue;
         double2 row = mk(0.0, 0.0);
-        for (int q = q0; q < q1; ++q) row = cfma(ld2(st.l_val, q), get(a, st.l_col[q]), row);
+        for (int q = q0; q < q1; ++q) row = cfma(ld2(st.l_val, q), getf(f, st.l_col[q]), row);
         t1 = cadd(t1, cconjmul(p0, row));
       }
       double2 gw = ld2(st.mode_gw, m);
@@ -274,6 +275,12 @@ __device__ void stage_scalars(const hops_structure& st, const StageIO& io, Get g
     ws[lay.n2()] = n2;
   }
   __syncthreads();
+}
+
+template <class Get>
+__device__ void stage_scalars(const hops_structure& st, const StageIO& io, Get get, double* red,
+                              double* sh) {
+  stage_scalars(st, io, get, [&](int f, int s) { return get(st.first_aux[f], s); }, red, sh);
 }
 
 }  // namespace hops

@@ -638,7 +638,7 @@ template <typename R, typename ST, typename PT>
 __global__ void __launch_bounds__(128) k_scalars(hops_structure st, hops_batch bt, int stage, int it,
                                                  double h, const void* yin, int recompute_scale,
                                                  double* psi_prev, const float* z1s,
-                                                 const float* z2s, double* dz_out) {
+                                                 const float* z2s, double* dz_out, int stage_rows) {
   using T = typename Prec<R>::T;
   extern __shared__ double shm[];
   double* red = shm;
@@ -699,7 +699,23 @@ __global__ void __launch_bounds__(128) k_scalars(hops_structure st, hops_batch b
     const size_t i = ((size_t)a * S + s) * B + b;
     return from_phi ? cscale(to_d(ph[i]), sc) : to_d(y[i]);
   };
-  stage_scalars(st, io, get, red, sh);
+  if (stage_rows) {
+    // The rows the scalars read (psi_0 and the first-order aux) are loaded
+    // once, all in flight together, instead of by dependent loads in the
+    // per-mode loops.
+    double2* rows = reinterpret_cast<double2*>(sh + 4 * L + 2);
+    const int nr = (1 + st.n_first) * S;
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) {
+      const int f = i / S, r = i - f * S;
+      rows[i] = get(f == 0 ? 0 : st.first_aux[f - 1], r);
+    }
+    __syncthreads();
+    stage_scalars(
+        st, io, [&](int a, int r) { return a == 0 ? rows[r] : get(a, r); },
+        [&](int f, int r) { return rows[(size_t)(f + 1) * S + r]; }, red, sh);
+  } else {
+    stage_scalars(st, io, get, red, sh);
+  }
   publish(st, bl, bt.work, B, b, ws);
 }
 
@@ -1058,11 +1074,20 @@ static size_t scalar_smem(const hops_structure* st) {
   return (size_t)(32 + 4 * st->n_lop + 2) * sizeof(double);
 }
 
+// Shared memory of k_scalars with the rows of psi_0 and the first-order aux
+// staged (stage_rows = 1), or 0 when they do not fit in 48 KB.
+static size_t scalar_smem_rows(const hops_structure* st) {
+  const size_t b = scalar_smem(st) + (size_t)(1 + st->n_first) * st->n_state * 16;
+  return b <= 48 * 1024 ? b : 0;
+}
+
 template <typename R, typename ST, typename PT>
 static int propagate_impl(const hops_structure* st, hops_batch* bt, int32_t it0, int32_t di,
                           int32_t n_steps, double h, double* psi_out, cudaStream_t s) {
   const int B = bt->n_traj, S = st->n_state;
-  const size_t smem = scalar_smem(st);
+  const size_t smem_rows = scalar_smem_rows(st);
+  const int stage_rows = smem_rows ? 1 : 0;
+  const size_t smem = stage_rows ? smem_rows : scalar_smem(st);
   const bool normalized = bt->eom == HOPS_EOM_NORMALIZED_NONLINEAR;
   const size_t psi_stride = (size_t)B * S * 2;
   void* shadow = bt->precision == HOPS_PREC_MIXED ? bt->phi_lo : nullptr;
@@ -1077,7 +1102,7 @@ static int propagate_impl(const hops_structure* st, hops_batch* bt, int32_t it0,
       const int recompute = (i == 0 && n > 0 && normalized) ? 1 : 0;
       double* psi_prev = (i == 0 && n > 0 && psi_out) ? psi_out + (size_t)(n - 1) * psi_stride : nullptr;
       k_scalars<R, ST, PT><<<B, 128, smem, s>>>(*st, *bt, i, it, h, yin, recompute, psi_prev,
-                                                nullptr, nullptr, nullptr);
+                                                nullptr, nullptr, nullptr, stage_rows);
       LAUNCH_CHECK();
       int rc = run_stage<R, ST, PT>(st, B, i, h, yin, yout, bt->phi, shadow, bt->acc, bt->work,
                                     bt->status, s);
@@ -1140,8 +1165,9 @@ extern "C" int hops_rk4_propagate(const hops_structure* st, hops_batch* bt, int3
 template <typename R, typename ST, typename PT>
 static int dsys_impl(const hops_structure* st, hops_batch* bt, const float* z1, const float* z2,
                      void* dphi, double* dz, cudaStream_t s) {
-  k_scalars<R, ST, PT><<<bt->n_traj, 128, scalar_smem(st), s>>>(*st, *bt, 4, 0, 0.0, bt->phi, 0,
-                                                                nullptr, z1, z2, dz);
+  const size_t smem_rows = scalar_smem_rows(st);
+  k_scalars<R, ST, PT><<<bt->n_traj, 128, smem_rows ? smem_rows : scalar_smem(st), s>>>(
+      *st, *bt, 4, 0, 0.0, bt->phi, 0, nullptr, z1, z2, dz, smem_rows ? 1 : 0);
   LAUNCH_CHECK();
   // stage 4 reads the state itself (mixed mode: its complex64 copy)
   const void* yin = bt->precision == HOPS_PREC_MIXED ? bt->phi_lo : bt->phi;
