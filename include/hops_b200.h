@@ -21,6 +21,7 @@
  *                               (possibly uneven) basis, all steps in one launch
  *   hops_noise_filter        <- noise/hops_noise.py:630-716 (_construct_correlated_noise)
  *                               with hops_noise.py:167-192,232-247 (alpha, complex64)
+ *   hops_noise_window_mean   <- integrator/integrator_rk.py:115-128 (effective noise)
  */
 #ifndef HOPS_B200_H
 #define HOPS_B200_H
@@ -271,6 +272,20 @@ int hops_noise_filter(const double* alpha_dev, const float* z_dev, int32_t n_lop
 
 /* Doubles of device work area hops_noise_filter needs (work_dev). */
 size_t hops_noise_filter_work_doubles(int32_t n_lop, int32_t n_t);
+
+/* Effective noise of EFFECTIVE_NOISE_INTEGRATION: replaces the window means of
+ * integrator/integrator_rk.py:115-128 (np.mean over complex64 samples).
+ * noise_dev: complex64 [rows][n_t]; out_dev: complex64 [rows][n_out] with
+ * out[r][w] = mean(noise[r][start + w*k .. start + (w+1)*k - 1]), summed in
+ * numpy's pairwise order and divided by k in single precision, so the means
+ * are bit-identical to the reference's.  real_only: FLAG_REAL noise (the real
+ * parts averaged as float32, imaginary parts 0).  The RK slots of step n are
+ * then windows 2n, 2n+1, 2n+2 of the series that starts at the step's time,
+ * i.e. hops_rk4_propagate with it0 = 0, di = 1 on out_dev.
+ * Requires start + n_out*k <= n_t. */
+int hops_noise_window_mean(const float* noise_dev, int64_t rows, int32_t n_t, int32_t start,
+                           int32_t k, int32_t n_out, int32_t real_only, float* out_dev,
+                           void* stream);
 
 /*
  * Shape of the batched stage kernel: 32*nb trajectories per warp task and

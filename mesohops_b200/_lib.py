@@ -102,6 +102,7 @@ def lib():
     L.hops_noise_filter.argtypes = [_p, _p, _i, _i, _p, _p, _p, C.POINTER(C.c_int64), _p]
     L.hops_noise_filter_work_doubles.restype = C.c_size_t
     L.hops_noise_filter_work_doubles.argtypes = [_i, _i]
+    L.hops_noise_window_mean.argtypes = [_p, C.c_int64, _i, _i, _i, _i, _i, _p, _p]
     L.hops_noalloc_scratch_bytes.restype = C.c_size_t
     L.hops_noalloc_scratch_bytes.argtypes = [C.POINTER(HopsStructure), _i, _i]
     L.hops_rk4_propagate_noalloc.argtypes = [C.POINTER(HopsStructure), _i, _i, _i, _p, _p, _p,
@@ -141,4 +142,4 @@ def exported_symbols():
             "hops_kernel_timing_read", "hops_noalloc_scratch_bytes",
             "hops_rk4_propagate_noalloc", "hops_stage_tuning", "hops_flux_errors",
             "hops_flux_errors_smem_doubles", "hops_tri_max_depth", "hops_tri_pass1",
-            "hops_tri_pass2"]
+            "hops_tri_pass2", "hops_noise_window_mean"]

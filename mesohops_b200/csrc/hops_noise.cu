@@ -172,3 +172,115 @@ extern "C" int hops_noise_filter(const double* alpha_dev, const float* z_dev, in
   cufftDestroy(plan);
   return rc;
 }
+
+// ------------------------------------------------ effective-noise windows ----
+// EFFECTIVE_NOISE_INTEGRATION (integrator/integrator_rk.py:115-128) replaces
+// the noise samples at t, t + tau/2, t + tau by the means of three windows of
+// k = tau / (2 TAU) consecutive complex64 samples.  The reference takes them
+// with numpy's mean, so the sums follow numpy's pairwise summation exactly:
+// fewer than 8 floats added in order, up to 128 floats in 8 running partial
+// sums (for complex data: 4 complex partials) combined as ((0+1)+(2+3)) +
+// ((4+5)+(6+7)) with the tail added in order, larger blocks split in halves
+// rounded down to 8 floats; then each component is divided by k in single
+// precision.  With real_only (FLAG_REAL noise: numpy sums the float32 real
+// parts alone) the real parts use the float32 form of the same scheme.
+__device__ void pw_complex(const float2* a, int m, float& rr, float& ri) {
+  const int n = 2 * m;
+  if (n < 8) {
+    rr = -0.0f;
+    ri = -0.0f;
+    for (int i = 0; i < m; ++i) {
+      rr = __fadd_rn(rr, a[i].x);
+      ri = __fadd_rn(ri, a[i].y);
+    }
+    return;
+  }
+  if (n <= 128) {
+    float r[8] = {a[0].x, a[0].y, a[1].x, a[1].y, a[2].x, a[2].y, a[3].x, a[3].y};
+    int i = 4;
+    for (; i + 4 <= m; i += 4) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        r[2 * j] = __fadd_rn(r[2 * j], a[i + j].x);
+        r[2 * j + 1] = __fadd_rn(r[2 * j + 1], a[i + j].y);
+      }
+    }
+    rr = __fadd_rn(__fadd_rn(r[0], r[2]), __fadd_rn(r[4], r[6]));
+    ri = __fadd_rn(__fadd_rn(r[1], r[3]), __fadd_rn(r[5], r[7]));
+    for (; i < m; ++i) {
+      rr = __fadd_rn(rr, a[i].x);
+      ri = __fadd_rn(ri, a[i].y);
+    }
+    return;
+  }
+  int n2 = n / 2;
+  n2 -= n2 % 8;
+  const int m2 = n2 / 2;
+  float r1, i1, r2, i2;
+  pw_complex(a, m2, r1, i1);
+  pw_complex(a + m2, m - m2, r2, i2);
+  rr = __fadd_rn(r1, r2);
+  ri = __fadd_rn(i1, i2);
+}
+
+// Real parts a[i].x, i < n, as numpy sums a float32 row.
+__device__ float pw_real(const float2* a, int n) {
+  if (n < 8) {
+    float r = -0.0f;
+    for (int i = 0; i < n; ++i) r = __fadd_rn(r, a[i].x);
+    return r;
+  }
+  if (n <= 128) {
+    float r[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) r[j] = a[j].x;
+    int i = 8;
+    for (; i + 8 <= n; i += 8) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) r[j] = __fadd_rn(r[j], a[i + j].x);
+    }
+    float s = __fadd_rn(__fadd_rn(__fadd_rn(r[0], r[1]), __fadd_rn(r[2], r[3])),
+                        __fadd_rn(__fadd_rn(r[4], r[5]), __fadd_rn(r[6], r[7])));
+    for (; i < n; ++i) s = __fadd_rn(s, a[i].x);
+    return s;
+  }
+  int n2 = n / 2;
+  n2 -= n2 % 8;
+  return __fadd_rn(pw_real(a, n2), pw_real(a + n2, n - n2));
+}
+
+// out[r][w] = mean(in[r][start + w k .. start + (w+1) k - 1]), w < n_out.
+__global__ void k_window_mean(const float2* in, long rows, int n_t, int start, int k, int n_out,
+                              int real_only, float2* out) {
+  const long total = rows * (long)n_out;
+  const float fk = (float)k;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total;
+       q += (long)gridDim.x * blockDim.x) {
+    const long r = q / n_out;
+    const int w = (int)(q - r * n_out);
+    const float2* a = in + r * n_t + start + (long)w * k;
+    float sr, si = 0.0f;
+    if (real_only)
+      sr = pw_real(a, k);
+    else
+      pw_complex(a, k, sr, si);
+    out[q] = make_float2(__fdiv_rn(sr, fk), real_only ? 0.0f : __fdiv_rn(si, fk));
+  }
+}
+
+extern "C" int hops_noise_window_mean(const float* noise_dev, int64_t rows, int32_t n_t,
+                                      int32_t start, int32_t k, int32_t n_out,
+                                      int32_t real_only, float* out_dev, void* stream) {
+  if (!noise_dev || !out_dev || rows < 0 || n_t <= 0 || start < 0 || k < 1 || n_out < 0 ||
+      (int64_t)start + (int64_t)n_out * k > n_t)
+    return nerr(HOPS_EINVAL, "hops_noise_window_mean: windows [%d, %d + %d*%d) outside %d samples",
+                start, start, n_out, k, n_t);
+  if (rows == 0 || n_out == 0) return HOPS_OK;
+  const long total = rows * (long)n_out;
+  k_window_mean<<<grid_for(total), 128, 0, (cudaStream_t)stream>>>(
+      reinterpret_cast<const float2*>(noise_dev), rows, n_t, start, k, n_out, real_only,
+      reinterpret_cast<float2*>(out_dev));
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return nerr(HOPS_ECUDA, "window mean launch: %s", cudaGetErrorString(e));
+  return HOPS_OK;
+}

@@ -77,6 +77,23 @@ def filter_on_device(alpha, z_raw, device):
     return out64, int(nneg.value)
 
 
+def window_means(noise, start, k, n_out, real_only=False):
+    """Means of n_out consecutive windows of k samples from sample `start` of
+    each row of a complex64 device tensor [..., n_t], bit-identical to numpy's
+    mean of the same complex64 (real_only: float32 real parts) samples
+    (hops_noise_window_mean)."""
+    noise = noise.contiguous()
+    n_t = int(noise.shape[-1])
+    rows = noise.numel() // max(n_t, 1)
+    out = torch.empty(tuple(noise.shape[:-1]) + (int(n_out),), dtype=torch.complex64,
+                      device=noise.device)
+    rc = _lib.lib().hops_noise_window_mean(
+        noise.data_ptr(), rows, n_t, int(start), int(k), int(n_out), 1 if real_only else 0,
+        out.data_ptr(), torch.cuda.current_stream(noise.device).cuda_stream)
+    _lib.check(rc, "hops_noise_window_mean")
+    return out
+
+
 class HopsNoise:
     """One noise trajectory (noise 1 or noise 2) of a HOPS trajectory."""
 
@@ -159,6 +176,21 @@ class HopsNoise:
             noise = torch.complex(noise.real, torch.zeros_like(noise.real))
         self._dev = noise.contiguous()
         return self._dev
+
+    def effective(self, t0, tau, n_steps):
+        """Effective noise of EFFECTIVE_NOISE_INTEGRATION for n_steps RK4 steps from t0
+        (integrator_rk.py:115-128): complex64 device tensor [n_lop, 2 n_steps + 1] of
+        the means of consecutive windows of tau / (2 TAU) samples starting at t0, so
+        the RK slots of step n are windows 2n, 2n+1, 2n+2.  None for ZERO noise."""
+        if self._dev is None:
+            return None
+        k = int(round(tau * 0.5 / self.param["TAU"]))
+        start = self.time_index(t0)
+        n_out = 2 * int(n_steps) + 1
+        if start + n_out * k > self.n_t:
+            raise UnsupportedRequest("t-samples outside of the defined t-axis",
+                                     "NoiseModel.get_noise()")
+        return window_means(self._dev, start, k, n_out, bool(self.param["FLAG_REAL"]))
 
     def host(self):
         if self._host is None and self._dev is not None:

@@ -81,8 +81,6 @@ class HopsTrajectory:
         if self.integration_param["INTEGRATOR"] != "RUNGE_KUTTA":
             raise UnsupportedRequest("Integrator of type " + str(self.integration_param["INTEGRATOR"]),
                                      type(self).__name__)
-        if self.integration_param["EFFECTIVE_NOISE_INTEGRATION"]:
-            raise UnsupportedRequest("EFFECTIVE_NOISE_INTEGRATION", "mesohops_b200 HopsTrajectory")
         self.integrator_step = 0.5
         self.device_param = dict(DEVICE_DICT_DEFAULT)
         self.device_param.update(device_param or {})
@@ -102,6 +100,9 @@ class HopsTrajectory:
         psi_0 = np.array(psi_0, dtype=np.complex128)
         dev = torch.device(self.device_param["DEVICE"])
         if self.eom_param["ADAPTIVE"]:
+            if self.effective_noise_integration:
+                raise UnsupportedRequest("EFFECTIVE_NOISE_INTEGRATION with an adaptive basis",
+                                         "mesohops_b200 HopsTrajectory")
             self._initialize_adaptive(psi_0, dev)
             self.storage.metadata["INITIALIZATION_TIME"] = timer.time() - t0
             self.__initialized__ = True
@@ -129,8 +130,12 @@ class HopsTrajectory:
         self.storage.metadata["INITIALIZATION_TIME"] = timer.time() - t0
         self.__initialized__ = True
 
-    def _bind_noise(self, n1, n2):
-        self._n1, self._n2 = n1, n2
+    def _bind_noise(self, n1, n2, keep=True):
+        """Noise rows the kernels read; keep=False binds a temporary view (the
+        effective-noise windows of one propagate call) without replacing the
+        trajectory's own noise."""
+        if keep:
+            self._n1, self._n2 = n1, n2
         if self.kernel == "resident":
             self._traj.set_noise(n1, n2)
         else:
@@ -232,19 +237,31 @@ class HopsTrajectory:
                 _adaptive.drive(self.adaptive_step_gen(float(t), tau, index_t), dev)
             self.storage.metadata["LIST_PROPAGATION_TIME"].append(timer.time() - t_start)
             return
-        it0 = self.noise1.time_index(t0)
-        di = int(round(tau * 0.5 / self.noise1.param["TAU"]))
-        self._align_noise2(it0, di, n_steps)
+        if self.effective_noise_integration:
+            # window means of the noise (integrator_rk.py:115-128) on a half-step grid
+            # that starts at t0: slots of step n are windows 2n, 2n+1, 2n+2
+            self._bind_noise(self.noise1.effective(t0, tau, n_steps),
+                             self.noise2.effective(t0, tau, n_steps), keep=False)
+            it0, di = 0, 1
+        else:
+            it0 = self.noise1.time_index(t0)
+            di = int(round(tau * 0.5 / self.noise1.param["TAU"]))
+            self._align_noise2(it0, di, n_steps)
         h = tau / hbar
         dev = self.dstruct.device
         psi_dev = torch.empty((n_steps, self.n_state), dtype=torch.complex128, device=dev)
-        if self.kernel == "resident":
-            st = self._runner.run([self._traj], it0, di, n_steps, h, psi_out=[psi_dev])
-            if st[0] != 0:
-                raise TrajectoryError("non-finite state during propagation")
-        else:
-            self._traj.propagate(it0, di, n_steps, h, psi_out=psi_dev.view(n_steps, 1, self.n_state))
-            self._traj.check_status()
+        try:
+            if self.kernel == "resident":
+                st = self._runner.run([self._traj], it0, di, n_steps, h, psi_out=[psi_dev])
+                if st[0] != 0:
+                    raise TrajectoryError("non-finite state during propagation")
+            else:
+                self._traj.propagate(it0, di, n_steps, h,
+                                     psi_out=psi_dev.view(n_steps, 1, self.n_state))
+                self._traj.check_status()
+        finally:
+            if self.effective_noise_integration:
+                self._bind_noise(self._n1, self._n2)
         psi = psi_dev.cpu().numpy()
         need_phi = "phi_traj" in self.storage.data or "z_mem" in self.storage.data
         phi_end = zmem_end = None
@@ -311,6 +328,10 @@ class HopsTrajectory:
     @property
     def t(self):
         return self._t
+
+    @property
+    def effective_noise_integration(self):
+        return self.integration_param["EFFECTIVE_NOISE_INTEGRATION"]
 
     @property
     def n_hier(self):

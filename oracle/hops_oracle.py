@@ -301,12 +301,27 @@ def noise_lookup(noise, t_list, tau_noise):
     return out
 
 
+def effective_noise(noise, t, tau, tau_noise, real=False):
+    """EFFECTIVE_NOISE_INTEGRATION samples [n_L, 3]: means of the complex64
+    samples in [t, t + tau/2), [t + tau/2, t + tau), [t + tau, t + 3 tau/2)
+    taken with np.mean as integrator/integrator_rk.py:115-128 does (real: the
+    float32 real parts, FLAG_REAL noise)."""
+    r = round(tau / tau_noise)
+    raw = noise_lookup(noise, [t + (i / r) * tau for i in range(round(r * 1.5))], tau_noise)
+    if real:
+        raw = np.real(raw)
+    return np.array([np.mean(raw[:, :round(r / 2)], axis=1),
+                     np.mean(raw[:, round(r / 2):r], axis=1),
+                     np.mean(raw[:, r:], axis=1)]).T
+
+
 def propagate(basis, psi0, noise1, tau_noise, t_max, dt, noise2=None,
-              eom="NORMALIZED NONLINEAR"):
+              eom="NORMALIZED NONLINEAR", effective=False):
     """Run the non-adaptive trajectory loop; returns (t_axis, psi_traj, phi, zmem).
 
     trajectory/hops_trajectory.py:253-336 (phi_0 = [psi_0, 0 ...], z_mem = 0)
-    and :401-538 (runge_kutta_variables -> runge_kutta_step -> normalize).
+    and :401-538 (runge_kutta_variables -> runge_kutta_step -> normalize);
+    effective: EFFECTIVE_NOISE_INTEGRATION window means instead of the samples.
     """
     S, N = basis.nstate, basis.nhier
     phi = np.zeros(N * S, dtype=np.complex128)
@@ -319,9 +334,13 @@ def propagate(basis, psi0, noise1, tau_noise, t_max, dt, noise2=None,
     t_axis = [0.0]
     t = 0.0
     for n in range(n_steps):
-        tl = [t, t + dt * 0.5, t + dt]
-        zr = noise_lookup(noise1, tl, tau_noise)
-        zr2 = noise_lookup(noise2, tl, tau_noise)
+        if effective:
+            zr = effective_noise(noise1, t, dt, tau_noise)
+            zr2 = effective_noise(noise2, t, dt, tau_noise)
+        else:
+            tl = [t, t + dt * 0.5, t + dt]
+            zr = noise_lookup(noise1, tl, tau_noise)
+            zr2 = noise_lookup(noise2, tl, tau_noise)
         phi, zmem = rk4_step(basis, phi, zmem, zr, zr2, dt, eom)
         if eom == "NORMALIZED NONLINEAR":
             phi = normalize(phi, S)

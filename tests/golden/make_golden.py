@@ -4,7 +4,9 @@ Run in a container that has the reference source tree (its ``src`` directory on
 ``MESOHOPS_SRC`` or at the default path below).  The outputs are small ``.npz``
 files committed next to this script; the GPU box never needs the reference.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py               # plain fixtures
+    python tests/golden/make_golden.py --adaptive    # adaptive-basis fixtures
+    python tests/golden/make_golden.py --effective   # EFFECTIVE_NOISE_INTEGRATION
 
 Each fixture records the inputs (system, hierarchy depth, noise arrays, psi_0,
 time step) together with the reference outputs (psi_traj, derivative values,
@@ -67,9 +69,12 @@ def n_unique(sysp):
 
 
 def run_precalc(name, sysp, depth, psi0, t_max, dt, noise_seed, noise2=None,
-                eom="NORMALIZED NONLINEAR", extra=None):
-    """Propagate with PRE_CALCULATED noise; record psi_traj, phi, z_mem and derivatives."""
-    tau_noise = dt / 2.0
+                eom="NORMALIZED NONLINEAR", extra=None, tau_noise=None, integration=None):
+    """Propagate with PRE_CALCULATED noise; record psi_traj, phi, z_mem and derivatives.
+
+    tau_noise: noise time step (default dt / 2); integration: integration_param
+    of the reference trajectory (default: the reference's defaults)."""
+    tau_noise = dt / 2.0 if tau_noise is None else tau_noise
     tlen = t_max + dt
     n_t = int(np.ceil(tlen / tau_noise)) + 1
     nl = n_unique(sysp)
@@ -95,9 +100,10 @@ def run_precalc(name, sysp, depth, psi0, t_max, dt, noise_seed, noise2=None,
         sysp["L_NOISE2"] = sysp["L_HIER"]
         sysp["ALPHA_NOISE2"] = bcf_exp
         sysp["PARAM_NOISE2"] = sysp["GW_SYSBATH"]
+    kw = {} if integration is None else {"integration_param": integration}
     hops = HopsTrajectory(sysp, noise_param=noise_param, noise2_param=noise2_param,
                           hierarchy_param={"MAXHIER": depth},
-                          eom_param={"EQUATION_OF_MOTION": eom}, storage_param={})
+                          eom_param={"EQUATION_OF_MOTION": eom}, storage_param={}, **kw)
     quiet(hops.initialize, psi0)
     # one derivative at a random state with non-zero memory and noise
     nh, ns = hops.n_hier, hops.n_state
@@ -238,7 +244,34 @@ def main():
     make_noise_fixture()
 
 
-if __name__ == "__main__" and "--adaptive" not in sys.argv:
+def main_effective():
+    """EFFECTIVE_NOISE_INTEGRATION: noise on a finer axis than dt / 2, averaged over
+    windows of k = dt / (2 TAU) samples (k = 4, 5, 9: the short, 8-partial-sum and
+    tail branches of numpy's pairwise sum)."""
+    eff = {"INTEGRATOR": "RUNGE_KUTTA", "EFFECTIVE_NOISE_INTEGRATION": True}
+    H = np.array([[0, 50], [50, 0.0]])
+    run_precalc("eff_dimer_k4", site_system(H, [(50, 50, 295)]), 3,
+                np.array([1, 0], dtype=np.complex128), 100.0, 4.0, noise_seed=21,
+                tau_noise=0.5, integration=eff)
+    n = 6
+    rng = np.random.default_rng(2)
+    Hr = np.diag(rng.uniform(-100, 100, n))
+    for i in range(n):
+        Hr[i, (i + 1) % n] = Hr[(i + 1) % n, i] = 80.0
+    psi0 = np.zeros(n, dtype=np.complex128)
+    psi0[0] = 1.0
+    n_t = int(np.ceil(64.0 / 0.4)) + 1
+    n2 = (np.random.default_rng(98).normal(size=(n, n_t)) * 3.0).astype(np.complex64)
+    run_precalc("eff_ring6_k5", site_system(Hr, [(60, 60, 295)]), 2, psi0, 60.0, 4.0,
+                noise_seed=22, noise2=n2, tau_noise=0.4, integration=eff)
+    run_precalc("eff_dimer_k9", site_system(H, [(50, 50, 295)]), 2,
+                np.array([0, 1], dtype=np.complex128), 40.0, 4.0, noise_seed=23,
+                tau_noise=2.0 / 9.0, integration=eff)
+
+
+if __name__ == "__main__" and "--effective" in sys.argv:
+    main_effective()
+elif __name__ == "__main__" and "--adaptive" not in sys.argv:
     main()
 
 
