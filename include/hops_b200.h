@@ -110,6 +110,12 @@ typedef struct hops_structure {
   /* site-projector form: diagonal of -i H, kept out of the H CSR above and
      added to the per-state diagonal coefficient; NULL otherwise */
   const double* h_diag;        /* [n_state] complex */
+  /* low-temperature correction (eom/eom_functions.py:215-309 as applied by
+     eom/hops_eom.py:357-403,527-529); NULL when every coefficient is zero */
+  const double* lt_coef;  /* [n_lop] complex c_j (summed PARAM_LT_CORR of L_j) */
+  const int32_t* l2_ptr;  /* [n_lop * (n_state+1)] CSR of L_j^2 */
+  const int32_t* l2_col;
+  const double* l2_val;   /* complex */
 } hops_structure;
 
 /*

@@ -40,6 +40,7 @@ class HopsStructure(C.Structure):
         ("mode_site", _p), ("mode_gwv", _p), ("mode_gwv_f", _p),
         ("dn_coef_site", _p), ("dn_coef_site_f", _p),
         ("up_site", _p), ("dn_site", _p), ("h_diag", _p),
+        ("lt_coef", _p), ("l2_ptr", _p), ("l2_col", _p), ("l2_val", _p),
     ]
 
 

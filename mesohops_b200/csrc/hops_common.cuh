@@ -72,7 +72,7 @@ struct ScalarLayout {
   int S, M, L;
   int stride;  // doubles per trajectory
   __host__ __device__ ScalarLayout(int s, int m, int l) : S(s), M(m), L(l) {
-    int n = 4 + 4 * L + 7 * M + 3 * S;
+    int n = 4 + 6 * L + 7 * M + 6 * S;
     stride = (n + 1) & ~1;
   }
   __host__ __device__ int scale() const { return 0; }
@@ -84,8 +84,15 @@ struct ScalarLayout {
   __host__ __device__ int zacc() const { return 4 + 4 * L + 2 * M; }
   __host__ __device__ int upc() const { return 4 + 4 * L + 4 * M; }
   __host__ __device__ int diagD() const { return 4 + 4 * L + 6 * M; }
-  __host__ __device__ int upc_f() const { return 4 + 4 * L + 6 * M + 2 * S; }   // M float2
-  __host__ __device__ int diagD_f() const { return 4 + 4 * L + 7 * M + 2 * S; } // S float2
+  // low-temperature correction: additive term of the physical wavefunction
+  // (aux 0) per state, and <L_j^2>
+  __host__ __device__ int phys() const { return 4 + 4 * L + 6 * M + 2 * S; }
+  __host__ __device__ int avgL2() const { return 4 + 4 * L + 6 * M + 4 * S; }
+  // float2 copies last: every complex-double field above starts at an even
+  // offset (16-byte aligned), whatever the parity of M and S
+  __host__ __device__ int upc_f() const { return 4 + 6 * L + 6 * M + 4 * S; }   // M float2
+  __host__ __device__ int diagD_f() const { return 4 + 6 * L + 7 * M + 4 * S; } // S float2
+  __host__ __device__ int phys_f() const { return 4 + 6 * L + 7 * M + 5 * S; }  // S float2
 };
 
 // Stage constants of classic RK4 (integrator_rk.py:29-30).
@@ -170,6 +177,20 @@ __device__ void stage_scalars(const hops_structure& st, const StageIO& io, Get g
       num = mk(num.x / n2, num.y / n2);
     }
     avgL[j] = num;
+    double2 ltc = mk(0.0, 0.0);  // conj(c_j) <L_j>: LT term of every aux (calc_LT_corr)
+    if (st.lt_coef && !linear && act) {
+      const int base = j * (S + 1);
+      double2 num2 = mk(0.0, 0.0);
+      for (int r = 0; r < S; ++r) {
+        const int q0 = st.l2_ptr[base + r], q1 = st.l2_ptr[base + r + 1];
+        if (q0 == q1) continue;
+        double2 row = mk(0.0, 0.0);
+        for (int q = q0; q < q1; ++q) row = cfma(ld2(st.l2_val, q), get(0, st.l2_col[q]), row);
+        num2 = cadd(num2, cconjmul(get(0, r), row));
+      }
+      reinterpret_cast<double2*>(ws + lay.avgL2())[j] = mk(num2.x / n2, num2.y / n2);
+      ltc = cmul(cconj(ld2(st.lt_coef, j)), num);
+    }
     // compress_zmem: sum of z_mem over the modes of L_j, then + conj(z1).
     float2 z1 = io.noise1 ? io.noise1[(size_t)j * io.n_t1 + io.it] : mkf(0.f, 0.f);
     double2 zs = mk(0.0, 0.0);
@@ -182,6 +203,7 @@ __device__ void stage_scalars(const hops_structure& st, const StageIO& io, Get g
     zhat[j] = zh;
     float2 z2 = io.noise2 ? io.noise2[(size_t)j * io.n_t2 + io.it] : mkf(0.f, 0.f);
     double2 cz = (linear || act) ? mk(zh.x + (double)z2.y, zh.y - (double)z2.x) : mk(0.0, 0.0);
+    cz = cadd(cz, ltc);
     // The LINEAR closure forms conj(z1) - 1j*z2 from complex64 samples without
     // any complex128 term, so the reference rounds it to complex64
     // (hops_eom.py:520,535); the float sum of two floats taken in double and
@@ -201,6 +223,16 @@ __device__ void stage_scalars(const hops_structure& st, const StageIO& io, Get g
       for (int j = 0; j < L; ++j)
         if (st.lop_active[j]) d = cfma(zhat[j], avgL[j], d);
       part_re = d.x;
+      if (st.lt_coef) {
+        // calc_LT_corr_to_norm_corr (eom_functions.py:254-281): real part of
+        // sum_j Re(c_j) (2 <L_j>^2 - <L_j^2>)
+        const double2* a2 = reinterpret_cast<const double2*>(ws + lay.avgL2());
+        for (int j = 0; j < L; ++j) {
+          if (!st.lop_active[j]) continue;
+          const double2 l = avgL[j];
+          part_re += ld2(st.lt_coef, j).x * (2.0 * (l.x * l.x - l.y * l.y) - a2[j].x);
+        }
+      }
     }
     for (int f = threadIdx.x; f < st.n_first; f += blockDim.x) {
       const int m = st.first_mode[f], j = st.mode_lop[m];
@@ -269,6 +301,29 @@ __device__ void stage_scalars(const hops_structure& st, const StageIO& io, Get g
     }
     reinterpret_cast<double2*>(ws + lay.diagD())[s] = d;
     reinterpret_cast<float2*>(ws + lay.diagD_f())[s] = mkf((float)d.x, (float)d.y);
+    if (st.lt_coef) {
+      // LT term of the physical wavefunction: nonlinear
+      // sum_j (c_j <L_j> L_j - c_j L_j^2) psi_0 (calc_LT_corr), LINEAR
+      // -sum_j c_j L_j^2 psi_0 (calc_LT_corr_linear)
+      double2 ph = mk(0.0, 0.0);
+      for (int j = 0; j < L; ++j) {
+        if (!linear && !st.lop_active[j]) continue;
+        const double2 c = ld2(st.lt_coef, j);
+        const int base = j * (S + 1);
+        if (!linear) {
+          double2 lp = mk(0.0, 0.0);
+          for (int q = st.l_ptr[base + s]; q < st.l_ptr[base + s + 1]; ++q)
+            lp = cfma(ld2(st.l_val, q), get(0, st.l_col[q]), lp);
+          ph = cfma(cmul(c, avgL[j]), lp, ph);
+        }
+        double2 l2p = mk(0.0, 0.0);
+        for (int q = st.l2_ptr[base + s]; q < st.l2_ptr[base + s + 1]; ++q)
+          l2p = cfma(ld2(st.l2_val, q), get(0, st.l2_col[q]), l2p);
+        ph = csub(ph, cmul(c, l2p));
+      }
+      reinterpret_cast<double2*>(ws + lay.phys())[s] = ph;
+      reinterpret_cast<float2*>(ws + lay.phys_f())[s] = mkf((float)ph.x, (float)ph.y);
+    }
   }
   if (threadIdx.x == 0) {
     ws[lay.nc()] = nc;

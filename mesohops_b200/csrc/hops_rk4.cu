@@ -85,7 +85,7 @@ template <> struct Prec<float> {
 // stage coefficients in trajectory-fastest layout ([m][b], [s][b], [j][b]) so
 // that the stage kernel reads them coalesced.
 struct BatchLayout {
-  size_t upcT, upcT_f, diagT, diagT_f, czT, czT_f, ncB, scaleB, total;  // in doubles
+  size_t upcT, upcT_f, diagT, diagT_f, czT, czT_f, ncB, scaleB, physT, physT_f, total;  // doubles
   __host__ __device__ static size_t even(size_t x) { return (x + 1) & ~(size_t)1; }
   __host__ __device__ BatchLayout(int S, int M, int L, int B) {
     const ScalarLayout lay(S, M, L);
@@ -97,7 +97,9 @@ struct BatchLayout {
     czT_f = czT + 2 * (size_t)L * B;
     ncB = even(czT_f + (size_t)L * B);
     scaleB = ncB + B;
-    total = even(scaleB + B);
+    physT = even(scaleB + B);            // LT term of aux 0, [s][b] complex
+    physT_f = physT + 2 * (size_t)S * B;
+    total = even(physT_f + (size_t)S * B);
   }
 };
 
@@ -124,6 +126,10 @@ template <typename R> struct CoefT {
     else return ld2f(reinterpret_cast<const float*>(ws + bl.czT_f), j * B + b);
   }
   __device__ __forceinline__ R nc() const { return (R)ws[bl.ncB + b]; }
+  __device__ __forceinline__ T phys(int s) const {
+    if constexpr (sizeof(R) == 8) return ld2(ws + bl.physT, s * B + b);
+    else return ld2f(reinterpret_cast<const float*>(ws + bl.physT_f), s * B + b);
+  }
 };
 
 // Stage coefficients of one trajectory read from its ScalarLayout block
@@ -146,6 +152,10 @@ template <typename R> struct CoefWS {
     else return mkf((float)v.x, (float)v.y);
   }
   __device__ __forceinline__ R nc() const { return (R)ws[lay.nc()]; }
+  __device__ __forceinline__ T phys(int s) const {
+    if constexpr (sizeof(R) == 8) return ld2(ws + lay.phys(), s);
+    else return ld2f(reinterpret_cast<const float*>(ws + lay.phys_f()), s);
+  }
 };
 
 // ------------------------------------------------- derivative of one element --
@@ -559,6 +569,10 @@ __global__ void __launch_bounds__(wide_threads(NB), NB <= 2 ? 4 : (NB == 4 ? 4 :
       const size_t e = rowa + bg + lane + 32 * j;
       T kk = k[j];
       if (stage == 0 || stage == 4) kk = cscale(kk, (R)sc[j]);
+      if (st.lt_coef && a == 0) {  // LT term of psi_0 (computed from the scaled state)
+        if constexpr (sizeof(R) == 8) kk = cadd(kk, ld2(ws + bl.physT, s * B + bg + lane + 32 * j));
+        else kk = cadd(kk, ld2f(reinterpret_cast<const float*>(ws + bl.physT_f), s * B + bg + lane + 32 * j));
+      }
       const PT p = stage == 4 ? PT{} : cscale(ph[j], (decltype(PT{}.x))sc[j]);
       rk_finish<true, T, ST, PT>(stage, h, kk, p, accv[j], acc, yout, phi, shadow, e);
     }
@@ -595,6 +609,7 @@ __global__ void __launch_bounds__(256) k_narrow(hops_structure st, int B, int st
       const size_t e = (size_t)a * SB + r;
       const double sc = scaleB[b];
       if (stage == 0 || stage == 4) k = cscale(k, (R)sc);
+      if (st.lt_coef && a == 0) k = cadd(k, cf.phys(s));  // LT term of psi_0 (already scaled)
       const PT ph = stage == 4 ? PT{} : cscale(phi[e], (decltype(PT{}.x))sc);
       rk_update<true, T, ST, PT>(stage, h, k, ph, acc, yout, phi, shadow, e);
     }
@@ -628,6 +643,12 @@ __device__ void publish(const hops_structure& st, const BatchLayout& bl, double*
     reinterpret_cast<double2*>(wsall + bl.czT)[(size_t)j * B + b] = v;
     reinterpret_cast<float2*>(wsall + bl.czT_f)[(size_t)j * B + b] = mkf((float)v.x, (float)v.y);
   }
+  if (st.lt_coef)
+    for (int s = threadIdx.x; s < S; s += blockDim.x) {
+      double2 v = ld2(ws + lay.phys(), s);
+      reinterpret_cast<double2*>(wsall + bl.physT)[(size_t)s * B + b] = v;
+      reinterpret_cast<float2*>(wsall + bl.physT_f)[(size_t)s * B + b] = mkf((float)v.x, (float)v.y);
+    }
   if (threadIdx.x == 0) {
     wsall[bl.ncB + b] = ws[lay.nc()];
     wsall[bl.scaleB + b] = ws[lay.scale()];
@@ -847,7 +868,8 @@ __global__ void __launch_bounds__(512, 1) k_resident(hops_task* tasks, int mode,
         auto y = [&](int x, int sp) { return cv<T>(phi[x * S + sp]); };
         for (int e = threadIdx.x; e < E; e += blockDim.x) {
           const int a = e / S, s = e - a * S;
-          const T k = deriv_elem<R, SITE>(st, a, s, y, cf);
+          T k = deriv_elem<R, SITE>(st, a, s, y, cf);
+          if (st.lt_coef && a == 0) k = cadd(k, cf.phys(s));  // LT term of psi_0
           rk_update<false, T, ST, PT>(stage, io.h, k, phi[e], acc, yout, phi, (ST*)nullptr, (size_t)e);
         }
       } else {
@@ -856,7 +878,8 @@ __global__ void __launch_bounds__(512, 1) k_resident(hops_task* tasks, int mode,
         auto y = [&](int x, int sp) { return cv<T>(yin[x * S + sp]); };
         for (int e = threadIdx.x; e < E; e += blockDim.x) {
           const int a = e / S, s = e - a * S;
-          const T k = deriv_elem<R, SITE>(st, a, s, y, cf);
+          T k = deriv_elem<R, SITE>(st, a, s, y, cf);
+          if (st.lt_coef && a == 0) k = cadd(k, cf.phys(s));  // LT term of psi_0
           rk_update<false, T, ST, PT>(stage, io.h, k, phi[e], acc, yout, phi, (ST*)nullptr, (size_t)e);
         }
       }

@@ -151,6 +151,13 @@ def _state_mode_tables(system, states, modes):
         h_ptr, h_col, h_val = _csr_of_dense([-1j * H], S)
     G = system.G[modes]
     W = system.W[modes]
+    # low-temperature corrections of the relative L list, with the CSR of L_j^2
+    # (hops_eom.py:357-403 uses list_L2_sq_csr); none when every c_j is zero
+    lt = np.asarray(getattr(system, "lt_coef", np.zeros(system.n_lop)))[l_abs] if L else None
+    if lt is not None and np.any(lt != 0):
+        l2_ptr, l2_col, l2_val = _csr_of_dense([l @ l for l in lops], S)
+    else:
+        lt, l2_ptr, l2_col, l2_val = None, None, None, None
     # site-projector coefficients per mode
     mode_site = site[mode_lop] if M else np.zeros(0, dtype=np.int32)
     mode_gwv = (G / W) * sval[mode_lop] if M else np.zeros(0, dtype=complex)
@@ -161,6 +168,7 @@ def _state_mode_tables(system, states, modes):
         lop_active=lop_active, lop_site=site, lop_sval=sval,
         h_ptr=h_ptr, h_col=h_col, h_val=h_val, site_projector=int(is_site),
         mode_site=mode_site.astype(np.int32), mode_gwv=mode_gwv, h_diag=h_diag,
+        lt_coef=lt, l2_ptr=l2_ptr, l2_col=l2_col, l2_val=l2_val,
     )
 
 
@@ -269,6 +277,9 @@ class DeviceStructure:
         ]
         if t["h_diag"] is not None:
             fields.append(("h_diag", c2d(t["h_diag"])))
+        if t.get("lt_coef") is not None:
+            fields += [("lt_coef", c2d(t["lt_coef"])), ("l2_ptr", t["l2_ptr"].astype(i32)),
+                       ("l2_col", t["l2_col"].astype(i32)), ("l2_val", c2d(t["l2_val"]))]
         offs = {}
         off = 0
         for name, arr in fields:

@@ -90,10 +90,23 @@ class HopsSystem:
             self.l_by_nmode2, self.nmodes2_by_l = self._noise_map(p["L_NOISE2"], p["PARAM_NOISE2"])
             self.alpha2 = p.get("ALPHA_NOISE2")
             self.param_noise2 = list(p.get("PARAM_NOISE2", []))
-        lt = p.get("PARAM_LT_CORR", [])
-        if len(lt) and np.any(np.asarray(lt) != 0):
-            raise UnsupportedRequest("low-temperature correction (PARAM_LT_CORR)",
-                                     "mesohops_b200 HopsSystem")
+        # low-temperature corrections: summed per unique L; an operator of no
+        # bath is dropped with the reference's warning (system_functions.py:50-56,115-133)
+        lt_ops = list(p.get("L_LT_CORR", []))
+        lt_par = list(p.get("PARAM_LT_CORR", []))
+        if len(lt_ops) != len(lt_par):
+            raise UnsupportedRequest("L_LT_CORR and PARAM_LT_CORR of different lengths",
+                                     "HopsSystem", override=True)
+        self.lt_coef = np.zeros(self.n_lop, dtype=np.complex128)
+        for lop, c in zip(lt_ops, lt_par):
+            j = self._key_index.get(pattern_key(lop))
+            if j is None:
+                print("WARNING: the list of low-temperature correction L-operators contains "
+                      "an L-operator not associated with any existing thermal environment. "
+                      "This low-temperature correction factor will be discarded!")
+                continue
+            self.lt_coef[j] += complex(c)
+        self.has_lt = bool(np.any(self.lt_coef != 0))
         # state <-> mode maps (system_functions.py:33-39) and H couplings
         self.states_by_lop = [np.array(self.states_of_lop(j), dtype=np.int64)
                               for j in range(self.n_lop)]
@@ -112,6 +125,7 @@ class HopsSystem:
         self.param["LIST_INDEX_L2_BY_HMODE"] = list(self.l_by_mode)
         self.param["LIST_INDEX_L2_BY_NMODE1"] = list(self.l_by_nmode1)
         self.param["LIST_NMODE1_BY_INDEX_L2"] = [list(x) for x in self.nmodes1_by_l]
+        self.param["LIST_LT_PARAM"] = list(self.lt_coef)
 
     def _noise_map(self, lops, params):
         l_by_nmode = []

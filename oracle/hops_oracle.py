@@ -63,7 +63,10 @@ def expand_system(sys_param):
     """Subset of basis/system_functions.py:10-172 needed by the hot path.
 
     Returns dict with H (dense complex), G, W, the unique L list (dense, values of
-    the first mode with that nonzero pattern) and the mode -> unique-L map.
+    the first mode with that nonzero pattern), the mode -> unique-L map and LT,
+    the low-temperature correction coefficient of each unique L: the sum of the
+    PARAM_LT_CORR entries whose L_LT_CORR has that nonzero pattern; entries
+    matching no L_HIER operator are dropped (system_functions.py:115-133).
     """
     H = sys_param["HAMILTONIAN"]
     H = H.toarray() if sps.issparse(H) else np.asarray(H)
@@ -83,9 +86,14 @@ def expand_system(sys_param):
             lm = lm.toarray() if sps.issparse(lm) else np.asarray(lm)
             l_unique.append(np.array(lm, dtype=np.complex128))
         l_by_mode.append(uniq[k])
+    lt = np.zeros(len(l_unique), dtype=np.complex128)
+    for lop, c in zip(sys_param.get("L_LT_CORR", []), sys_param.get("PARAM_LT_CORR", [])):
+        j = uniq.get(_pattern_key(lop))
+        if j is not None:
+            lt[j] += c
     return {"H": H, "G": G, "W": W, "L": l_unique,
             "L_BY_MODE": np.array(l_by_mode, dtype=np.int64),
-            "NSTATE": H.shape[0], "NMODE": len(gw)}
+            "NSTATE": H.shape[0], "NMODE": len(gw), "LT": lt}
 
 
 # ---------------------------------------------------------------------------
@@ -219,11 +227,16 @@ def dsystem_dt(basis, phi, zmem, z1, z2, eom="NORMALIZED NONLINEAR"):
     z1 = np.asarray(z1)
     z2 = np.asarray(z2)
     pf = phi.reshape(N, S)  # row a = aux, column = state
+    lt = s.get("LT", np.zeros(len(L)))
+    has_lt = bool(np.any(lt))
     if eom == "LINEAR":
         dphi = basis.k2_stable @ phi
         d = dphi.reshape(N, S)
         d += basis.k2_k[:, None] * pf
         d += pf @ (-1j * s["H"]).T
+        if has_lt:
+            # calc_LT_corr_linear (eom_functions.py:284-309), physical wavefunction only
+            d[0] += -sum(lt[j] * (L[j] @ L[j]) for j in range(len(L))) @ pf[0]
         for j in range(len(L)):
             rows, cols, lsub = basis.l_mask[j]
             d[:, rows] += (np.conj(z1[j]) - 1j * z2[j]) * (pf[:, cols] @ lsub.T)
@@ -251,6 +264,17 @@ def dsystem_dt(basis, phi, zmem, z1, z2, eom="NORMALIZED NONLINEAR"):
     d = dphi.reshape(N, S)
     d += basis.k2_k[:, None] * pf
     d += pf @ (-1j * s["H"]).T
+    if has_lt:
+        # calc_LT_corr / calc_LT_corr_to_norm_corr (eom_functions.py:215-281),
+        # applied as hops_eom.py:357-403
+        l2 = [L[j] @ L[j] for j in range(len(L))]
+        avg2 = np.array([np.vdot(psi0, l2[j] @ psi0) / n2 for j in range(len(L))])
+        c_phys = sum(lt[j] * avg[j] * L[j] - lt[j] * l2[j] for j in act)
+        c_hier = sum(np.conj(lt[j]) * avg[j] * L[j] for j in act)
+        d += pf @ np.asarray(c_hier).T
+        d[0] += np.asarray(c_phys) @ pf[0]
+        if normalized:
+            nc = nc + np.sum(np.real(lt[act]) * (2 * avg[act] ** 2 - avg2[act]))
     if normalized:
         d -= nc * pf
     for j in act:

@@ -23,8 +23,12 @@ def golden_system(f):
     from mesohops_b200.bath import bcf_exp
     gw = [[g, w] for g, w in zip(f["G"], f["W"])]
     lops = [np.array(l) for l in f["L"]]
-    return {"HAMILTONIAN": np.array(f["H"]), "GW_SYSBATH": gw, "L_HIER": lops,
+    sysp = {"HAMILTONIAN": np.array(f["H"]), "GW_SYSBATH": gw, "L_HIER": lops,
             "L_NOISE1": lops, "ALPHA_NOISE1": bcf_exp, "PARAM_NOISE1": gw}
+    if "LT_L" in f:   # low-temperature corrections
+        sysp["L_LT_CORR"] = [np.array(l) for l in f["LT_L"]]
+        sysp["PARAM_LT_CORR"] = [complex(c) for c in f["LT_P"]]
+    return sysp
 
 
 @pytest.fixture(scope="session")

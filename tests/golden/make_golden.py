@@ -7,6 +7,7 @@ files committed next to this script; the GPU box never needs the reference.
     python tests/golden/make_golden.py               # plain fixtures
     python tests/golden/make_golden.py --adaptive    # adaptive-basis fixtures
     python tests/golden/make_golden.py --effective   # EFFECTIVE_NOISE_INTEGRATION
+    python tests/golden/make_golden.py --ltc         # low-temperature corrections
 
 Each fixture records the inputs (system, hierarchy depth, noise arrays, psi_0,
 time step) together with the reference outputs (psi_traj, derivative values,
@@ -269,7 +270,72 @@ def main_effective():
                 tau_noise=2.0 / 9.0, integration=eff)
 
 
-if __name__ == "__main__" and "--effective" in sys.argv:
+def with_ltc(sysp, lt_ops, lt_params):
+    """System dictionary with low-temperature corrections (L_LT_CORR, PARAM_LT_CORR)."""
+    out = dict(sysp)
+    out["L_LT_CORR"] = list(lt_ops)
+    out["PARAM_LT_CORR"] = list(lt_params)
+    dense = np.array([np.array(l.toarray() if sps.issparse(l) else l, dtype=np.complex128)
+                      for l in lt_ops])
+    return out, {"LT_L": dense, "LT_P": np.array(lt_params, dtype=np.complex128)}
+
+
+def main_ltc():
+    """Low-temperature correction (eom_functions.py:215-309, hops_eom.py:357-403,
+    527-529) on site projectors and on general L, for the three equations of
+    motion; one correction names an L-operator of no bath and is dropped."""
+    H = np.array([[0, 50], [50, 0.0]])
+    base = site_system(H, [(50, 50, 295)])
+    l0 = sps.coo_matrix(([1.0], ([0], [0])), shape=(2, 2))
+    l1 = sps.coo_matrix(([1.0], ([1], [1])), shape=(2, 2))
+    for eom, tag, seed in [("NORMALIZED NONLINEAR", "norm", 41), ("NONLINEAR", "nonlinear", 42),
+                           ("LINEAR", "linear", 43)]:
+        sysp, extra = with_ltc(base, [l0, l1], [0.25 - 0.1j, 0.125 + 0.05j])
+        run_precalc("ltc_dimer_" + tag, sysp, 3, np.array([1, 0], dtype=np.complex128),
+                    100.0, 4.0, noise_seed=seed, eom=eom, extra=extra)
+    # ring of 6 sites, corrections on three sites plus one operator of no bath
+    n = 6
+    rng = np.random.default_rng(2)
+    Hr = np.diag(rng.uniform(-100, 100, n))
+    for i in range(n):
+        Hr[i, (i + 1) % n] = Hr[(i + 1) % n, i] = 80.0
+    psi0 = np.zeros(n, dtype=np.complex128)
+    psi0[0] = 1.0
+    ops, pars = [], []
+    for i, c in [(0, 0.2), (2, 0.1 - 0.05j), (4, 0.3j)]:
+        ops.append(sps.coo_matrix(([1.0], ([i], [i])), shape=(n, n)))
+        pars.append(c)
+    stray = np.zeros((n, n))
+    stray[0, 1] = stray[1, 0] = 1.0
+    ops.append(stray)
+    pars.append(0.5)
+    sysp, extra = with_ltc(site_system(Hr, [(60, 60, 295)]), ops, pars)
+    run_precalc("ltc_ring6", sysp, 2, psi0, 60.0, 4.0, noise_seed=44, extra=extra)
+    # general (off-diagonal, imaginary) L-operators with noise 2
+    lg = np.zeros((3, 3, 3), dtype=np.complex128)
+    lg[0, 0, 1] = 1j
+    lg[0, 1, 0] = -1j
+    lg[1, 1, 2] = 1
+    lg[1, 2, 1] = 1
+    lg[2, 0, 0] = 0.5
+    lg[2, 1, 1] = 1
+    lg[2, 2, 2] = -1
+    by_mode = [0, 0, 1, 1, 2, 2]
+    gw6 = [[12.0, 18.0], [7.0, 3.0], [11.0, 9.0], [6.0, 4.0], [10.0, 10.0], [5.0, 5.0]]
+    base_ham = np.array([[1.0, 14.0, 8.0], [14.0, 0, 10.0], [8.0, 10.0, -1.0]])
+    sysg = {"HAMILTONIAN": base_ham, "GW_SYSBATH": gw6,
+            "L_HIER": [lg[i] for i in by_mode], "L_NOISE1": [lg[i] for i in by_mode],
+            "ALPHA_NOISE1": bcf_exp, "PARAM_NOISE1": gw6}
+    sysg, extra = with_ltc(sysg, [lg[0], lg[2]], [0.4 + 0.1j, 0.15])
+    rngn2 = np.random.default_rng(97)
+    n2 = (rngn2.normal(size=(3, int(np.ceil(21.0 / 0.5)) + 1)) * 3.0).astype(np.complex64)
+    run_precalc("ltc_general", sysg, 3, np.array([1, 0, 0], dtype=np.complex128),
+                20.0, 1.0, noise_seed=45, noise2=n2, extra=extra)
+
+
+if __name__ == "__main__" and "--ltc" in sys.argv:
+    main_ltc()
+elif __name__ == "__main__" and "--effective" in sys.argv:
     main_effective()
 elif __name__ == "__main__" and "--adaptive" not in sys.argv:
     main()
