@@ -1348,8 +1348,9 @@ __global__ void __launch_bounds__(256) k_flux_errors(hops_flux_task* tasks, doub
     const int a = e / S, s = e - a * S;
     double val = 0.0;
     if (!mask || mask[a]) {
-      const double2 k = st.site_projector ? deriv_elem<double, true>(st, a, s, y, cf)
-                                          : deriv_elem<double, false>(st, a, s, y, cf);
+      double2 k = st.site_projector ? deriv_elem<double, true>(st, a, s, y, cf)
+                                    : deriv_elem<double, false>(st, a, s, y, cf);
+      if (st.lt_coef && a == 0) k = cadd(k, cf.phys(s));  // LT term of psi_0
       const double2 ph = phi[e];
       const double re = k.x * inv_h + ph.x * inv_dt, im = k.y * inv_h + ph.y * inv_dt;
       val = re * re + im * im;

@@ -103,9 +103,6 @@ class HopsTrajectory:
             if self.effective_noise_integration:
                 raise UnsupportedRequest("EFFECTIVE_NOISE_INTEGRATION with an adaptive basis",
                                          "mesohops_b200 HopsTrajectory")
-            if self.system.has_lt:
-                raise UnsupportedRequest("low-temperature correction with an adaptive basis",
-                                         "mesohops_b200 HopsTrajectory")
             self._initialize_adaptive(psi_0, dev)
             self.storage.metadata["INITIALIZATION_TIME"] = timer.time() - t0
             self.__initialized__ = True

@@ -397,7 +397,8 @@ class OracleSubBasis(OracleBasis):
                     "L": [full["L"][j][ix] for j in self.l_abs],
                     "L_BY_MODE": np.array([rel[int(full["L_BY_MODE"][m])] for m in modes],
                                           dtype=np.int64),
-                    "NSTATE": len(states), "NMODE": len(modes)}
+                    "NSTATE": len(states), "NMODE": len(modes),
+                    "LT": np.asarray(full.get("LT", np.zeros(len(full["L"]))))[self.l_abs]}
         self.states, self.modes = states, modes
         self.nstate, self.nmode = len(states), len(modes)
         self.aux = np.asarray(aux, dtype=np.int64)[:, modes].reshape(-1, len(modes))

@@ -8,6 +8,7 @@ files committed next to this script; the GPU box never needs the reference.
     python tests/golden/make_golden.py --adaptive    # adaptive-basis fixtures
     python tests/golden/make_golden.py --effective   # EFFECTIVE_NOISE_INTEGRATION
     python tests/golden/make_golden.py --ltc         # low-temperature corrections
+    python tests/golden/make_golden.py --ltc-adaptive  # the same with an adaptive basis
 
 Each fixture records the inputs (system, hierarchy depth, noise arrays, psi_0,
 time step) together with the reference outputs (psi_traj, derivative values,
@@ -333,16 +334,24 @@ def main_ltc():
                 20.0, 1.0, noise_seed=45, noise2=n2, extra=extra)
 
 
-if __name__ == "__main__" and "--ltc" in sys.argv:
-    main_ltc()
-elif __name__ == "__main__" and "--effective" in sys.argv:
-    main_effective()
-elif __name__ == "__main__" and "--adaptive" not in sys.argv:
-    main()
+def main_ltc_adaptive():
+    """Adaptive basis with low-temperature corrections on every site of a chain."""
+    n = 8
+    rng = np.random.default_rng(3)
+    H = np.diag(rng.normal(0, 100, n))
+    for i in range(n - 1):
+        H[i, i + 1] = H[i + 1, i] = 50.0
+    psi0 = np.zeros(n, dtype=np.complex128)
+    psi0[n // 2] = 1.0
+    ops = [sps.coo_matrix(([1.0], ([i], [i])), shape=(n, n)) for i in range(n)]
+    pars = [0.2 - 0.05j * (i % 3) for i in range(n)]
+    sysp, extra = with_ltc(site_system(H, [(50, 50, 295)]), ops, pars)
+    run_adaptive("adaptive_chain8_ltc", sysp, 3, psi0, 120.0, 4.0, 3e-4, 3e-4, noise_seed=34,
+                 extra=extra)
 
 
 def run_adaptive(name, sysp, depth, psi0, t_max, dt, delta_a, delta_s, noise_seed,
-                 update_step=1, f_discard=0.0):
+                 update_step=1, f_discard=0.0, extra=None):
     """Adaptive propagation with PRE_CALCULATED noise; records the basis per step."""
     tau_noise = dt / 2.0
     tlen = t_max + dt
@@ -393,7 +402,8 @@ def run_adaptive(name, sysp, depth, psi0, t_max, dt, delta_a, delta_s, noise_see
         list_nhier=np.array(d["list_nhier"]), list_nstate=np.array(d["list_nstate"]),
         aux_counts=np.array(aux_counts, dtype=np.int16).reshape(-1, n_mode),
         aux_ptr=np.array(aux_ptr), states=np.array(states), state_ptr=np.array(state_ptr),
-        phi_end=np.array(hops.phi), n_hier_end=hops.n_hier, n_state_end=hops.n_state)
+        phi_end=np.array(hops.phi), n_hier_end=hops.n_hier, n_state_end=hops.n_state,
+        **(extra or {}))
     print(name, "adaptive steps", len(psi_full) - 1, "n_hier", list(d["list_nhier"])[:8],
           "n_state", list(d["list_nstate"])[:8])
 
@@ -432,5 +442,14 @@ def main_adaptive():
                      delta, delta, noise_seed=seed)
 
 
-if __name__ == "__main__" and "--adaptive" in sys.argv:
-    main_adaptive()
+if __name__ == "__main__":
+    if "--adaptive" in sys.argv:
+        main_adaptive()
+    elif "--effective" in sys.argv:
+        main_effective()
+    elif "--ltc" in sys.argv:
+        main_ltc()
+    elif "--ltc-adaptive" in sys.argv:
+        main_ltc_adaptive()
+    else:
+        main()

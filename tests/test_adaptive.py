@@ -24,7 +24,7 @@ from mesohops_b200.exceptions import UnsupportedRequest
 from oracle import hops_oracle as O
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-CASES = ["adaptive_dod_full", "adaptive_chain8", "adaptive_chain12"]
+CASES = ["adaptive_dod_full", "adaptive_chain8", "adaptive_chain12", "adaptive_chain8_ltc"]
 
 
 def load(name):
@@ -34,8 +34,12 @@ def load(name):
 def system_param(f):
     gw = [(complex(g), complex(w)) for g, w in zip(f["G"], f["W"])]
     lops = [np.array(l) for l in f["L"]]
-    return {"HAMILTONIAN": np.array(f["H"]), "GW_SYSBATH": gw, "L_HIER": lops,
+    sysp = {"HAMILTONIAN": np.array(f["H"]), "GW_SYSBATH": gw, "L_HIER": lops,
             "L_NOISE1": lops, "ALPHA_NOISE1": O.bcf_exp, "PARAM_NOISE1": gw}
+    if "LT_L" in f:   # low-temperature corrections
+        sysp["L_LT_CORR"] = [np.array(l) for l in f["LT_L"]]
+        sysp["PARAM_LT_CORR"] = [complex(c) for c in f["LT_P"]]
+    return sysp
 
 
 def make_traj(f, tmp_path, device):

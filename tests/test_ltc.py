@@ -61,18 +61,6 @@ def test_ltc_coefficients_by_unique_l():
     assert lt[1] == 0 and lt[3] == 0 and lt[5] == 0
 
 
-def test_ltc_rejected_with_adaptive_basis():
-    from mesohops_b200 import HopsTrajectory
-    from mesohops_b200.exceptions import UnsupportedRequest
-    f = load_golden("ltc_dimer_norm")
-    hops = HopsTrajectory(golden_system(f),
-                          noise_param={"MODEL": "ZERO", "TLEN": 100.0, "TAU": 2.0},
-                          hierarchy_param={"MAXHIER": 2}, device_param={"DEVICE": "cpu"})
-    hops.make_adaptive(1e-3, 1e-3)
-    with pytest.raises(UnsupportedRequest):
-        hops.initialize(f["psi0"])
-
-
 def make_traj(f, kernel, precision="complex128"):
     from mesohops_b200 import HopsTrajectory
     from mesohops_b200.bath import bcf_exp
