@@ -67,7 +67,7 @@ def gt_precision(z):
 class Basis:
     """One adaptive basis: states, aux list, mode list and the device structure."""
 
-    def __init__(self, system, keyer, maxhier, counts, states, device):
+    def __init__(self, system, keyer, maxhier, counts, states, device, noise_host=(None, None)):
         self.system = system
         self.states = np.array(sorted(int(s) for s in states), dtype=np.int64)
         counts = np.asarray(counts, dtype=np.int16).reshape(-1, system.n_mode)
@@ -78,7 +78,12 @@ class Basis:
         self.aux = AuxBasis(counts, keyer, maxhier, modes=self.modes)
         self.counts = self.aux.counts
         self.tables = build_tables(system, self.aux, self.states, self.modes)
-        self.dstruct = DeviceStructure(self.tables, device)
+        # the noise rows of the basis L list travel with the structure tables
+        extras = {}
+        for name, nh in zip(("noise1", "noise2"), noise_host):
+            if nh is not None and self.tables["n_lop"]:
+                extras[name] = np.ascontiguousarray(nh[self.tables["l_abs"]])
+        self.dstruct = DeviceStructure(self.tables, device, extras)
         self.n_hier = self.aux.n_hier
         self.n_state = len(self.states)
         self.n_mode = len(self.modes)
@@ -343,11 +348,13 @@ class AdaptiveHops:
         self.phi = None
         self.zmem_abs = None
         self.noise1_dev = self.noise2_dev = None
+        self.noise1_host = self.noise2_host = None
         self.t = 0.0
 
     # ------------------------------------------------------------ basis setup
     def _set_basis(self, states, counts):
-        self.basis = Basis(self.system, self.keyer, self.maxhier, counts, states, self.device)
+        self.basis = Basis(self.system, self.keyer, self.maxhier, counts, states, self.device,
+                           (self.noise1_host, self.noise2_host))
         b = self.basis
         n_elem = b.n_hier * b.n_state
         req = self.kernel_request
@@ -363,11 +370,8 @@ class AdaptiveHops:
         """Device buffers of the current basis (created on first use)."""
         if self._engine is None:
             b = self.basis
-            l_abs = torch.as_tensor(b.tables["l_abs"], device=self.device)
-            n1 = (self.noise1_dev.index_select(0, l_abs).contiguous()
-                  if self.noise1_dev is not None and b.tables["n_lop"] else None)
-            n2 = (self.noise2_dev.index_select(0, l_abs).contiguous()
-                  if self.noise2_dev is not None and b.tables["n_lop"] else None)
+            n1 = b.dstruct.extra.get("noise1")
+            n2 = b.dstruct.extra.get("noise2")
             if self.kernel == "resident":
                 self._engine = ResidentTrajectory(b.dstruct, self.precision, self.eom)
                 self._engine.set_noise(n1, n2)
@@ -386,6 +390,9 @@ class AdaptiveHops:
     def initialize_gen(self, psi0, noise1_dev, noise2_dev):
         """hops_trajectory.py:282-326 for an adaptive basis (coroutine)."""
         self.noise1_dev, self.noise2_dev = noise1_dev, noise2_dev
+        # host copies of the noise rows: each basis packs its rows with its tables
+        self.noise1_host = noise1_dev.cpu().numpy() if noise1_dev is not None else None
+        self.noise2_host = noise2_dev.cpu().numpy() if noise2_dev is not None else None
         sysm = self.system
         if self.adaptive_h:
             counts = np.zeros((1, sysm.n_mode), dtype=np.int16)

@@ -239,13 +239,16 @@ class DeviceStructure:
     """hops_structure with its arrays resident on one CUDA device.
 
     Every table and a device copy of the struct itself live in one packed
-    buffer uploaded with a single host->device copy (cheap enough to rebuild
-    at every adaptive basis change).
+    buffer uploaded with a single asynchronous host->device copy from pinned
+    memory (cheap enough to rebuild at every adaptive basis change, and no
+    wait for the work already queued on the stream).  `extras` (name -> numpy
+    array) are packed into the same buffer and exposed as device tensors in
+    `self.extra` (e.g. the noise rows of an adaptive basis).
     """
 
     _ALIGN = 256
 
-    def __init__(self, tables, device):
+    def __init__(self, tables, device, extras=None):
         self.tables = tables
         self.device = torch.device(device)
         t = tables
@@ -282,6 +285,10 @@ class DeviceStructure:
                        ("l2_col", t["l2_col"].astype(i32)), ("l2_val", c2d(t["l2_val"]))]
         offs = {}
         off = 0
+        extra_names = []
+        for name, arr in (extras or {}).items():
+            fields.append(("extra:" + name, np.ascontiguousarray(arr)))
+            extra_names.append(name)
         for name, arr in fields:
             if isinstance(arr, torch.Tensor):
                 a = arr.contiguous()
@@ -299,7 +306,9 @@ class DeviceStructure:
         total = off + C.sizeof(HopsStructure)
         self.buffer = torch.empty(total, dtype=torch.uint8, device=self.device)
         base = self.buffer.data_ptr()
-        host = np.zeros(total, dtype=np.uint8)
+        pinned = torch.empty(total, dtype=torch.uint8,
+                             pin_memory=self.device.type == "cuda")
+        host = pinned.numpy()
         s = HopsStructure()
         s.n_hier, s.n_state, s.n_mode, s.n_lop = t["n_hier"], t["n_state"], t["n_mode"], t["n_lop"]
         s.n_first = len(t["first_aux"])
@@ -308,14 +317,23 @@ class DeviceStructure:
         s.site_projector = t["site_projector"]
         s.max_up, s.max_dn = t["max_up"], t["max_dn"]
         dev_parts = []
+        self.extra = {}
         for name, (o, a, nbytes) in offs.items():
             if isinstance(a, torch.Tensor):
                 dev_parts.append((o, a, nbytes))
             else:
                 host[o:o + nbytes] = a.view(np.uint8).ravel()
-            setattr(s, name, base + o)
+            if name.startswith("extra:"):
+                arr = (extras or {})[name[6:]]
+                t = torch.from_numpy(np.zeros(0, dtype=arr.dtype)).dtype
+                self.extra[name[6:]] = (self.buffer[o:o + arr.nbytes].view(t)
+                                        .view(arr.shape) if arr.size else None)
+            else:
+                setattr(s, name, base + o)
         host[struct_off:] = np.frombuffer(bytes(s), dtype=np.uint8)
-        self.buffer.copy_(torch.from_numpy(host))
+        # the pinned staging buffer stays referenced until the copy has run
+        self.buffer.copy_(pinned, non_blocking=True)
+        self._staging = pinned
         for o, a, nbytes in dev_parts:
             self.buffer[o:o + nbytes].copy_(a.view(torch.uint8).reshape(-1))
         self.cstruct = s

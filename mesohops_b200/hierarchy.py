@@ -215,14 +215,12 @@ class AuxBasis:
 
     def first_level(self):
         """(aux index, relative mode) of every depth-1 aux along a basis mode."""
-        out = []
-        for rel, m in enumerate(self.modes):
-            e = np.zeros((1, self.counts.shape[1]), dtype=self.counts.dtype)
-            e[0, m] = 1
-            i = int(self.index_of(e)[0])
-            if i >= 0:
-                out.append((i, rel))
-        return out
+        if len(self.modes) == 0:
+            return []
+        e = np.zeros((len(self.modes), self.counts.shape[1]), dtype=self.counts.dtype)
+        e[np.arange(len(self.modes)), self.modes] = 1
+        idx = self.index_of(e)
+        return [(int(i), rel) for rel, i in enumerate(idx) if i >= 0]
 
 
 def triangular_basis(n_mode, maxhier, static_filters=()):
