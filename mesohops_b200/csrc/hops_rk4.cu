@@ -360,7 +360,7 @@ constexpr size_t wide_smem_bytes(int warps) {
 // steps at the register counts the wider tasks take).
 constexpr int wide_threads(int nb) { return nb <= 2 ? 256 : 128; }
 
-template <typename R, typename ST, typename PT, bool SITE, int NB>
+template <typename R, typename ST, typename PT, bool SITE, int NB, bool LT>
 __global__ void __launch_bounds__(wide_threads(NB), NB <= 2 ? 4 : (NB == 4 ? 4 : 2))
     k_wide(hops_structure st, int B, int stage, double h, const ST* __restrict__ yin,
            ST* __restrict__ yout, PT* phi, ST* shadow, ST* acc, const double* __restrict__ ws,
@@ -569,7 +569,7 @@ __global__ void __launch_bounds__(wide_threads(NB), NB <= 2 ? 4 : (NB == 4 ? 4 :
       const size_t e = rowa + bg + lane + 32 * j;
       T kk = k[j];
       if (stage == 0 || stage == 4) kk = cscale(kk, (R)sc[j]);
-      if (st.lt_coef && a == 0) {  // LT term of psi_0 (computed from the scaled state)
+      if (LT && a == 0) {  // LT term of psi_0 (computed from the scaled state)
         if constexpr (sizeof(R) == 8) kk = cadd(kk, ld2(ws + bl.physT, s * B + bg + lane + 32 * j));
         else kk = cadd(kk, ld2f(reinterpret_cast<const float*>(ws + bl.physT_f), s * B + bg + lane + 32 * j));
       }
@@ -1021,10 +1021,10 @@ extern "C" int hops_stage_tuning(int32_t nb, int32_t chunk_major) {
   return HOPS_OK;
 }
 
-template <typename R, typename ST, typename PT, bool SITE, int NB>
-static void launch_wide(const hops_structure* st, int B, int stage, double h, const void* yin,
-                        void* yout, void* phi, void* shadow, void* acc, const double* ws,
-                        int chunk_major, cudaStream_t s) {
+template <typename R, typename ST, typename PT, bool SITE, int NB, bool LT>
+static void launch_wide_lt(const hops_structure* st, int B, int stage, double h, const void* yin,
+                           void* yout, void* phi, void* shadow, void* acc, const double* ws,
+                           int chunk_major, cudaStream_t s) {
   const unsigned n_as = (unsigned)st->n_hier * st->n_state;
   const long nchunk = (B + 32 * NB - 1) / (32 * NB);
   constexpr int threads = wide_threads(NB);
@@ -1036,15 +1036,28 @@ static void launch_wide(const hops_structure* st, int B, int stage, double h, co
     int dev = 0;
     cudaGetDevice(&dev);
     if (set_for != dev) {
-      cudaFuncSetAttribute(k_wide<R, ST, PT, SITE, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
+      cudaFuncSetAttribute(k_wide<R, ST, PT, SITE, NB, LT>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       set_for = dev;
     }
   }
-  k_wide<R, ST, PT, SITE, NB><<<grid, threads, smem, s>>>(*st, B, stage, h, (const ST*)yin, (ST*)yout,
-                                                   (PT*)phi, (ST*)shadow, (ST*)acc, ws,
-                                                   FastDiv((unsigned)st->n_state), FastDiv(n_as),
-                                                   chunk_major);
+  k_wide<R, ST, PT, SITE, NB, LT><<<grid, threads, smem, s>>>(
+      *st, B, stage, h, (const ST*)yin, (ST*)yout, (PT*)phi, (ST*)shadow, (ST*)acc, ws,
+      FastDiv((unsigned)st->n_state), FastDiv(n_as), chunk_major);
+}
+
+// The low-temperature term is a separate instantiation: the check alone in the
+// per-segment update measured 9 % on kernels without a correction.
+template <typename R, typename ST, typename PT, bool SITE, int NB>
+static void launch_wide(const hops_structure* st, int B, int stage, double h, const void* yin,
+                        void* yout, void* phi, void* shadow, void* acc, const double* ws,
+                        int chunk_major, cudaStream_t s) {
+  if (st->lt_coef)
+    launch_wide_lt<R, ST, PT, SITE, NB, true>(st, B, stage, h, yin, yout, phi, shadow, acc, ws,
+                                              chunk_major, s);
+  else
+    launch_wide_lt<R, ST, PT, SITE, NB, false>(st, B, stage, h, yin, yout, phi, shadow, acc, ws,
+                                               chunk_major, s);
 }
 
 template <typename R, typename ST, typename PT, bool SITE>
