@@ -603,15 +603,19 @@ __global__ void __launch_bounds__(256) k_narrow(hops_structure st, int B, int st
     for (int r = lane; r < SB; r += 32) {
       const int s = (int)divB.div((unsigned)r);
       const int b = r - s * B;
+      const size_t e = (size_t)a * SB + r;
+      // the element's own streamed operands first: their DRAM latency then
+      // overlaps the neighbour gather instead of following it
+      const PT ph0 = stage == 4 ? PT{} : phi[e];
+      const ST accv = (stage >= 1 && stage <= 3) ? acc_load<true>(acc + e) : ST{};
+      const double sc = scaleB[b];
       auto y = [&](int x, int sp) { return cv<T>(yin[((size_t)x * S + sp) * B + b]); };
       const CoefT<R> cf{ws, bl, B, b};
       T k = deriv_elem<R, SITE>(st, a, s, y, cf);
-      const size_t e = (size_t)a * SB + r;
-      const double sc = scaleB[b];
       if (stage == 0 || stage == 4) k = cscale(k, (R)sc);
       if (st.lt_coef && a == 0) k = cadd(k, cf.phys(s));  // LT term of psi_0 (already scaled)
-      const PT ph = stage == 4 ? PT{} : cscale(phi[e], (decltype(PT{}.x))sc);
-      rk_update<true, T, ST, PT>(stage, h, k, ph, acc, yout, phi, shadow, e);
+      const PT ph = cscale(ph0, (decltype(PT{}.x))sc);
+      rk_finish<true, T, ST, PT>(stage, h, k, ph, accv, acc, yout, phi, shadow, e);
     }
   }
 }
