@@ -3,6 +3,7 @@
 Public API:
   HopsTrajectory  -- drop-in for mesohops.trajectory.hops_trajectory.HopsTrajectory
   HopsEnsemble    -- B trajectories sharing one hierarchy, batched on one GPU
+  DyadicTrajectory -- drop-in for mesohops.trajectory.hops_dyadic.DyadicTrajectory
   bcf_exp, bcf_convert_dl_to_exp -- bath helpers for system dictionaries
 The CUDA library is mesohops_b200/lib/libhops_b200.so (C ABI in
 include/hops_b200.h); build it with ``python -m mesohops_b200.build``.
@@ -22,4 +23,7 @@ def __getattr__(name):
     if name == "HopsEnsemble":
         from .ensemble import HopsEnsemble
         return HopsEnsemble
+    if name == "DyadicTrajectory":
+        from .dyadic import DyadicTrajectory
+        return DyadicTrajectory
     raise AttributeError(name)

@@ -18,6 +18,7 @@ from __future__ import annotations
 import time as timer
 
 import numpy as np
+import scipy.sparse as sps
 import torch
 
 from . import adaptive as _adaptive
@@ -316,6 +317,35 @@ class HopsTrajectory:
     @property
     def phi(self):
         return self._get_state()[0]
+
+    @phi.setter
+    def phi(self, phi):
+        """Replace the hierarchy state (z_mem kept); non-adaptive trajectories."""
+        if self._adhops is not None:
+            raise UnsupportedRequest("setting phi of an adaptive basis",
+                                     "mesohops_b200 HopsTrajectory")
+        phi = np.asarray(phi, dtype=np.complex128).reshape(-1)
+        if len(phi) != self.n_hier * self.n_state:
+            raise UnsupportedRequest(f"phi of length {len(phi)} (expected "
+                                     f"{self.n_hier * self.n_state})", "HopsTrajectory.phi")
+        self._set_state(phi, self._get_state()[1])
+
+    def _operator(self, op):
+        """Act an operator on the state index of every aux of the hierarchy
+        (hops_trajectory.py:540-577): phi[aux] <- op[state_list, state_list] phi[aux].
+        The basis expansion the reference performs around it for state-adaptive
+        bases is not supported (UnsupportedRequest)."""
+        if self._adhops is not None:
+            raise UnsupportedRequest("operator on an adaptive basis",
+                                     "mesohops_b200 HopsTrajectory")
+        sl = np.asarray(self.state_list)
+        if sps.issparse(op):
+            op = sps.csr_matrix(op)[sl, :][:, sl]
+        else:
+            op = np.asarray(op)[np.ix_(sl, sl)]
+        phi = self.phi
+        phi_mat = phi.reshape(self.n_hier, self.n_state).T        # [state, aux]
+        self.phi = np.asarray(op @ phi_mat).T.reshape(-1)
 
     @property
     def z_mem(self):

@@ -9,6 +9,7 @@ files committed next to this script; the GPU box never needs the reference.
     python tests/golden/make_golden.py --effective   # EFFECTIVE_NOISE_INTEGRATION
     python tests/golden/make_golden.py --ltc         # low-temperature corrections
     python tests/golden/make_golden.py --ltc-adaptive  # the same with an adaptive basis
+    python tests/golden/make_golden.py --dyadic      # DyadicTrajectory
 
 Each fixture records the inputs (system, hierarchy depth, noise arrays, psi_0,
 time step) together with the reference outputs (psi_traj, derivative values,
@@ -442,8 +443,80 @@ def main_adaptive():
                      delta, delta, noise_seed=seed)
 
 
+def run_dyadic(name, eom, sparse_input, noise_seed):
+    """DyadicTrajectory (trajectory/hops_dyadic.py) on a 3-site system with a
+    ground state: ket and bra excitations, propagation, a bra de-excitation,
+    more propagation; records the states after each operator, psi_traj, the
+    response normalisation factors and a response-function component."""
+    from mesohops.trajectory.hops_dyadic import DyadicTrajectory
+    nsite = 3
+    H = np.zeros((nsite + 1, nsite + 1))
+    H[1:, 1:] = [[0.0, 50.0, 0.0], [50.0, 30.0, 40.0], [0.0, 40.0, -20.0]]
+    lops = []
+    for i in range(1, nsite + 1):
+        L = np.zeros((nsite + 1, nsite + 1))
+        L[i, i] = 1.0
+        lops.append(sps.coo_matrix(L) if sparse_input else L)
+    gw = [list(bcf_convert_dl_to_exp(50.0, 50.0, 295.0)) for _ in range(nsite)]
+    sysp = {"HAMILTONIAN": sps.coo_matrix(H) if sparse_input else H, "GW_SYSBATH": gw,
+            "L_HIER": lops, "L_NOISE1": lops, "ALPHA_NOISE1": bcf_exp, "PARAM_NOISE1": gw}
+    dt, t1 = 2.0, 10.0
+    tau_noise, tlen = dt / 2, 2 * t1 + 2 * dt
+    n_t = int(np.ceil(tlen / tau_noise)) + 1
+    rng = np.random.default_rng(noise_seed)
+    noise = ((rng.normal(size=(nsite, n_t)) + 1j * rng.normal(size=(nsite, n_t))) * 20.0
+             ).astype(np.complex64)
+    path = os.path.join(tempfile.mkdtemp(), "noise1.npy")
+    np.save(path, noise)
+    hops = DyadicTrajectory(sysp, noise_param={"SEED": path, "MODEL": "PRE_CALCULATED",
+                                               "TLEN": float(tlen), "TAU": float(tau_noise)},
+                            hierarchy_param={"MAXHIER": 2},
+                            eom_param={"EQUATION_OF_MOTION": eom}, storage_param={})
+    psi_k = np.array([1.0, 0, 0, 0], dtype=np.complex128)
+    psi_b = np.array([1.0, 0, 0, 0], dtype=np.complex128)
+    op_ket = np.zeros((nsite + 1, nsite + 1))
+    op_ket[1:, 0] = [1.0, 0.5, 0.25]
+    op_bra = np.zeros((nsite + 1, nsite + 1))
+    op_bra[1:, 0] = [0.3, 1.0, 0.6]
+    op_down = np.zeros((nsite + 1, nsite + 1))
+    op_down[0, 1:] = 1.0
+    conv = (lambda m: sps.coo_matrix(m)) if sparse_input else (lambda m: m)
+    quiet(hops.initialize, psi_k, psi_b)
+    psi_init = np.array(hops.psi)
+    quiet(hops._dyad_operator, conv(op_ket), "ket")
+    psi_op1 = np.array(hops.psi)
+    quiet(hops._dyad_operator, conv(op_bra), "bra")
+    psi_op2 = np.array(hops.psi)
+    quiet(hops.propagate, t1, dt)
+    quiet(hops._dyad_operator, conv(op_down), "bra")
+    psi_op3 = np.array(hops.psi)
+    quiet(hops.propagate, t1, dt)
+    f_op = np.zeros((2 * (nsite + 1), 2 * (nsite + 1)))
+    f_op[nsite + 1, 0] = 1.0      # |bra ground><ket ground|
+    resp = hops._response_function_comp(f_op, 5)
+    np.savez_compressed(
+        os.path.join(HERE, name + ".npz"),
+        H=H, G=np.array([g for g, w in gw]), W=np.array([w for g, w in gw]),
+        L=np.array([np.array(l.toarray() if sps.issparse(l) else l) for l in lops]),
+        sparse_input=sparse_input, eom=eom, depth=2, dt=dt, t1=t1, tau_noise=tau_noise,
+        tlen=tlen, noise1=noise, psi_k=psi_k, psi_b=psi_b, op_ket=op_ket, op_bra=op_bra,
+        op_down=op_down, f_op=f_op, psi_init=psi_init, psi_op1=psi_op1, psi_op2=psi_op2,
+        psi_op3=psi_op3, psi_traj=np.array(hops.storage["psi_traj"]),
+        t_axis=np.array(hops.storage["t_axis"]), phi_end=np.array(hops.phi),
+        norm_sq=np.array(hops.list_response_norm_sq), response=np.array(resp))
+    print(name, "n_hier", hops.n_hier, "n_state", hops.n_state, "norms",
+          np.round(hops.list_response_norm_sq, 4))
+
+
+def main_dyadic():
+    run_dyadic("dyadic_norm_dense", "NORMALIZED NONLINEAR", False, noise_seed=51)
+    run_dyadic("dyadic_linear_sparse", "LINEAR", True, noise_seed=52)
+
+
 if __name__ == "__main__":
-    if "--adaptive" in sys.argv:
+    if "--dyadic" in sys.argv:
+        main_dyadic()
+    elif "--adaptive" in sys.argv:
         main_adaptive()
     elif "--effective" in sys.argv:
         main_effective()
