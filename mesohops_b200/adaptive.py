@@ -116,11 +116,14 @@ class Basis:
 
 # ----------------------------------------------------------------- requests
 class StepRequest:
-    """One RK4 step of ``driver`` in its current basis from (phi, zmem_abs) at t."""
-    __slots__ = ("driver", "phi", "zmem_abs", "t", "tau")
+    """One RK4 step of ``driver`` in its current basis from (phi, zmem_abs) at t.
+    effective: the RK noise slots are EFFECTIVE_NOISE_INTEGRATION window means
+    (integrator_rk.py:115-128) instead of the samples at t, t + tau/2, t + tau."""
+    __slots__ = ("driver", "phi", "zmem_abs", "t", "tau", "effective")
 
-    def __init__(self, driver, phi, zmem_abs, t, tau):
+    def __init__(self, driver, phi, zmem_abs, t, tau, effective=False):
         self.driver, self.phi, self.zmem_abs, self.t, self.tau = driver, phi, zmem_abs, t, tau
+        self.effective = effective
 
 
 class FluxRequest:
@@ -142,11 +145,12 @@ def serve_steps(reqs, device):
             r = reqs[i]
             d = r.driver
             b = d.basis
+            it0, di = d.bind_noise(r)
             trajs.append(d.engine)
             phis.append(r.phi)
             zms.append(r.zmem_abs[b.modes] if b.n_mode else None)
-            it0s.append(d.noise_index(r.t))
-            dis.append(d.noise_di(r.tau))
+            it0s.append(it0)
+            dis.append(di)
             hs.append(r.tau / hbar)
         st, phis_o, zms_o = ResidentRunner(device).run_packed(trajs, phis, zms, it0s, dis, 1, hs)
         if np.any(st != 0):
@@ -158,10 +162,11 @@ def serve_steps(reqs, device):
             continue
         d = r.driver
         b = d.basis
+        it0, di = d.bind_noise(r)
         eng = d.engine
         eng.set_state(r.phi.reshape(1, -1),
                       r.zmem_abs[b.modes].reshape(1, -1) if b.n_mode else None)
-        eng.propagate(d.noise_index(r.t), d.noise_di(r.tau), 1, r.tau / hbar, tuned=False)
+        eng.propagate(it0, di, 1, r.tau / hbar, tuned=False)
         eng.check_status()
         phi, z = eng.get_state()
         out[i] = (phi[0], z[0])
@@ -380,6 +385,59 @@ class AdaptiveHops:
                 self._engine.set_noise(n1.unsqueeze(0) if n1 is not None else None,
                                        n2.unsqueeze(0) if n2 is not None else None)
         return self._engine
+
+    def bind_noise(self, req):
+        """Bind the noise rows a step request reads to the current engine and
+        return its (first noise index, index step): the samples, or for an
+        effective-noise request the window means on the half-step grid (the
+        slots of the step at t are windows 2t/tau, +1, +2)."""
+        eng = self.engine
+        b = self.basis
+        if not req.effective:
+            rows = (b.dstruct.extra.get("noise1"), b.dstruct.extra.get("noise2"))
+            it0, di = self.noise_index(req.t), self.noise_di(req.tau)
+        else:
+            key = ("eff", req.tau)
+            if getattr(b, "_eff_key", None) != key:
+                e1, e2 = self._effective_host(req.tau)
+                l_abs = b.tables["l_abs"]
+                dev = self.device
+                b._eff_rows = tuple(
+                    (torch.from_numpy(np.ascontiguousarray(e[l_abs])).to(dev)
+                     if e is not None and b.tables["n_lop"] else None) for e in (e1, e2))
+                b._eff_key = key
+            rows = b._eff_rows
+            half = req.tau * 0.5
+            it0 = int(round(req.t / half))
+            if abs(it0 * half - req.t) >= precision:
+                raise UnsupportedRequest("EFFECTIVE_NOISE_INTEGRATION with a step start off "
+                                         "the half-step grid", "mesohops_b200 adaptive")
+            di = 1
+        if isinstance(eng, StreamBatch):
+            eng.set_noise(rows[0].unsqueeze(0) if rows[0] is not None else None,
+                          rows[1].unsqueeze(0) if rows[1] is not None else None)
+        else:
+            eng.set_noise(rows[0], rows[1])
+        return it0, di
+
+    def _effective_host(self, tau):
+        """Window means of every noise row for steps of tau (host copies, cached)."""
+        if getattr(self, "_eff_tau", None) != tau:
+            from .noise import window_means
+            k = int(round(tau * 0.5 / self.traj.noise1.param["TAU"]))
+            out = []
+            for nd in (self.noise1_dev, self.noise2_dev):
+                if nd is None:
+                    out.append(None)
+                    continue
+                n_out = nd.shape[-1] // k
+                out.append(window_means(nd, 0, k, n_out,
+                                        bool(self.traj.noise1.param["FLAG_REAL"])
+                                        if nd is self.noise1_dev else
+                                        bool(self.traj.noise2.param["FLAG_REAL"])).cpu().numpy())
+            self._eff_host_rows = tuple(out)
+            self._eff_tau = tau
+        return self._eff_host_rows
 
     def noise_index(self, t):
         return self.traj.noise1.time_index(t)
@@ -701,7 +759,11 @@ class AdaptiveHops:
         Returns the z_mem the reference stores with this step (the one from
         before the step: hops_trajectory.py:523-526 stores self.z_mem before
         assigning the new value)."""
-        phi, z = yield StepRequest(self, self.phi, self.zmem_abs, self.t, tau)
+        # the propagate loop passes EFFECTIVE_NOISE_INTEGRATION to its steps; the
+        # inch-worm re-steps below take the plain samples, as the reference does
+        # (hops_trajectory.py:457-460 against :684)
+        phi, z = yield StepRequest(self, self.phi, self.zmem_abs, self.t, tau,
+                                   effective=self.traj.effective_noise_integration)
         phi = self._normalize(phi)
         if self.early_counter < self.early_steps:
             if self.early == "INCH_WORM":

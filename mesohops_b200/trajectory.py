@@ -101,9 +101,6 @@ class HopsTrajectory:
         psi_0 = np.array(psi_0, dtype=np.complex128)
         dev = torch.device(self.device_param["DEVICE"])
         if self.eom_param["ADAPTIVE"]:
-            if self.effective_noise_integration:
-                raise UnsupportedRequest("EFFECTIVE_NOISE_INTEGRATION with an adaptive basis",
-                                         "mesohops_b200 HopsTrajectory")
             self._initialize_adaptive(psi_0, dev)
             self.storage.metadata["INITIALIZATION_TIME"] = timer.time() - t0
             self.__initialized__ = True

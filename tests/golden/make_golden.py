@@ -10,6 +10,7 @@ files committed next to this script; the GPU box never needs the reference.
     python tests/golden/make_golden.py --ltc         # low-temperature corrections
     python tests/golden/make_golden.py --ltc-adaptive  # the same with an adaptive basis
     python tests/golden/make_golden.py --dyadic      # DyadicTrajectory
+    python tests/golden/make_golden.py --effective-adaptive  # effective noise, adaptive basis
 
 Each fixture records the inputs (system, hierarchy depth, noise arrays, psi_0,
 time step) together with the reference outputs (psi_traj, derivative values,
@@ -352,9 +353,10 @@ def main_ltc_adaptive():
 
 
 def run_adaptive(name, sysp, depth, psi0, t_max, dt, delta_a, delta_s, noise_seed,
-                 update_step=1, f_discard=0.0, extra=None):
-    """Adaptive propagation with PRE_CALCULATED noise; records the basis per step."""
-    tau_noise = dt / 2.0
+                 update_step=1, f_discard=0.0, extra=None, tau_noise=None, integration=None):
+    """Adaptive propagation with PRE_CALCULATED noise; records the basis per step.
+    tau_noise: noise time step (default dt / 2); integration: integration_param."""
+    tau_noise = dt / 2.0 if tau_noise is None else tau_noise
     tlen = t_max + dt
     n_t = int(np.ceil(tlen / tau_noise)) + 1
     nl = n_unique(sysp)
@@ -367,7 +369,8 @@ def run_adaptive(name, sysp, depth, psi0, t_max, dt, delta_a, delta_s, noise_see
                                              "TLEN": float(tlen), "TAU": float(tau_noise)},
                           hierarchy_param={"MAXHIER": depth},
                           eom_param={"EQUATION_OF_MOTION": "NORMALIZED NONLINEAR"},
-                          storage_param={})
+                          storage_param={},
+                          **({} if integration is None else {"integration_param": integration}))
     # adaptive_noise=False: the reference only supports sparse noise storage for
     # FFT_FILTER (hops_noise.py:244-245,320-323); values are the same either way
     hops.make_adaptive(delta_a, delta_s, update_step=update_step, f_discard=f_discard,
@@ -508,6 +511,21 @@ def run_dyadic(name, eom, sparse_input, noise_seed):
           np.round(hops.list_response_norm_sq, 4))
 
 
+def main_effective_adaptive():
+    """Adaptive basis with EFFECTIVE_NOISE_INTEGRATION (noise axis dt / 8, windows
+    of 4 samples); the reference's inch-worm sub-steps take the plain samples."""
+    n = 8
+    rng = np.random.default_rng(3)
+    H = np.diag(rng.normal(0, 100, n))
+    for i in range(n - 1):
+        H[i, i + 1] = H[i + 1, i] = 50.0
+    psi0 = np.zeros(n, dtype=np.complex128)
+    psi0[n // 2] = 1.0
+    eff = {"INTEGRATOR": "RUNGE_KUTTA", "EFFECTIVE_NOISE_INTEGRATION": True}
+    run_adaptive("adaptive_chain8_eff", site_system(H, [(50, 50, 295)]), 3, psi0, 120.0, 4.0,
+                 3e-4, 3e-4, noise_seed=35, tau_noise=0.5, integration=eff)
+
+
 def main_dyadic():
     run_dyadic("dyadic_norm_dense", "NORMALIZED NONLINEAR", False, noise_seed=51)
     run_dyadic("dyadic_linear_sparse", "LINEAR", True, noise_seed=52)
@@ -516,6 +534,8 @@ def main_dyadic():
 if __name__ == "__main__":
     if "--dyadic" in sys.argv:
         main_dyadic()
+    elif "--effective-adaptive" in sys.argv:
+        main_effective_adaptive()
     elif "--adaptive" in sys.argv:
         main_adaptive()
     elif "--effective" in sys.argv:

@@ -24,7 +24,8 @@ from mesohops_b200.exceptions import UnsupportedRequest
 from oracle import hops_oracle as O
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-CASES = ["adaptive_dod_full", "adaptive_chain8", "adaptive_chain12", "adaptive_chain8_ltc"]
+CASES = ["adaptive_dod_full", "adaptive_chain8", "adaptive_chain12", "adaptive_chain8_ltc",
+         "adaptive_chain8_eff"]
 
 
 def load(name):
@@ -51,7 +52,12 @@ def make_traj(f, tmp_path, device):
                           hierarchy_param={"MAXHIER": int(f["depth"])},
                           eom_param={"EQUATION_OF_MOTION": "NORMALIZED NONLINEAR"},
                           storage_param={}, device_param={"DEVICE": device,
-                                                          "PRECISION": "complex128"})
+                                                          "PRECISION": "complex128"},
+                          # the fixture with noise finer than dt / 2 was made with
+                          # EFFECTIVE_NOISE_INTEGRATION (make_golden.py --effective-adaptive)
+                          integration_param={"INTEGRATOR": "RUNGE_KUTTA",
+                                             "EFFECTIVE_NOISE_INTEGRATION":
+                                             2 * float(f["tau_noise"]) < float(f["dt"]) - 1e-12})
     hops.make_adaptive(float(f["delta_a"]), float(f["delta_s"]),
                        update_step=int(f["update_step"]), f_discard=float(f["f_discard"]),
                        adaptive_noise=False)
@@ -78,8 +84,11 @@ class OracleServer:
     def step(self, r):
         d = r.driver
         ob = self.sub(d.basis)
-        tl = [r.t, r.t + 0.5 * r.tau, r.t + r.tau]
-        zr = O.noise_lookup(self.noise1[ob.l_abs], tl, self.tau_noise)
+        if r.effective:
+            zr = O.effective_noise(self.noise1[ob.l_abs], r.t, r.tau, self.tau_noise)
+        else:
+            tl = [r.t, r.t + 0.5 * r.tau, r.t + r.tau]
+            zr = O.noise_lookup(self.noise1[ob.l_abs], tl, self.tau_noise)
         zm = r.zmem_abs[d.basis.modes]
         phi, z = O.rk4_step(ob, r.phi, zm, zr, np.zeros_like(zr), r.tau)
         return d.finish_step(r, phi, z)

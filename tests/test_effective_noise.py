@@ -40,21 +40,6 @@ def test_oracle_effective_noise_pinned(name):
     assert np.max(np.abs(psi_plain - ref)) > 1e-6
 
 
-def test_effective_noise_rejected_with_adaptive_basis():
-    from mesohops_b200 import HopsTrajectory
-    from mesohops_b200.exceptions import UnsupportedRequest
-    f = load_golden("eff_dimer_k4")
-    hops = HopsTrajectory(golden_system(f),
-                          noise_param={"MODEL": "ZERO", "TLEN": 100.0, "TAU": 0.5},
-                          hierarchy_param={"MAXHIER": 2},
-                          integration_param={"INTEGRATOR": "RUNGE_KUTTA",
-                                             "EFFECTIVE_NOISE_INTEGRATION": True},
-                          device_param={"DEVICE": "cpu"})
-    hops.make_adaptive(1e-3, 1e-3)
-    with pytest.raises(UnsupportedRequest):
-        hops.initialize(f["psi0"])
-
-
 def make_traj(f, kernel, precision="complex128"):
     from mesohops_b200 import HopsTrajectory
     from mesohops_b200.bath import bcf_exp

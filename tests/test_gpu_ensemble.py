@@ -1,6 +1,7 @@
 """Batched ensembles (one structure, B trajectories, layout [aux][state][traj])
-against the CPU oracle run trajectory by trajectory.  B = 40 and 33 exercise the
-wide kernel with a partial 32-trajectory chunk, B = 7 the narrow kernel."""
+against the CPU oracle run trajectory by trajectory.  B = 40, 33 and 129 exercise
+the wide kernel with a partial last chunk, B = 32 the smallest wide batch, B = 31
+and 7 the narrow kernel, B = 1 the single-trajectory case."""
 import numpy as np
 import pytest
 
@@ -42,14 +43,15 @@ def oracle_psi(f, noise_b, n_steps):
 
 
 @pytest.mark.parametrize("name,B", [("ring6", 40), ("ring6", 7), ("general_lop", 33),
-                                    ("chain4_2mode", 64)])
+                                    ("chain4_2mode", 64), ("ring6", 1), ("ring6", 31),
+                                    ("ring6", 32), ("ring6", 129)])
 def test_ensemble_c128_matches_oracle(cuda_device, name, B):
     f = load_golden(name)
     n_steps = 12
     noise = ensemble_noise(f, B, 5)
     psi, ens = run_ensemble(f, B, "complex128", noise, n_steps)
     phi, _ = ens.state()
-    for b in sorted({0, 1, B // 2, B - 1}):
+    for b in sorted({0, min(1, B - 1), B // 2, B - 1}):
         ref, phi_ref = oracle_psi(f, noise[b], n_steps)
         assert np.max(np.abs(psi[:, b] - ref)) <= 1e-10 * np.max(np.abs(ref))
         assert np.max(np.abs(phi[b] - phi_ref)) <= 1e-10 * np.max(np.abs(phi_ref))
@@ -119,3 +121,27 @@ def test_stage_kernel_shapes_agree(cuda_device, name, B, tuning):
     ref = run_forced(f, B, "complex128", noise, n_steps, (2, 0))
     got = run_forced(f, B, "complex128", noise, n_steps, tuning)
     assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+
+def test_c_abi_rejects_bad_propagation_arguments(cuda_device):
+    """hops_rk4_propagate refuses a noise window past the noise axis and negative
+    step / index arguments with HOPS_EINVAL and an error text, launching nothing:
+    the state is unchanged afterwards."""
+    import ctypes as C
+    from mesohops_b200 import _lib
+    from mesohops_b200.engine import _stream
+    f = load_golden("ring6")
+    B = 40
+    noise = ensemble_noise(f, B, 8)
+    _, ens = run_ensemble(f, B, "complex128", noise, 1)
+    before, _ = ens.state()
+    L = _lib.lib()
+    b = ens.batch
+    n_t = noise.shape[2]
+    for it0, di, n in [(0, 1, n_t), (n_t, 1, 1), (-1, 1, 1), (0, -1, 1), (0, 1, -1)]:
+        rc = L.hops_rk4_propagate(C.byref(b.st.cstruct), C.byref(b.cb), it0, di, n, 0.01,
+                                  None, _stream(cuda_device))
+        assert rc == _lib.HOPS_EINVAL, (it0, di, n)
+        assert L.hops_last_error()
+    after, _ = ens.state()
+    assert np.array_equal(before, after)
