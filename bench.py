@@ -160,7 +160,7 @@ def run_gpu(args):
     tau_noise = dt / 2.0
     tlen = (W + 2 * K + 120 + wl["n_steps"]) * dt + dt
     noise = {"MODEL": "FFT_FILTER", "TLEN": float(tlen), "TAU": tau_noise,
-             "SEED": list(range(rank * B, rank * B + B))}
+             "SEED": rank_seeds(rank, B)}
     sysp = wl["system"]()
     ens = HopsEnsemble(sysp, B, noise_param=noise, hierarchy_param={"MAXHIER": depth},
                        precision=args.precision, device=dev)
@@ -185,11 +185,7 @@ def run_gpu(args):
     if world > 1:
         dist.barrier()
     clocks = sampler.stop()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), dev)
     ens.check()
     value = B * K * world / (ms / 1e3)
     launches = 8 * K + 3
@@ -243,8 +239,16 @@ def run_gpu(args):
                           "peak_source": "of measured" if peaks else "of fallback"}
     result["clocks"] = clocks
 
-    if rank == 0 and not args.no_extras:
-        result.update(extras(args, wl, sysp, ens, dev, value, K))
+    if not args.no_extras:
+        # every rank: the end-to-end number at N GPUs (max wall clock over ranks)
+        sec, ke, h2d, d2h = e2e_leg(ens, B, K, dt, dev)
+        result["e2e"] = e2e_record(B, world, max_over_ranks(sec, dev), ke, h2d, d2h)
+        # the single-GPU legs take minutes; at N > 1 they would keep the other
+        # ranks waiting past the process-group timeout, so they run at N = 1
+        if world == 1:
+            result.update(extras(args, wl, sysp, ens, dev, value, K))
+        else:
+            result["single_gpu_legs"] = "reported by the N = 1 run"
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -252,9 +256,58 @@ def run_gpu(args):
         print(json.dumps(result), flush=True)
 
 
+def e2e_leg(ens, B, K, dt, dev):
+    """End to end through the public API with host buffers: every step copies its
+    noise window host->device (pinned) and reads psi back device->host.  Returns
+    (seconds of this rank's host wall clock, steps, h2d bytes, d2h bytes)."""
+    import torch
+    ke = min(K, 50)
+    noise_host = ens.noise.cpu().pin_memory()
+    psi_dev = torch.empty((1, B, ens.n_state), dtype=torch.complex128, device=dev)
+    psi_host = torch.empty((1, B, ens.n_state), dtype=torch.complex128).pin_memory()
+    di = int(round(dt * 0.5 / ens.noise_param["TAU"]))
+    h2d = d2h = 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        it0 = int(round(ens.t / ens.noise_param["TAU"]))
+        sl = slice(it0, it0 + 2 * di + 1)
+        ens.noise[:, :, sl].copy_(noise_host[:, :, sl], non_blocking=True)
+        h2d += noise_host[:, :, sl].numel() * 8
+        ens.propagate(dt, dt, psi_out=psi_dev)
+        psi_host.copy_(psi_dev, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        d2h += psi_host.numel() * 16
+    return time.perf_counter() - t0, ke, h2d, d2h
+
+
+def e2e_record(B, world, seconds, ke, h2d, d2h):
+    return {"value": round(B * world * ke / seconds, 2), "unit": UNIT,
+            "h2d_bytes_per_step": int(h2d / ke), "d2h_bytes_per_step": int(d2h / ke),
+            "note": "HopsEnsemble.propagate one step per call, noise window h2d from pinned "
+                    "memory and psi d2h each step, host wall clock (max over ranks)"}
+
+
+def rank_seeds(rank, B):
+    """Noise seeds of one rank: disjoint blocks of B per rank (weak scaling)."""
+    return list(range(rank * B, rank * B + B))
+
+
+def max_over_ranks(x, device):
+    """Max of a float over the ranks of the process group (x itself without one)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def extras(args, wl, sysp, ens, dev, value, K):
-    """Plain complex128 path, accuracy of the batched complex64 path, the
-    end-to-end API number and the CPU baseline (rank 0 only)."""
+    """Single-GPU legs (N = 1 only): plain complex128 path, accuracy of the
+    batched reduced-precision path, the CPU baseline, the served stream and the
+    adaptive batch."""
     import torch
     from mesohops_b200.ensemble import HopsEnsemble
     from mesohops_b200.constants import hbar
@@ -304,30 +357,6 @@ def extras(args, wl, sysp, ens, dev, value, K):
         "sample": f"{B} trajectories x {na} steps; the complex128 GPU path matches the "
                   "FP64 CPU oracle to <=1e-10 (tests/test_gpu_parity.py)"}
 
-    # end to end through the public API with host buffers: every step copies its
-    # noise window host->device (pinned) and reads psi back device->host
-    ke = min(K, 50)
-    noise_host = ens.noise.cpu().pin_memory()
-    psi_dev = torch.empty((1, B, ens.n_state), dtype=torch.complex128, device=dev)
-    psi_host = torch.empty((1, B, ens.n_state), dtype=torch.complex128).pin_memory()
-    di = int(round(dt * 0.5 / ens.noise_param["TAU"]))
-    h2d = d2h = 0
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(ke):
-        it0 = int(round(ens.t / ens.noise_param["TAU"]))
-        sl = slice(it0, it0 + 2 * di + 1)
-        ens.noise[:, :, sl].copy_(noise_host[:, :, sl], non_blocking=True)
-        h2d += noise_host[:, :, sl].numel() * 8
-        ens.propagate(dt, dt, psi_out=psi_dev)
-        psi_host.copy_(psi_dev, non_blocking=True)
-        torch.cuda.current_stream().synchronize()
-        d2h += psi_host.numel() * 16
-    e2e_s = time.perf_counter() - t0
-    out["e2e"] = {"value": round(B * ke / e2e_s, 2), "unit": UNIT,
-                  "h2d_bytes_per_step": int(h2d / ke), "d2h_bytes_per_step": int(d2h / ke),
-                  "note": "HopsEnsemble.propagate one step per call, noise window h2d "
-                          "from pinned memory and psi d2h each step, host wall clock"}
     out["cpu_baseline"] = cpu_baseline(wl, sysp)
     if not args.no_served:
         out["served"] = served_leg(args, dev)
