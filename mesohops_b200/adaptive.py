@@ -110,8 +110,11 @@ class Basis:
             return False
         if not np.array_equal(np.sort(states), self.states):
             return False
-        keys = self.aux.keyer.keys_from_counts(np.asarray(counts))
-        return np.array_equal(np.sort(keys), self.aux.keys)
+        # the aux rows are unique, so equal lengths and equal row sets suffice
+        if getattr(self, "_row_set", None) is None:
+            self._row_set = {r.tobytes() for r in self.counts}
+        rows = np.ascontiguousarray(np.asarray(counts, dtype=self.counts.dtype))
+        return {r.tobytes() for r in rows} == self._row_set
 
 
 # ----------------------------------------------------------------- requests
@@ -419,6 +422,33 @@ class AdaptiveHops:
         else:
             eng.set_noise(rows[0], rows[1])
         return it0, di
+
+    def apply_operator(self, op):
+        """_operator (hops_trajectory.py:540-577) on the adaptive basis: with state
+        adaptivity the states op reaches from the basis join it first (phi
+        permuted and rescaled as in update_basis), op acts on the state index of
+        every aux, and the early-time integrator restarts so that the next steps
+        update the basis by inch-worm again."""
+        import scipy.sparse as sps
+        b = self.basis
+        if self.adaptive_s:
+            if sps.issparse(op):
+                reach = np.unique(sps.csr_matrix(op)[:, b.states].nonzero()[0])
+            else:
+                reach = np.nonzero(np.asarray(op)[:, b.states])[0]
+            states_u = np.array(sorted(set(b.states.tolist()) | set(int(x) for x in reach)),
+                                dtype=np.int64)
+            self.phi = self.update_basis(self.phi, states_u, b.counts)
+            b = self.basis
+        sl = b.states
+        if sps.issparse(op):
+            sub = sps.csr_matrix(op)[sl, :][:, sl]
+        else:
+            sub = np.asarray(op)[np.ix_(sl, sl)]
+        phi_mat = self.phi.reshape(b.n_hier, b.n_state).T
+        self.phi = np.asarray(sub @ phi_mat).T.reshape(-1).astype(np.complex128)
+        if self.adaptive_s:
+            self.early_counter = 0
 
     def _effective_host(self, tau):
         """Window means of every noise row for steps of tau (host copies, cached)."""

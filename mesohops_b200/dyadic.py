@@ -105,7 +105,8 @@ class DyadicTrajectory(HopsTrajectory):
                 op[:n, :n] = op_hilbert
         self._operator(op)
         phi = self.phi
-        nrm = np.linalg.norm(phi[:len(sl)]) ** 2
+        # the state basis may have grown (adaptive): the norm is over the new one
+        nrm = np.linalg.norm(phi[:len(self.state_list)]) ** 2
         if self.eom_param["EQUATION_OF_MOTION"] == "NORMALIZED NONLINEAR":
             self._list_response_norm_sq.append(nrm)
             self.phi = phi / np.sqrt(np.sum(np.abs(phi[:self.n_state]) ** 2))

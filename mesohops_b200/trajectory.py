@@ -317,24 +317,24 @@ class HopsTrajectory:
 
     @phi.setter
     def phi(self, phi):
-        """Replace the hierarchy state (z_mem kept); non-adaptive trajectories."""
-        if self._adhops is not None:
-            raise UnsupportedRequest("setting phi of an adaptive basis",
-                                     "mesohops_b200 HopsTrajectory")
+        """Replace the hierarchy state in the current basis (z_mem kept)."""
         phi = np.asarray(phi, dtype=np.complex128).reshape(-1)
         if len(phi) != self.n_hier * self.n_state:
             raise UnsupportedRequest(f"phi of length {len(phi)} (expected "
                                      f"{self.n_hier * self.n_state})", "HopsTrajectory.phi")
+        if self._adhops is not None:
+            self._adhops.phi = phi.copy()
+            return
         self._set_state(phi, self._get_state()[1])
 
     def _operator(self, op):
         """Act an operator on the state index of every aux of the hierarchy
-        (hops_trajectory.py:540-577): phi[aux] <- op[state_list, state_list] phi[aux].
-        The basis expansion the reference performs around it for state-adaptive
-        bases is not supported (UnsupportedRequest)."""
+        (hops_trajectory.py:540-577): phi[aux] <- op[state_list, state_list] phi[aux];
+        a state-adaptive basis first takes in the states op reaches and restarts
+        its early-time integrator."""
         if self._adhops is not None:
-            raise UnsupportedRequest("operator on an adaptive basis",
-                                     "mesohops_b200 HopsTrajectory")
+            self._adhops.apply_operator(op)
+            return
         sl = np.asarray(self.state_list)
         if sps.issparse(op):
             op = sps.csr_matrix(op)[sl, :][:, sl]

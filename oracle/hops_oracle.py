@@ -401,7 +401,8 @@ class OracleSubBasis(OracleBasis):
                     "LT": np.asarray(full.get("LT", np.zeros(len(full["L"]))))[self.l_abs]}
         self.states, self.modes = states, modes
         self.nstate, self.nmode = len(states), len(modes)
-        self.aux = np.asarray(aux, dtype=np.int64)[:, modes].reshape(-1, len(modes))
+        aux = np.asarray(aux, dtype=np.int64)
+        self.aux = aux[:, modes].reshape(len(aux), len(modes))
         self.nhier = len(self.aux)
         self.index = {tuple(v): i for i, v in enumerate(self.aux)}
         self._build_super_operators()

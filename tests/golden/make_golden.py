@@ -446,7 +446,7 @@ def main_adaptive():
                      delta, delta, noise_seed=seed)
 
 
-def run_dyadic(name, eom, sparse_input, noise_seed):
+def run_dyadic(name, eom, sparse_input, noise_seed, adaptive=None):
     """DyadicTrajectory (trajectory/hops_dyadic.py) on a 3-site system with a
     ground state: ket and bra excitations, propagation, a bra de-excitation,
     more propagation; records the states after each operator, psi_traj, the
@@ -475,6 +475,8 @@ def run_dyadic(name, eom, sparse_input, noise_seed):
                                                "TLEN": float(tlen), "TAU": float(tau_noise)},
                             hierarchy_param={"MAXHIER": 2},
                             eom_param={"EQUATION_OF_MOTION": eom}, storage_param={})
+    if adaptive is not None:
+        hops.make_adaptive(adaptive[0], adaptive[1], adaptive_noise=False)
     psi_k = np.array([1.0, 0, 0, 0], dtype=np.complex128)
     psi_b = np.array([1.0, 0, 0, 0], dtype=np.complex128)
     op_ket = np.zeros((nsite + 1, nsite + 1))
@@ -506,7 +508,8 @@ def run_dyadic(name, eom, sparse_input, noise_seed):
         op_down=op_down, f_op=f_op, psi_init=psi_init, psi_op1=psi_op1, psi_op2=psi_op2,
         psi_op3=psi_op3, psi_traj=np.array(hops.storage["psi_traj"]),
         t_axis=np.array(hops.storage["t_axis"]), phi_end=np.array(hops.phi),
-        norm_sq=np.array(hops.list_response_norm_sq), response=np.array(resp))
+        norm_sq=np.array(hops.list_response_norm_sq), response=np.array(resp),
+        adaptive=np.array(adaptive if adaptive is not None else [0.0, 0.0]))
     print(name, "n_hier", hops.n_hier, "n_state", hops.n_state, "norms",
           np.round(hops.list_response_norm_sq, 4))
 
@@ -529,6 +532,8 @@ def main_effective_adaptive():
 def main_dyadic():
     run_dyadic("dyadic_norm_dense", "NORMALIZED NONLINEAR", False, noise_seed=51)
     run_dyadic("dyadic_linear_sparse", "LINEAR", True, noise_seed=52)
+    run_dyadic("dyadic_adaptive", "NORMALIZED NONLINEAR", False, noise_seed=53,
+               adaptive=(1e-3, 1e-3))
 
 
 if __name__ == "__main__":

@@ -3,10 +3,12 @@
 Fixtures tests/golden/dyadic_*.npz come from the unmodified reference
 (tests/golden/make_golden.py --dyadic): a 3-site system with a ground state,
 ket and bra excitations, propagation, a bra de-excitation and more
-propagation, for the normalised equation of motion with dense operators and
-the LINEAR one with sparse operators.  On the CPU the operator bookkeeping
+propagation, for the normalised equation of motion with dense operators, the
+LINEAR one with sparse operators, and the normalised one on an adaptive basis
+(which the operators grow).  On the CPU the operator bookkeeping
 (states after each operator, normalisation factors, response function) is
-checked without propagation; on the GPU the whole sequence must match the
+checked without propagation, and the adaptive sequence with the device
+requests served by the oracle; on the GPU the whole sequence must match the
 reference to 1e-10 (complex128)."""
 import numpy as np
 import pytest
@@ -18,6 +20,9 @@ from mesohops_b200.dyadic import dyad_conversion, response_function_calc
 from mesohops_b200.exceptions import UnsupportedRequest
 
 FIXTURES = ["dyadic_norm_dense", "dyadic_linear_sparse"]
+# the same sequence with an adaptive basis (delta_a = delta_s = 1e-3): states the
+# operators reach join the basis, which the early-time integrator then updates
+ADAPTIVE = ["dyadic_adaptive"]
 
 
 def system(f):
@@ -38,6 +43,9 @@ def make(f, device):
                             hierarchy_param={"MAXHIER": int(f["depth"])},
                             eom_param={"EQUATION_OF_MOTION": str(f["eom"])},
                             device_param={"DEVICE": device, "PRECISION": "complex128"})
+    if "adaptive" in f and float(f["adaptive"][0]) > 0:
+        hops.make_adaptive(float(f["adaptive"][0]), float(f["adaptive"][1]),
+                           adaptive_noise=False)
     hops.initialize(f["psi_k"], f["psi_b"])
     return hops, conv
 
@@ -74,12 +82,14 @@ def test_response_function_calc_matches_reference(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", FIXTURES)
+@pytest.mark.parametrize("name", FIXTURES + ADAPTIVE)
 def test_dyadic_trajectory_matches_reference(cuda_device, name):
     f = load_golden(name)
     hops, conv = make(f, "cuda:0")
     hops._dyad_operator(conv(f["op_ket"]), "ket")
+    np.testing.assert_allclose(hops.psi, f["psi_op1"], rtol=1e-12, atol=1e-14)
     hops._dyad_operator(conv(f["op_bra"]), "bra")
+    np.testing.assert_allclose(hops.psi, f["psi_op2"], rtol=1e-12, atol=1e-14)
     dt, t1 = float(f["dt"]), float(f["t1"])
     hops.propagate(t1, dt)
     hops._dyad_operator(conv(f["op_down"]), "bra")
@@ -93,3 +103,36 @@ def test_dyadic_trajectory_matches_reference(cuda_device, name):
     resp = hops._response_function_comp(f["f_op"], 5)
     scale = max(1e-300, np.max(np.abs(f["response"])))
     assert np.max(np.abs(resp - f["response"])) <= 1e-10 * scale
+
+
+def test_dyadic_adaptive_sequence_oracle_served(monkeypatch):
+    """The adaptive sequence with the device requests served by the oracle: the
+    basis grows by the states the operators reach, and states, norms, psi(t)
+    and the response function equal the reference's."""
+    import mesohops_b200.adaptive as ad
+    from test_adaptive import OracleServer
+    f = load_golden("dyadic_adaptive")
+    from mesohops_b200.dyadic import DyadicTrajectory
+    sysp, conv = system(f)
+    hops = DyadicTrajectory(sysp, noise_param={"SEED": f["noise1"], "MODEL": "PRE_CALCULATED",
+                                               "TLEN": float(f["tlen"]),
+                                               "TAU": float(f["tau_noise"])},
+                            hierarchy_param={"MAXHIER": int(f["depth"])},
+                            eom_param={"EQUATION_OF_MOTION": str(f["eom"])},
+                            device_param={"DEVICE": "cpu", "PRECISION": "complex128"})
+    server = OracleServer(sysp, f["noise1"], float(f["tau_noise"]))  # sysp is dyadic now
+    monkeypatch.setattr(ad, "drive", server.drive)
+    hops.make_adaptive(float(f["adaptive"][0]), float(f["adaptive"][1]), adaptive_noise=False)
+    hops.initialize(f["psi_k"], f["psi_b"])
+    for key, op, side in [("psi_op1", "op_ket", "ket"), ("psi_op2", "op_bra", "bra")]:
+        hops._dyad_operator(conv(f[op]), side)
+        np.testing.assert_allclose(hops.psi, f[key], rtol=1e-12, atol=1e-14)
+    hops.propagate(float(f["t1"]), float(f["dt"]))
+    hops._dyad_operator(conv(f["op_down"]), "bra")
+    np.testing.assert_allclose(hops.psi, f["psi_op3"], rtol=1e-10, atol=1e-12)
+    hops.propagate(float(f["t1"]), float(f["dt"]))
+    psi = np.array(hops.storage["psi_traj"])
+    assert np.max(np.abs(psi - f["psi_traj"])) <= 1e-10 * np.max(np.abs(f["psi_traj"]))
+    np.testing.assert_allclose(hops.list_response_norm_sq, f["norm_sq"], rtol=1e-10)
+    np.testing.assert_allclose(hops._response_function_comp(f["f_op"], 5), f["response"],
+                               rtol=1e-10, atol=1e-14)
