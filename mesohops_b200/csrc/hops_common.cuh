@@ -166,13 +166,22 @@ __device__ void stage_scalars(const hops_structure& st, const StageIO& io, Get g
     double2 num = mk(0.0, 0.0);
     const bool act = st.lop_active[j] != 0;
     if (!linear && act) {
-      const int base = j * (S + 1);
-      for (int r = 0; r < S; ++r) {
-        int q0 = st.l_ptr[base + r], q1 = st.l_ptr[base + r + 1];
-        if (q0 == q1) continue;
-        double2 row = mk(0.0, 0.0);
-        for (int q = q0; q < q1; ++q) row = cfma(ld2(st.l_val, q), get(0, st.l_col[q]), row);
-        num = cadd(num, cconjmul(get(0, r), row));
+      if (st.site_projector) {
+        // L_j = v_j |s_j><s_j|: the one nonzero row, same operations as below
+        const int sj = st.lop_site[j];
+        if (sj >= 0) {
+          const double2 row = cfma(ld2(st.lop_sval, j), get(0, sj), mk(0.0, 0.0));
+          num = cadd(num, cconjmul(get(0, sj), row));
+        }
+      } else {
+        const int base = j * (S + 1);
+        for (int r = 0; r < S; ++r) {
+          int q0 = st.l_ptr[base + r], q1 = st.l_ptr[base + r + 1];
+          if (q0 == q1) continue;
+          double2 row = mk(0.0, 0.0);
+          for (int q = q0; q < q1; ++q) row = cfma(ld2(st.l_val, q), get(0, st.l_col[q]), row);
+          num = cadd(num, cconjmul(get(0, r), row));
+        }
       }
       num = mk(num.x / n2, num.y / n2);
     }
@@ -239,14 +248,24 @@ __device__ void stage_scalars(const hops_structure& st, const StageIO& io, Get g
       if (!st.lop_active[j]) continue;
       const int base = j * (S + 1);
       double2 t1 = mk(0.0, 0.0), t2 = mk(0.0, 0.0);
-      for (int r = 0; r < S; ++r) {
-        double2 p0 = get(0, r);
-        t2 = cadd(t2, cconjmul(p0, getf(f, r)));
-        int q0 = st.l_ptr[base + r], q1 = st.l_ptr[base + r + 1];
-        if (q0 == q1) continue;
-        double2 row = mk(0.0, 0.0);
-        for (int q = q0; q < q1; ++q) row = cfma(ld2(st.l_val, q), getf(f, st.l_col[q]), row);
-        t1 = cadd(t1, cconjmul(p0, row));
+      if (st.site_projector) {
+        // one nonzero row of L_j: t1 has the single term of row s_j
+        for (int r = 0; r < S; ++r) t2 = cadd(t2, cconjmul(get(0, r), getf(f, r)));
+        const int sj = st.lop_site[j];
+        if (sj >= 0) {
+          const double2 row = cfma(ld2(st.lop_sval, j), getf(f, sj), mk(0.0, 0.0));
+          t1 = cadd(t1, cconjmul(get(0, sj), row));
+        }
+      } else {
+        for (int r = 0; r < S; ++r) {
+          double2 p0 = get(0, r);
+          t2 = cadd(t2, cconjmul(p0, getf(f, r)));
+          int q0 = st.l_ptr[base + r], q1 = st.l_ptr[base + r + 1];
+          if (q0 == q1) continue;
+          double2 row = mk(0.0, 0.0);
+          for (int q = q0; q < q1; ++q) row = cfma(ld2(st.l_val, q), getf(f, st.l_col[q]), row);
+          t1 = cadd(t1, cconjmul(p0, row));
+        }
       }
       double2 gw = ld2(st.mode_gw, m);
       // -(g/w) (t1 - <L> t2)
