@@ -5,7 +5,9 @@ EOM with or without an adaptive basis, noise, psi_0, t_max, dt) arrive over
 time.  The server
 
 * admits a request when its HBM footprint fits what is left of the budget
-  (requests that can never fit are rejected with a status; the rest wait);
+  (requests that can never fit are rejected with a status; the rest wait),
+  holding requests for the streaming kernel back while light ones wait or
+  run, up to ``heavy_hold_s`` (shortest job first, with ageing);
 * builds its device state (structure tables, correlated noise, phi) on a
   builder thread while the GPU keeps stepping the admitted requests;
 * advances every admitted request by up to ``chunk_steps`` RK4 steps per tick:
@@ -144,7 +146,8 @@ def footprint(req, precision):
     return vec + table + noise + psi, kern
 
 
-def plan_admission(queue, arrival, used, budget, now, fairness_s, precision, small_frac=0.02):
+def plan_admission(queue, arrival, used, budget, now, fairness_s, precision, small_frac=0.02,
+                   hold_heavy=False, heavy_hold_s=0.0):
     """Admission decisions for the waiting requests (in arrival order).
 
     Returns (admit [(req, bytes, kernel)], reject [(req, bytes)]): a request whose
@@ -152,7 +155,11 @@ def plan_admission(queue, arrival, used, budget, now, fairness_s, precision, sma
     first-fit while the budget lasts.  Once the oldest waiting request has
     waited longer than fairness_s, later requests overtake it only if they are
     small (at most small_frac of the budget), so a large request is not starved
-    and small ones do not queue behind it."""
+    and small ones do not queue behind it.  hold_heavy (set by the server while
+    light requests -- adaptive or resident-kernel ones -- wait or run): heavy
+    requests (streaming kernel) younger than heavy_hold_s are held back, so the
+    short jobs are not slowed by the long ones sharing the GPU (shortest job
+    first, with ageing)."""
     admit, reject = [], []
     blocked = False
     head_seen = False
@@ -160,6 +167,8 @@ def plan_admission(queue, arrival, used, budget, now, fairness_s, precision, sma
         fp, kern = footprint(req, precision)
         if fp > budget:
             reject.append((req, fp))
+            continue
+        if hold_heavy and kern == "streaming" and now - arrival[req.rid] <= heavy_hold_s:
             continue
         if blocked and fp > small_frac * budget:
             continue
@@ -190,14 +199,18 @@ class HopsServer:
     """Continuous-batching server for HOPS trajectories on one GPU."""
 
     def __init__(self, device="cuda:0", precision="mixed", hbm_budget=None, chunk_steps=32,
-                 builders=2, realtime=True, fairness_s=1.0, adaptive_workers=0):
+                 builders=2, realtime=True, fairness_s=1.0, adaptive_workers=0,
+                 heavy_hold_s=10.0):
         """hbm_budget: device bytes the admitted requests may hold (default 80 %
         of the free memory).  realtime: honour the arrival times (False: every
         request is present at t = 0).  fairness_s: once the oldest waiting
         request has waited this long, later ones are not admitted ahead of it.
         adaptive_workers: > 0 runs the adaptive requests in that many worker
         processes on the same GPU (adaptive_pool.AdaptiveWorkers), so their
-        host-side basis updates run in parallel; 0 steps them in this process."""
+        host-side basis updates run in parallel; 0 steps them in this process.
+        heavy_hold_s: while light requests (adaptive, or small enough for the
+        resident kernel) wait or run, requests for the streaming kernel are
+        admitted only once they have waited this long (0: no holding)."""
         self.device = torch.device(device)
         self.precision = precision
         if hbm_budget is None:
@@ -208,6 +221,7 @@ class HopsServer:
         self.builders = int(builders)
         self.realtime = realtime
         self.fairness_s = float(fairness_s)
+        self.heavy_hold_s = float(heavy_hold_s)
         self.stats = {}
         self.pool = None
         if adaptive_workers > 0:
@@ -278,8 +292,13 @@ class HopsServer:
                 now = clock()
                 while pending and arrival[pending[0].rid] <= now:
                     queue.append(pending.popleft())
+                light = (bool(pooled) or any(a.kernel != "streaming" for a in active)
+                         or any(k != "streaming" for _, _, _, k in building)
+                         or any(footprint(r, self.precision)[1] != "streaming" for r in queue))
                 admit, reject = plan_admission(list(queue), arrival, used, self.budget, now,
-                                               self.fairness_s, self.precision)
+                                               self.fairness_s, self.precision,
+                                               hold_heavy=self.heavy_hold_s > 0 and light,
+                                               heavy_hold_s=self.heavy_hold_s)
                 for req, fp in reject:
                     queue.remove(req)
                     results[req.rid] = ServedResult(

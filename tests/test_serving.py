@@ -75,6 +75,29 @@ def test_admission_first_fit_reject_and_fairness():
     assert [r.rid for r, _, _ in admit] == [0]
 
 
+def test_heavy_requests_held_while_light_ones_run():
+    """Shortest job first with ageing: a streaming-kernel request waits while
+    light requests run, unless it has waited longer than heavy_hold_s."""
+    heavy = _req(0, ring20(), 4, 10)
+    light = _req(1, dimer(), 4, 10, arrival=0.001)
+    assert sv.footprint(heavy, "mixed")[1] == "streaming"
+    assert sv.footprint(light, "mixed")[1] == "resident"
+    arrival = {0: 0.0, 1: 0.001}
+    big = 1 << 40
+    admit, _ = sv.plan_admission([heavy, light], arrival, used=0, budget=big, now=1.0,
+                                 fairness_s=1.0, precision="mixed", hold_heavy=True,
+                                 heavy_hold_s=10.0)
+    assert [r.rid for r, _, _ in admit] == [1]
+    admit, _ = sv.plan_admission([heavy, light], arrival, used=0, budget=big, now=11.0,
+                                 fairness_s=100.0, precision="mixed", hold_heavy=True,
+                                 heavy_hold_s=10.0)
+    assert [r.rid for r, _, _ in admit] == [0, 1]
+    admit, _ = sv.plan_admission([heavy, light], arrival, used=0, budget=big, now=1.0,
+                                 fairness_s=1.0, precision="mixed", hold_heavy=False,
+                                 heavy_hold_s=10.0)
+    assert [r.rid for r, _, _ in admit] == [0, 1]
+
+
 def test_served_stream_specs_are_seeded():
     s1 = served_stream_specs(64)
     s2 = served_stream_specs(64)
