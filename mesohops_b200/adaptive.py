@@ -24,12 +24,13 @@ basis sizes in one persistent launch) and ONE flux-error launch.
 from __future__ import annotations
 
 import numpy as np
+import scipy.sparse as sps
 import torch
 
 from . import _lib
 from ._lib import HopsFluxTask, EOM_CODES
 from .constants import hbar, precision
-from .device import DeviceStructure, build_tables
+from .device import DeviceStructure, _state_mode_tables, build_tables
 from .engine import ResidentRunner, ResidentTrajectory, StreamBatch
 from .exceptions import TrajectoryError, UnsupportedRequest
 from .hierarchy import AuxBasis, AuxKeyer, apply_static_filters, triangular_counts
@@ -77,7 +78,8 @@ class Basis:
         self.modes = np.array(sorted(hier_modes | state_modes), dtype=np.int64)
         self.aux = AuxBasis(counts, keyer, maxhier, modes=self.modes)
         self.counts = self.aux.counts
-        self.tables = build_tables(system, self.aux, self.states, self.modes)
+        part = _state_mode_part(system, self.states, self.modes)
+        self.tables = build_tables(system, self.aux, self.states, self.modes, small=part["small"])
         # the noise rows of the basis L list travel with the structure tables
         extras = {}
         for name, nh in zip(("noise1", "noise2"), noise_host):
@@ -87,22 +89,12 @@ class Basis:
         self.n_hier = self.aux.n_hier
         self.n_state = len(self.states)
         self.n_mode = len(self.modes)
-        self.rel_mode = {int(m): i for i, m in enumerate(self.modes)}
+        self.rel_mode = part["rel_mode"]
         self.depth = self.aux.depth
         # K2_aux_by_mode (hops_basis.py:1140-1151)
         self.k_aux = np.ascontiguousarray(self.counts[:, self.modes].T.astype(np.uint8))
-        # M2_mode_from_state_diag (hops_basis.py:1031-1050), dense [mode, state]
-        self.lred = [system.lop_block(j, self.states) for j in self.tables["l_abs"]]
-        rel_l = {int(j): i for i, j in enumerate(self.tables["l_abs"])}
-        self.m2 = np.zeros((self.n_mode, self.n_state), dtype=np.complex128)
-        for i, m in enumerate(self.modes):
-            self.m2[i] = np.diag(self.lred[rel_l[int(system.l_by_mode[m])]])
-        # HopsSystem.list_sc: states outside the basis coupled to it by H
-        sset = set(self.states.tolist())
-        sc = set()
-        for s in self.states:
-            sc.update(int(c) for c in system.coupled_states[s])
-        self.list_sc = np.array(sorted(sc - sset), dtype=np.int64)
+        self.lred, self.m2 = part["lred"], part["m2"]
+        self.list_sc, self.h_sc = part["list_sc"], part["h_sc"]
 
     def same_as(self, states, counts):
         states = np.asarray(states)
@@ -115,6 +107,48 @@ class Basis:
             self._row_set = {r.tobytes() for r in self.counts}
         rows = np.ascontiguousarray(np.asarray(counts, dtype=self.counts.dtype))
         return {r.tobytes() for r in rows} == self._row_set
+
+
+# Parts of a basis that depend only on its states and modes, shared by every
+# basis (of any trajectory of the same system) with the same two lists: an
+# adaptive basis usually changes its aux list while its states stay.
+_PART_CACHE_SIZE = 512
+
+
+def _state_mode_part(system, states, modes):
+    cache = system.__dict__.setdefault("_adaptive_part_cache", {})
+    key = (states.tobytes(), modes.tobytes())
+    part = cache.get(key)
+    if part is not None:
+        return part
+    small = _state_mode_tables(system, states, modes)
+    l_abs = small["l_abs"]
+    # M2_mode_from_state_diag (hops_basis.py:1031-1050), dense [mode, state]
+    lred = [system.lop_block(j, states) for j in l_abs]
+    rel_l = {int(j): i for i, j in enumerate(l_abs)}
+    m2 = np.zeros((len(modes), len(states)), dtype=np.complex128)
+    for i, m in enumerate(modes):
+        m2[i] = np.diag(lred[rel_l[int(system.l_by_mode[m])]])
+    # HopsSystem.list_sc: states outside the basis coupled to it by H
+    sset = set(states.tolist())
+    sc = set()
+    for s in states:
+        sc.update(int(c) for c in system.coupled_states[s])
+    list_sc = np.array(sorted(sc - sset), dtype=np.int64)
+    h_sc = None
+    if len(list_sc):
+        H = system.hamiltonian
+        blk = (sps.csr_matrix(H)[list_sc][:, states].toarray() if sps.issparse(H)
+               else np.asarray(H)[np.ix_(list_sc, states)])
+        h_sc = -1j * np.asarray(blk, dtype=np.complex128)
+    for a in [m2, list_sc] + lred + ([h_sc] if h_sc is not None else []):
+        a.flags.writeable = False
+    part = dict(small=small, lred=lred, m2=m2, list_sc=list_sc, h_sc=h_sc,
+                rel_mode={int(m): i for i, m in enumerate(modes)})
+    if len(cache) >= _PART_CACHE_SIZE:
+        cache.pop(next(iter(cache)))
+    cache[key] = part
+    return part
 
 
 # ----------------------------------------------------------------- requests
@@ -574,8 +608,7 @@ class AdaptiveHops:
         b = self.basis
         if len(b.list_sc) == 0:
             return np.zeros(b.n_hier)
-        H = -1j * self.Hd[np.ix_(b.list_sc, b.states)]
-        D = (H @ phi_sn) / hbar
+        D = (b.h_sc @ phi_sn) / hbar
         return np.sum(np.abs(D) ** 2, axis=0)
 
     def _hierarchy_gen(self, phi, dt, z_step):
@@ -617,27 +650,28 @@ class AdaptiveHops:
         discarded = np.sum(Eu[Eu <= thresh]) + np.sum(Ed[Ed <= thresh])
         Eu = np.where(Eu <= thresh, 0.0, Eu)
         Ed = np.where(Ed <= thresh, 0.0, Ed)
-        acc = {}
-        for i, a in enumerate(idx_stable):
-            base = b.counts[a]
-            for m in np.nonzero(Eu[:, i])[0]:
-                v = base.copy()
-                v[b.modes[m]] += 1
-                key = v.tobytes()
-                acc[key] = acc.get(key, 0.0) + Eu[m, i]
-            if np.any(Ed[:, i]):
-                for mabs in np.nonzero(base)[0]:
-                    m = b.rel_mode[int(mabs)]
-                    if Ed[m, i] != 0:
-                        v = base.copy()
-                        v[mabs] -= 1
-                        key = v.tobytes()
-                        acc[key] = acc.get(key, 0.0) + Ed[m, i]
-        if not acc:
+        # candidate aux with their error terms, in the order of a loop over the
+        # stable aux (flux up along each mode, then flux down along each of its
+        # modes); the terms of one candidate are summed in that order
+        iu, mu = np.nonzero(Eu.T)
+        idn, md = np.nonzero(Ed.T)
+        n_abs = self.system.n_mode
+        cand = np.concatenate([b.counts[idx_stable[iu]], b.counts[idx_stable[idn]]], axis=0)
+        cand[np.arange(len(iu)), b.modes[mu]] += 1
+        cand[len(iu) + np.arange(len(idn)), b.modes[md]] -= 1
+        vals = np.concatenate([Eu[mu, iu], Ed[md, idn]])
+        order = np.argsort(np.concatenate([2 * iu, 2 * idn + 1]), kind="stable")
+        cand, vals = cand[order].reshape(-1, n_abs), vals[order]
+        if len(vals) == 0:
             return []
-        vals = np.array(list(acc.values()))
-        thresh = error_thresh(np.sort(vals), bound_sq, offset=discarded)
-        return [np.frombuffer(k, dtype=b.counts.dtype) for k, v in acc.items() if v > thresh]
+        keys = self.keyer.sort_keys(cand)
+        _, first, inv = np.unique(keys, return_index=True, return_inverse=True)
+        sums = np.zeros(len(first))
+        np.add.at(sums, inv.ravel(), vals)
+        seq = np.argsort(first)                     # first-occurrence order
+        sums, rows = sums[seq], cand[first[seq]]
+        thresh = error_thresh(np.sort(sums), bound_sq, offset=discarded)
+        return list(rows[sums > thresh])
 
     # ----------------------------------------------------------------- states
     def _state_gen(self, phi, dt, z_step, idx_stable_aux, bound_aux):
@@ -693,7 +727,7 @@ class AdaptiveHops:
         # error_sflux_boundary_state (:997-1132)
         bound_states = []
         if len(rel_stable) < self.system.n_state and len(b.list_sc):
-            Hsc = -1j * self.Hd[np.ix_(b.list_sc, stable_states)]
+            Hsc = b.h_sc[:, rel_stable]
             Cst = phi_sn[np.ix_(rel_stable, idx_stable_aux)]
             Esc = np.sum(np.abs(Hsc @ (Cst / hbar)) ** 2, axis=1)
             nz = np.nonzero(Esc)[0]
@@ -827,7 +861,7 @@ class AdaptiveHops:
                                    | set(b.states.tolist())), dtype=np.int64)
         counts_new = np.asarray(counts_new, dtype=np.int16).reshape(-1, self.system.n_mode)
         allc = np.concatenate([b.counts, counts_new], axis=0)
-        allk = self.keyer.keys_from_counts(allc)
+        allk = self.keyer.sort_keys(allc)
         _, first = np.unique(allk, return_index=True)
         counts_u = allc[np.sort(first)]
         self.phi = self.update_basis(self.phi, states_u, counts_u)

@@ -66,17 +66,19 @@ def _i32_any(a):
     return np.asarray(a).astype(np.int32)
 
 
-def build_tables(system, basis, state_list=None, mode_list=None):
+def build_tables(system, basis, state_list=None, mode_list=None, small=None):
     """Host arrays of one basis.
 
     state_list: sorted absolute states of the state basis (default: all).
     mode_list:  sorted absolute modes of the mode basis (default: basis.modes).
+    small:      ``_state_mode_tables`` of these states and modes when the caller
+                has them already (copied, not modified).
     Returns a dict of numpy arrays and sizes plus index maps.
     """
     S_abs = system.n_state
     states = np.arange(S_abs) if state_list is None else np.asarray(state_list, dtype=np.int64)
     modes = basis.modes if mode_list is None else np.asarray(mode_list, dtype=np.int64)
-    small = _state_mode_tables(system, states, modes)
+    small = _state_mode_tables(system, states, modes) if small is None else dict(small)
     M = small["n_mode"]
     mode_lop, sval = small["mode_lop"], small["lop_sval"]
     W = small["mode_w"]

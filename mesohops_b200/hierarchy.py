@@ -13,7 +13,10 @@ tuple c_0 <= ... <= c_{k-1} maps to the strictly increasing b_i = c_i + i in
 combinations is sum_i C(n-1-b_{i-1}, k-i) - C(n-b_i, k-i) (b_{-1} = -1).
 Adding the number of aux of depth < k gives a global key whose order equals
 the reference order, so any aux subset is sorted, and neighbours are found,
-with integer arithmetic (searchsorted) instead of string manipulation.
+with integer arithmetic (searchsorted) instead of string manipulation.  Where
+the ranks exceed int64 (e.g. 500 modes to depth 10) the sort keys are
+fixed-width byte strings (depth, then the sorted mode tuple, big-endian) with
+the same order and equality.
 """
 from __future__ import annotations
 
@@ -54,7 +57,9 @@ class AuxKeyer:
         depth = counts.sum(axis=1).astype(np.int64)
         if depth.size and depth.max() > self.D:
             raise AuxError("aux deeper than MAXHIER")
-        keys = np.zeros(N, dtype=np.int64 if self.use_int64 else object)
+        if self.use_int64:
+            return self._keys_int64(counts, depth)
+        keys = np.zeros(N, dtype=object)
         for k in np.unique(depth):
             idx = np.nonzero(depth == k)[0]
             if k == 0:
@@ -69,6 +74,58 @@ class AuxKeyer:
             keys[idx] = self._rank(tup, int(k)) + self.offsets[k]
             del rows
         return keys
+
+    @staticmethod
+    def _tuples(counts, depth):
+        """Sorted mode tuples of all rows laid end to end: (row, mode, position
+        in the row's tuple) of every entry and the start of each row."""
+        N = counts.shape[0]
+        row, mode = np.nonzero(counts)
+        reps = counts[row, mode].astype(np.int64)
+        row_t = np.repeat(row, reps)
+        c = np.repeat(mode.astype(np.int64), reps)
+        start = np.zeros(N + 1, dtype=np.int64)
+        np.cumsum(depth, out=start[1:])
+        i = np.arange(len(c), dtype=np.int64) - start[row_t]
+        return row_t, c, i, start
+
+    def _keys_int64(self, counts, depth):
+        """keys_from_counts for every depth at once (int64 keys): each row's
+        rank is a difference of running sums of its per-position binomial
+        terms."""
+        row_t, c, i, start = self._tuples(counts, depth)
+        k = depth[row_t]
+        n = self.M + k - 1
+        b = c + i
+        prev = np.empty_like(b)
+        prev[1:] = b[:-1]
+        prev[i == 0] = -1
+        B = self.binom64
+        term = B[n - 1 - prev, k - i] - B[n - b, k - i]
+        cs = np.zeros(len(term) + 1, dtype=np.int64)
+        np.cumsum(term, out=cs[1:])
+        keys = cs[start[1:]] - cs[start[:-1]]
+        off = np.asarray(self.offsets, dtype=np.int64)
+        return keys + np.where(depth > 0, off[np.minimum(depth, len(off) - 1)], 0)
+
+    def sort_keys(self, counts):
+        """Keys whose order is the aux order and whose equality is aux equality,
+        in a fixed-width numpy dtype: the global ranks when they fit in int64,
+        else byte strings of the depth followed by the sorted mode tuple
+        (big-endian, so that byte order is the reference's order: depth first,
+        then lexicographic)."""
+        counts = np.asarray(counts)
+        if self.use_int64:
+            return self.keys_from_counts(counts)
+        depth = counts.sum(axis=1).astype(np.int64)
+        if depth.size and depth.max() > self.D:
+            raise AuxError("aux deeper than MAXHIER")
+        row_t, c, i, _ = self._tuples(counts, depth)
+        w = ">u2" if self.M < (1 << 16) else ">u4"
+        arr = np.zeros((counts.shape[0], self.D + 1), dtype=w)
+        arr[:, 0] = depth
+        arr[row_t, 1 + i] = c
+        return np.ascontiguousarray(arr).view(f"S{arr.itemsize * (self.D + 1)}").ravel()
 
     def _rank(self, tup, k):
         n = self.M + k - 1
@@ -155,7 +212,7 @@ class AuxBasis:
 
     def __init__(self, counts, keyer, maxhier, modes=None):
         counts = np.asarray(counts)
-        keys = keyer.keys_from_counts(counts)
+        keys = keyer.sort_keys(counts)
         order = np.argsort(keys, kind="stable")
         self.counts = counts[order]
         self.keys = keys[order]
@@ -171,7 +228,7 @@ class AuxBasis:
 
     def index_of(self, counts):
         """Indices of the given aux (count rows) in this basis, -1 if absent."""
-        k = self.keyer.keys_from_counts(counts)
+        k = self.keyer.sort_keys(counts)
         pos = np.searchsorted(self.keys, k)
         pos = np.minimum(pos, self.n_hier - 1)
         found = self.keys[pos] == k

@@ -49,6 +49,25 @@ def test_big_mode_keys_exact():
     assert keys[2] == 501 and keys[3] == 502
 
 
+@pytest.mark.parametrize("M,D", [(7, 4), (500, 10)])
+def test_sort_keys_order_and_equality_are_the_ranks(M, D):
+    """sort_keys (int64 ranks, or fixed-width byte keys when the ranks exceed
+    int64) orders and identifies aux exactly as the exact global ranks do."""
+    k = H.AuxKeyer(M, D)
+    rng = np.random.default_rng(1)
+    c = np.zeros((400, M), dtype=np.int16)
+    for r in range(1, len(c)):
+        np.add.at(c[r], rng.integers(0, min(M, 12), rng.integers(1, D + 1)), 1)
+    exact = np.array([int(x) for x in k.keys_from_counts(c)], dtype=object)
+    sk = k.sort_keys(c)
+    o = np.argsort(exact, kind="stable")
+    assert np.array_equal(o, np.argsort(sk, kind="stable"))
+    assert np.array_equal(exact[o][1:] == exact[o][:-1], sk[o][1:] == sk[o][:-1])
+    assert np.array_equal(H.AuxBasis(c[np.unique(sk, return_index=True)[1]], k, D).counts,
+                          c[np.unique(sk, return_index=True)[1]][np.argsort(
+                              exact[np.unique(sk, return_index=True)[1]], kind="stable")])
+
+
 def test_missing_zero_aux_raises():
     c = np.array([[1, 0], [0, 1]])
     with pytest.raises(AuxError):
