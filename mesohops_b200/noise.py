@@ -39,20 +39,24 @@ def raw_slot_index(ntaus):
 
 def raw_white_noise(seed, lops, ntaus, rand_model="SUM_GAUSSIAN"):
     """Uncorrelated complex64 draws [len(lops), 2(ntaus-1)] (hops_noise.py:453-590)."""
+    if rand_model not in ("SUM_GAUSSIAN", "BOX_MULLER"):
+        raise UnsupportedRequest(f"Noise.param[RAND_MODEL] {rand_model}", "Noise._prepare_rand")
     re, im = raw_slot_index(ntaus)
-    out = np.empty((len(lops), 2 * (ntaus - 1)), dtype=np.complex64)
+    x = np.empty((len(lops), 4 * (ntaus - 1)), dtype=np.float64)
+    # jumped() leaves its generator untouched, so one seeded PCG64 serves every
+    # L-operator of the trajectory (SEED None: fresh entropy per row, as the
+    # reference constructs one generator per row)
+    base = np.random.PCG64(seed=seed) if seed is not None else None
     for i, lop in enumerate(lops):
-        gen = np.random.default_rng(np.random.PCG64(seed=seed).jumped(int(lop)))
+        bg = (base if base is not None else np.random.PCG64(seed=None)).jumped(int(lop))
+        gen = np.random.Generator(bg)
         if rand_model == "SUM_GAUSSIAN":
-            x = gen.normal(loc=0, size=4 * (ntaus - 1))
-            out[i] = np.complex64(x[re] + 1j * x[im])
-        elif rand_model == "BOX_MULLER":
-            x = gen.random(size=4 * (ntaus - 1))
-            out[i] = np.complex64(np.sqrt(-2.0 * np.log(x[re])) * np.exp(2.0j * np.pi * x[im]))
+            x[i] = gen.normal(loc=0, size=4 * (ntaus - 1))
         else:
-            raise UnsupportedRequest(f"Noise.param[RAND_MODEL] {rand_model}",
-                                     "Noise._prepare_rand")
-    return out
+            x[i] = gen.random(size=4 * (ntaus - 1))
+    if rand_model == "SUM_GAUSSIAN":
+        return np.complex64(x[:, re] + 1j * x[:, im])
+    return np.complex64(np.sqrt(-2.0 * np.log(x[:, re])) * np.exp(2.0j * np.pi * x[:, im]))
 
 
 def filter_on_device(alpha, z_raw, device):
