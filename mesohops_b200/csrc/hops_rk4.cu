@@ -356,12 +356,20 @@ constexpr size_t wide_smem_bytes(int warps) {
 // is held to 64 registers (4 CTAs of 256 threads, 32 warps per SM), NB = 4 to
 // 128 (4 CTAs of 128 threads); both measured faster than the registers the
 // compiler would otherwise take.  NB = 8 is left nearly uncapped.
+// Resident CTAs per SM that the NB = 4 stage kernel is compiled for (its
+// register budget: 65536 / (128 threads x this) per thread).  4 is the
+// fastest on the 20-site ring: 5 or 6 (96 / 80 registers, more warps, more of
+// the SM's on-chip memory as shared memory) made the mixed-precision stage
+// 1.4x / 1.8x slower.
+#ifndef HOPS_WIDE_MIN_BLOCKS4
+#define HOPS_WIDE_MIN_BLOCKS4 4
+#endif
 // CTA size of k_wide: 256 threads for NB <= 2, else 128 (finer occupancy
 // steps at the register counts the wider tasks take).
 constexpr int wide_threads(int nb) { return nb <= 2 ? 256 : 128; }
 
 template <typename R, typename ST, typename PT, bool SITE, int NB, bool LT>
-__global__ void __launch_bounds__(wide_threads(NB), NB <= 2 ? 4 : (NB == 4 ? 4 : 2))
+__global__ void __launch_bounds__(wide_threads(NB), NB <= 2 ? 4 : (NB == 4 ? HOPS_WIDE_MIN_BLOCKS4 : 2))
     k_wide(hops_structure st, int B, int stage, double h, const ST* __restrict__ yin,
            ST* __restrict__ yout, PT* phi, ST* shadow, ST* acc, const double* __restrict__ ws,
            FastDiv divS, FastDiv divAS, int chunk_major) {
