@@ -360,7 +360,7 @@ constexpr size_t wide_smem_bytes(int warps) {
 // register budget: 65536 / (128 threads x this) per thread).  4 is the
 // fastest on the 20-site ring: 5 or 6 (96 / 80 registers, more warps, more of
 // the SM's on-chip memory as shared memory) made the mixed-precision stage
-// 1.4x / 1.8x slower.
+// 1.4x / 1.8x slower, 3 (148 registers, 12 warps per SM) 1.24x slower.
 #ifndef HOPS_WIDE_MIN_BLOCKS4
 #define HOPS_WIDE_MIN_BLOCKS4 4
 #endif
