@@ -140,6 +140,8 @@ typedef struct hops_batch {
   const float* noise2; /* [B][n_lop][n_t2] complex64, or NULL for zero noise 2 */
   int32_t* status;     /* [B] 0 ok, HOPS_ENONFINITE if a norm went NaN/Inf */
   void* phi_lo;        /* HOPS_PREC_MIXED: complex64 copy of phi read by stage 1 */
+  int32_t defer_scale; /* 1: hops_rk4_propagate leaves the renormalisation of its
+                          last step pending (see there) */
 } hops_batch;
 
 /* One trajectory of hops_resident_propagate (array in device memory). */
@@ -206,11 +208,22 @@ int hops_dsystem_dt(const hops_structure* st, hops_batch* bt, const float* z1_de
  * index it0; stage noise is read at it0 + 2*n*di + {0, di, di, 2*di}.  For the
  * normalized EOM the state is renormalised after every step; psi_out_dev
  * (nullable) receives [n_steps][B][n_state] complex128 normalised psi_0 after
- * each step.  On return phi holds the normalised state.
+ * each step.  On return phi holds the normalised state -- unless
+ * bt->defer_scale is set: then the last step's 1/||psi_0|| stays pending in
+ * the workspace (phi and phi_lo unscaled, psi_out_dev already normalised),
+ * the next hops_rk4_propagate or hops_dsystem_dt applies it on the fly as the
+ * steps within one call do, and hops_batch_settle applies it to phi.  That
+ * saves a read and write of the whole state per call when the caller steps
+ * one call at a time (hops_trajectory.py:456-533 calls the integrator once
+ * per step).
  */
 int hops_rk4_propagate(const hops_structure* st, hops_batch* bt, int32_t it0,
                        int32_t di, int32_t n_steps, double tau_over_hbar,
                        double* psi_out_dev, void* stream);
+
+/* Apply a pending renormalisation (bt->defer_scale) to phi and phi_lo and
+ * reset it to 1; status is kept.  No counterpart in the reference. */
+int hops_batch_settle(const hops_structure* st, hops_batch* bt, void* stream);
 
 /*
  * Resident propagation: one CTA per task, all n_steps steps of every task in

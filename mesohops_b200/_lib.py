@@ -50,7 +50,7 @@ class HopsBatch(C.Structure):
         ("n_traj", _i), ("precision", _i), ("eom", _i), ("n_t1", _i), ("n_t2", _i),
         ("phi", _p), ("acc", _p), ("y0", _p), ("y1", _p),
         ("zmem", _p), ("work", _p), ("noise1", _p), ("noise2", _p), ("status", _p),
-        ("phi_lo", _p),
+        ("phi_lo", _p), ("defer_scale", _i),
     ]
 
 
@@ -114,6 +114,7 @@ def lib():
     L.hops_tri_max_depth.argtypes = []
     L.hops_tri_pass1.argtypes = [_i, _i, _p, C.c_int64, _p, _p, _p, _p]
     L.hops_tri_pass2.argtypes = [_i, _i, _p, C.c_int64, C.c_int64, _p, _p, _p, _p, _p, _p, _p]
+    L.hops_batch_settle.argtypes = [C.POINTER(HopsStructure), C.POINTER(HopsBatch), _p]
     L.hops_flux_errors_smem_doubles.restype = _i
     L.hops_flux_errors_smem_doubles.argtypes = [_i, _i, _i]
     L.hops_kernel_timing.argtypes = [C.c_int]
@@ -143,4 +144,4 @@ def exported_symbols():
             "hops_kernel_timing_read", "hops_noalloc_scratch_bytes",
             "hops_rk4_propagate_noalloc", "hops_stage_tuning", "hops_flux_errors",
             "hops_flux_errors_smem_doubles", "hops_tri_max_depth", "hops_tri_pass1",
-            "hops_tri_pass2", "hops_noise_window_mean"]
+            "hops_tri_pass2", "hops_noise_window_mean", "hops_batch_settle"]

@@ -1161,7 +1161,7 @@ static int propagate_impl(const hops_structure* st, hops_batch* bt, int32_t it0,
     double* psi_last = psi_out ? psi_out + (size_t)(n_steps - 1) * psi_stride : nullptr;
     k_finalize<PT><<<B, 128, 0, s>>>(*st, *bt, psi_last, normalized ? 1 : 0);
     LAUNCH_CHECK();
-    if (normalized) {
+    if (normalized && !bt->defer_scale) {
       const size_t E = (size_t)st->n_hier * B * S;
       long blocks = (long)((E + 255) / 256);
       if (blocks > (long)sm_count() * 8) blocks = (long)sm_count() * 8;
@@ -1185,6 +1185,36 @@ extern "C" int hops_batch_reset(const hops_structure* st, hops_batch* bt, void* 
   const BatchLayout bl(st->n_state, st->n_mode, st->n_lop, bt->n_traj);
   k_reset<<<(bt->n_traj + 127) / 128, 128, 0, (cudaStream_t)stream>>>(
       bt->work, lay.stride, bl.scaleB, bt->n_traj, bt->status, 1);
+  LAUNCH_CHECK();
+  return HOPS_OK;
+}
+
+template <typename PT, typename ST>
+static void settle_impl(const hops_structure* st, hops_batch* bt, cudaStream_t s) {
+  const int B = bt->n_traj, S = st->n_state;
+  const size_t E = (size_t)st->n_hier * B * S;
+  long blocks = (long)((E + 255) / 256);
+  if (blocks > (long)sm_count() * 8) blocks = (long)sm_count() * 8;
+  const ScalarLayout lay(S, st->n_mode, st->n_lop);
+  const BatchLayout bl(S, st->n_mode, st->n_lop, B);
+  void* shadow = bt->precision == HOPS_PREC_MIXED ? bt->phi_lo : nullptr;
+  k_apply_scale<PT, ST><<<(int)blocks, 256, 0, s>>>((PT*)bt->phi, (ST*)shadow, B, E,
+                                                     bt->work + bl.scaleB);
+  k_reset<<<(B + 127) / 128, 128, 0, s>>>(bt->work, lay.stride, bl.scaleB, B, nullptr, 0);
+}
+
+extern "C" int hops_batch_settle(const hops_structure* st, hops_batch* bt, void* stream) {
+  int rc = check_structure(st);
+  if (rc) return rc;
+  if ((rc = check_batch(st, bt))) return rc;
+  if (bt->eom != HOPS_EOM_NORMALIZED_NONLINEAR) return HOPS_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (bt->precision == HOPS_PREC_C128)
+    settle_impl<double2, double2>(st, bt, s);
+  else if (bt->precision == HOPS_PREC_MIXED)
+    settle_impl<double2, float2>(st, bt, s);
+  else
+    settle_impl<float2, float2>(st, bt, s);
   LAUNCH_CHECK();
   return HOPS_OK;
 }

@@ -84,12 +84,36 @@ class StreamBatch:
         b.noise1 = b.noise2 = None
         b.n_t1 = b.n_t2 = 0
         b.phi_lo = self.phi_lo.data_ptr() if self.phi_lo is not None else None
+        b.defer_scale = 0
         self.cb = b
+        self._pending = False
         self.reset()
+
+    @property
+    def defer_scale(self):
+        """Leave the renormalisation after each propagate call pending in the
+        workspace (applied on the fly by the next call, or by ``settle``)
+        instead of rescaling the whole state in a separate pass."""
+        return bool(self.cb.defer_scale)
+
+    @defer_scale.setter
+    def defer_scale(self, on):
+        if not on:
+            self.settle()
+        self.cb.defer_scale = 1 if on else 0
+
+    def settle(self):
+        """Apply a pending renormalisation to phi (no-op when none is pending)."""
+        if self._pending:
+            rc = _lib.lib().hops_batch_settle(C.byref(self.st.cstruct), C.byref(self.cb),
+                                              _stream(self.dev))
+            _lib.check(rc, "hops_batch_settle")
+            self._pending = False
 
     def reset(self):
         rc = _lib.lib().hops_batch_reset(C.byref(self.st.cstruct), C.byref(self.cb), _stream(self.dev))
         _lib.check(rc, "hops_batch_reset")
+        self._pending = False
 
     def set_noise(self, noise1, noise2=None):
         """noise tensors [B, L, n_t] complex64 on the device (noise2 may be None)."""
@@ -111,6 +135,7 @@ class StreamBatch:
         self.reset()
 
     def get_state(self):
+        self.settle()
         ph = self.phi.permute(2, 0, 1).reshape(self.B, self.N * self.S).to(torch.complex128)
         return ph.cpu().numpy(), self.zmem[:, :self.M].cpu().numpy()
 
@@ -137,6 +162,7 @@ class StreamBatch:
             self.tuning = _TUNE_CACHE[key]
             return self.tuning
         L = _lib.lib()
+        pending = self._pending
         saved = [t.clone() for t in (self.phi, self.zmem, self.work, self.status)]
         if self.phi_lo is not None:
             saved.append(self.phi_lo.clone())
@@ -158,6 +184,7 @@ class StreamBatch:
             for dst, src in zip((self.phi, self.zmem, self.work, self.status, self.phi_lo), saved):
                 dst.copy_(src)
         L.hops_stage_tuning(0, -1)
+        self._pending = pending
         _TUNE_CACHE[key] = best
         self.tuning = best
         return best
@@ -172,6 +199,8 @@ class StreamBatch:
         rc = L.hops_rk4_propagate(C.byref(self.st.cstruct), C.byref(self.cb), int(it0), int(di),
                                   int(n_steps), float(tau_over_hbar), ptr, _stream(self.dev))
         _lib.check(rc, "hops_rk4_propagate")
+        if n_steps > 0 and self.cb.defer_scale:
+            self._pending = True
 
     def check_status(self):
         st = self.status.cpu().numpy()

@@ -47,6 +47,9 @@ class HopsEnsemble:
                                                        self.device)
         self.batch = StreamBatch(self.dstruct, self.B, precision,
                                  self.eom_param["EQUATION_OF_MOTION"])
+        # renormalisation after each call left pending and applied by the next
+        # call (or by state()): a call per step costs no extra pass over phi
+        self.batch.defer_scale = True
         self.t = 0.0
         self.noise = None
         self.autotune = autotune

@@ -123,6 +123,48 @@ def test_stage_kernel_shapes_agree(cuda_device, name, B, tuning):
     assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref))
 
 
+@pytest.mark.parametrize("precision", ["complex128", "mixed"])
+def test_deferred_renormalisation_one_call_per_step(cuda_device, precision):
+    """HopsEnsemble leaves each call's last renormalisation pending (hops_batch
+    defer_scale) and the next call applies it on the fly, as the steps within
+    a call do: twelve one-step calls give the psi(t), state and z_mem of one
+    twelve-step call bit for bit, and the path that rescales the state on
+    return agrees to the rounding of its precision."""
+    import torch
+    from mesohops_b200 import HopsEnsemble
+    f = load_golden("ring6")
+    B, n = 40, 12
+    noise = ensemble_noise(f, B, 9)
+    psi_one, ens_one = run_ensemble(f, B, precision, noise, n)
+    phi_one, z_one = ens_one.state()
+    dt = float(f["dt"])
+    out = {}
+    for defer in (True, False):
+        ens = HopsEnsemble(golden_system(f), B,
+                           noise_param={"SEED": noise, "MODEL": "PRE_CALCULATED",
+                                        "TLEN": float(f["tlen"]), "TAU": float(f["tau_noise"])},
+                           hierarchy_param={"MAXHIER": int(f["depth"])}, precision=precision)
+        ens.batch.defer_scale = defer
+        ens.initialize(f["psi0"])
+        psi = torch.empty((n, B, ens.n_state), dtype=torch.complex128, device="cuda")
+        for k in range(n):
+            ens.propagate(dt, dt, psi_out=psi[k:k + 1])
+        assert ens.batch._pending == defer
+        phi, z = ens.state()
+        assert not ens.batch._pending
+        ens.check()
+        out[defer] = (psi.cpu().numpy(), phi, z)
+    psi_d, phi_d, z_d = out[True]
+    assert np.array_equal(psi_d, psi_one)
+    assert np.array_equal(phi_d, phi_one) and np.array_equal(z_d, z_one)
+    # rescaling on return rounds differently: at complex128, or (mixed) where
+    # the complex64 copy of the state is taken from the rescaled state
+    tol = 1e-12 if precision == "complex128" else 1e-6
+    psi_e, phi_e, _ = out[False]
+    assert np.max(np.abs(psi_e - psi_one)) <= tol * np.max(np.abs(psi_one))
+    assert np.max(np.abs(phi_e - phi_one)) <= tol * np.max(np.abs(phi_one))
+
+
 def test_c_abi_rejects_bad_propagation_arguments(cuda_device):
     """hops_rk4_propagate refuses a noise window past the noise axis and negative
     step / index arguments with HOPS_EINVAL and an error text, launching nothing:
