@@ -109,9 +109,9 @@ class Basis:
         return {r.tobytes() for r in rows} == self._row_set
 
 
-# Parts of a basis that depend only on its states and modes, shared by every
-# basis (of any trajectory of the same system) with the same two lists: an
-# adaptive basis usually changes its aux list while its states stay.
+# Parts of a basis that depend only on its states and modes, cached on the
+# HopsSystem object for every basis with the same two lists: an adaptive basis
+# usually changes its aux list while its states stay.
 _PART_CACHE_SIZE = 512
 
 
@@ -377,10 +377,12 @@ class AdaptiveHops:
         self.precision = traj.device_param["PRECISION"]
         self.kernel_request = traj.device_param.get("KERNEL", "auto")
         self.prec_bytes = 16 if self.precision in ("complex128", "c128", "mixed") else 8
-        self.Hd = self.system.hamiltonian_dense()
-        Hoff = self.Hd - np.diag(np.diag(self.Hd))
-        # column norms of the off-diagonal H (error_sflux_stable_state)
+        Hd = self.system.hamiltonian_dense()
+        Hoff = Hd - np.diag(np.diag(Hd))
+        # column norms of the off-diagonal H (error_sflux_stable_state); the
+        # couplings to states outside a basis come from the basis's own block
         self.h_col_norm2 = np.sum(np.abs(Hoff) ** 2, axis=0)
+        del Hd, Hoff
         self.W = self.system.W
         self.G = self.system.G
         self.early_counter = 0
