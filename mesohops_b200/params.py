@@ -97,7 +97,8 @@ STORAGE_DICT_DEFAULT = {
 # Options of this implementation; kept in a separate dictionary so that the
 # reference dictionaries above stay exactly as MesoHOPS defines them.
 DEVICE_DICT_DEFAULT = {
-    "PRECISION": "complex128",   # or "complex64" (FP64 kept for <L>, norm, z_mem)
+    "PRECISION": "complex128",   # or "mixed" (complex128 state, complex64 stage vectors)
+                                 # or "complex64"; FP64 kept for <L>, norm, z_mem
     "DEVICE": "cuda:0",
     "KERNEL": "auto",            # "auto", "resident" or "streaming"
 }
