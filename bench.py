@@ -193,7 +193,9 @@ def run_gpu(args):
     result = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
               "steps": K, "warmup": W, "ms_per_step": round(ms / K, 4),
               "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-              "dtype": {"mixed": "c64", "complex64": "c64", "complex128": "c128"}[args.precision],
+              # mixed: complex128 state and FP64 arithmetic, complex64 stage vectors
+              "dtype": {"mixed": "c128/c64", "complex64": "c64",
+                        "complex128": "c128"}[args.precision],
               "data": "synthetic (seeded)",
               "gpu_launches": launches}
     t = ens.dstruct.tables
