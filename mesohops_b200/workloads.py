@@ -61,6 +61,12 @@ def chain(n, J, eps, lam, gam, temp=295.0):
     return site_system(H, [(lam, gam, temp)])
 
 
+def chain_sites(n):
+    """n-site chain, J = 50 cm^-1, eps ~ N(0, 100) from seed 5, one DL mode
+    (50, 50, 295 K) per site."""
+    return chain(n, 50.0, np.random.default_rng(5).normal(0, 100, n), 50.0, 50.0)
+
+
 WORKLOADS = {
     "ring20": dict(system=ring20, depth=4, n_traj=128, dt=4.0, n_steps=250,
                    desc="20-site ring (J=80 cm^-1, eps~U(-100,100) seed 2), one Drude-Lorentz "
@@ -71,6 +77,11 @@ WORKLOADS = {
                     desc="10-site chain (J=100 cm^-1, eps~N(0,50) seed 1), two DL modes per "
                          "site (35,50)+(10,500) cm^-1 at 300 K, depth 6 (230230 aux x 10 "
                          "states), 256 trajectories (seeds 0..255), dt=2 fs"),
+    "chain120": dict(system=lambda: chain_sites(120), depth=3, n_traj=1, dt=4.0, n_steps=250,
+                     desc="120-site chain (J=50 cm^-1, eps~N(0,100) seed 5), DL (50,50,295 K) "
+                          "per site, depth 3 (302621 aux x 120 states), one trajectory, "
+                          "dt=4 fs: a single large trajectory like the served stream's "
+                          "streaming requests"),
     "dimer": dict(system=dimer, depth=4, n_traj=1, dt=4.0, n_steps=250,
                   desc="2-site dimer H=[[0,50],[50,0]], DL (50,50,295 K) per site, depth 4 "
                        "(15 aux x 2 states), one trajectory, dt=4 fs, 1000 fs"),
