@@ -312,7 +312,6 @@ def extras(args, wl, sysp, ens, dev, value, K):
     adaptive batch."""
     import torch
     from mesohops_b200.ensemble import HopsEnsemble
-    from mesohops_b200.constants import hbar
     out = {}
     B, dt, depth = wl["n_traj"], wl["dt"], wl["depth"]
     tlen = ens.noise_param["TLEN"]
