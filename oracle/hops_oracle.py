@@ -17,7 +17,6 @@ by running the unmodified reference (``tests/golden/make_golden.py``).
 from __future__ import annotations
 
 import itertools
-from collections import Counter
 
 import numpy as np
 import scipy.sparse as sps

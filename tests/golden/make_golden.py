@@ -33,7 +33,6 @@ sys.path.insert(0, REF_SRC)
 from mesohops.trajectory.hops_trajectory import HopsTrajectory  # noqa: E402
 from mesohops.trajectory.exp_noise import bcf_exp  # noqa: E402
 from mesohops.util.bath_corr_functions import bcf_convert_dl_to_exp  # noqa: E402
-from mesohops.util.physical_constants import hbar  # noqa: E402
 
 
 def quiet(fn, *a, **k):

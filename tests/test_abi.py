@@ -4,8 +4,6 @@ import ctypes
 import os
 import re
 
-import pytest
-
 from conftest import ROOT
 
 HEADER = os.path.join(ROOT, "include", "hops_b200.h")

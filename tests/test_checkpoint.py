@@ -1,7 +1,6 @@
 """save_checkpoint / load_checkpoint (trajectory/hops_trajectory.py:853-1034):
 a run interrupted by a checkpoint and resumed from the file must continue as
 if it had not been interrupted."""
-import os
 
 import numpy as np
 import pytest
