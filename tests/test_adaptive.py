@@ -235,3 +235,27 @@ def test_flux_errors_kernel_vs_oracle(name, tmp_path):
         assert np.max(np.abs(ed - od)) <= 1e-11 * scale
         assert np.allclose(eu, ou, rtol=1e-12, atol=1e-300)
         assert np.allclose(edn, odn, rtol=1e-12, atol=1e-300)
+
+
+def test_state_mode_part_is_cached_and_read_only():
+    """The state/mode-dependent part of an adaptive basis (tables, L blocks,
+    M2 diagonal, the H couplings to states outside the basis) is built once per
+    (states, modes) pair of a system, is read-only, and its coupling block is
+    -i H[outside, basis]."""
+    from mesohops_b200.system import HopsSystem
+    from mesohops_b200.workloads import chain_sites
+    sysp = chain_sites(12)
+    system = HopsSystem(sysp)
+    states = np.array([3, 4, 5], dtype=np.int64)
+    modes = np.array([3, 4, 5], dtype=np.int64)
+    p1 = ad._state_mode_part(system, states, modes)
+    p2 = ad._state_mode_part(system, states.copy(), modes.copy())
+    assert p1 is p2
+    assert p1 is not ad._state_mode_part(system, np.array([3, 4], dtype=np.int64),
+                                         np.array([3, 4], dtype=np.int64))
+    assert p1["list_sc"].tolist() == [2, 6]
+    H = np.asarray(sysp["HAMILTONIAN"])
+    assert np.array_equal(p1["h_sc"], -1j * H[np.ix_([2, 6], states)])
+    for arr in [p1["m2"], p1["list_sc"], p1["h_sc"]] + p1["lred"]:
+        with pytest.raises(ValueError):
+            arr[(0,) * arr.ndim] = 1
