@@ -352,9 +352,12 @@ def main_ltc_adaptive():
 
 
 def run_adaptive(name, sysp, depth, psi0, t_max, dt, delta_a, delta_s, noise_seed,
-                 update_step=1, f_discard=0.0, extra=None, tau_noise=None, integration=None):
+                 update_step=1, f_discard=0.0, extra=None, tau_noise=None, integration=None,
+                 site_map=None):
     """Adaptive propagation with PRE_CALCULATED noise; records the basis per step.
-    tau_noise: noise time step (default dt / 2); integration: integration_param."""
+    tau_noise: noise time step (default dt / 2); integration: integration_param;
+    site_map: for site-projector systems too large for dense L storage, the
+    site of each mode's L = |site><site| is stored instead of L."""
     tau_noise = dt / 2.0 if tau_noise is None else tau_noise
     tlen = t_max + dt
     n_t = int(np.ceil(tlen / tau_noise)) + 1
@@ -398,7 +401,8 @@ def run_adaptive(name, sysp, depth, psi0, t_max, dt, delta_a, delta_s, noise_see
     np.savez_compressed(
         os.path.join(HERE, name + ".npz"),
         H=np.array(H, dtype=np.complex128), G=np.array([g for g, w in sysp["GW_SYSBATH"]]),
-        W=np.array([w for g, w in sysp["GW_SYSBATH"]]), L=dense_lops(sysp), depth=depth,
+        W=np.array([w for g, w in sysp["GW_SYSBATH"]]), depth=depth,
+        **({"L": dense_lops(sysp)} if site_map is None else {"L_site": np.asarray(site_map)}),
         psi0=np.array(psi0, dtype=np.complex128), t_max=t_max, dt=dt, tau_noise=tau_noise,
         tlen=tlen, noise1=noise, delta_a=delta_a, delta_s=delta_s, update_step=update_step,
         f_discard=f_discard, psi_traj=psi_full, t_axis=np.array(d["t_axis"]),
@@ -528,6 +532,24 @@ def main_effective_adaptive():
                  3e-4, 3e-4, noise_seed=35, tau_noise=0.5, integration=eff)
 
 
+def main_adaptive_chain500():
+    """The adaptive batch workload of the benchmark: 500-site chain (J = 50,
+    eps ~ N(0, 100) and psi_0's site from default_rng(3)), one DL mode
+    (50, 50, 295 K) per site, depth 10, delta_a = delta_s = 1e-3, 20 steps of
+    4 fs, with seeded PRE_CALCULATED noise."""
+    n = 500
+    rng = np.random.default_rng(3)
+    eps = rng.normal(0, 100, n)
+    start = int(rng.integers(0, n))
+    H = np.diag(eps)
+    for i in range(n - 1):
+        H[i, i + 1] = H[i + 1, i] = 50.0
+    psi0 = np.zeros(n, dtype=np.complex128)
+    psi0[start] = 1.0
+    run_adaptive("adaptive_chain500", site_system(H, [(50, 50, 295)]), 10, psi0, 80.0, 4.0,
+                 1e-3, 1e-3, noise_seed=37, site_map=np.arange(n))
+
+
 def main_dyadic():
     run_dyadic("dyadic_norm_dense", "NORMALIZED NONLINEAR", False, noise_seed=51)
     run_dyadic("dyadic_linear_sparse", "LINEAR", True, noise_seed=52)
@@ -540,6 +562,8 @@ if __name__ == "__main__":
         main_dyadic()
     elif "--effective-adaptive" in sys.argv:
         main_effective_adaptive()
+    elif "--adaptive-chain500" in sys.argv:
+        main_adaptive_chain500()
     elif "--adaptive" in sys.argv:
         main_adaptive()
     elif "--effective" in sys.argv:

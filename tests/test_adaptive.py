@@ -17,6 +17,7 @@ import os
 
 import numpy as np
 import pytest
+import scipy.sparse as sps
 
 import mesohops_b200.adaptive as ad
 from mesohops_b200 import HopsTrajectory
@@ -26,6 +27,9 @@ from oracle import hops_oracle as O
 HERE = os.path.dirname(os.path.abspath(__file__))
 CASES = ["adaptive_dod_full", "adaptive_chain8", "adaptive_chain12", "adaptive_chain8_ltc",
          "adaptive_chain8_eff"]
+# the benchmark's 500-site chain at depth 10 (aux keys beyond int64): the oracle
+# would need its 500 dense L-operators, so only the GPU run is compared
+GPU_ONLY_CASES = ["adaptive_chain500"]
 
 
 def load(name):
@@ -34,7 +38,11 @@ def load(name):
 
 def system_param(f):
     gw = [(complex(g), complex(w)) for g, w in zip(f["G"], f["W"])]
-    lops = [np.array(l) for l in f["L"]]
+    if "L" in f:
+        lops = [np.array(l) for l in f["L"]]
+    else:   # site projectors stored as each mode's site (systems too large for dense L)
+        n = f["H"].shape[0]
+        lops = [sps.coo_matrix(([1.0], ([int(i)], [int(i)])), shape=(n, n)) for i in f["L_site"]]
     sysp = {"HAMILTONIAN": np.array(f["H"]), "GW_SYSBATH": gw, "L_HIER": lops,
             "L_NOISE1": lops, "ALPHA_NOISE1": O.bcf_exp, "PARAM_NOISE1": gw}
     if "LT_L" in f:   # low-temperature corrections
@@ -201,7 +209,7 @@ def test_make_adaptive_validates_f_discard():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name", CASES + GPU_ONLY_CASES)
 def test_adaptive_gpu_matches_reference(name, tmp_path):
     f = load(name)
     hops = make_traj(f, tmp_path, "cuda:0")
@@ -259,3 +267,34 @@ def test_state_mode_part_is_cached_and_read_only():
     for arr in [p1["m2"], p1["list_sc"], p1["h_sc"]] + p1["lred"]:
         with pytest.raises(ValueError):
             arr[(0,) * arr.ndim] = 1
+
+
+def test_chain500_reference_aux_sets_in_byte_key_order():
+    """The reference's aux lists of the 500-site, depth-10 run (ranks beyond
+    int64, so byte sort keys) are ordered by the same keys as the exact ranks,
+    and every aux's k+1 / k-1 neighbours inside the set are found."""
+    from mesohops_b200.hierarchy import AuxBasis, AuxKeyer
+    f = load("adaptive_chain500")
+    keyer = AuxKeyer(500, int(f["depth"]))
+    assert not keyer.use_int64
+    ptr, counts = f["aux_ptr"], f["aux_counts"]
+    for i in range(len(ptr) - 1):
+        c = counts[ptr[i]:ptr[i + 1]]
+        b = AuxBasis(c, keyer, int(f["depth"]))
+        exact = [int(x) for x in keyer.keys_from_counts(b.counts)]
+        assert exact == sorted(exact) and len(set(exact)) == len(exact)
+        rows = {r.tobytes(): j for j, r in enumerate(b.counts)}
+        for a, u, m in zip(b.up_a, b.up_u, b.up_m):
+            v = b.counts[a].copy()
+            v[b.modes[m]] += 1
+            assert rows[v.tobytes()] == u
+        n_up = sum(1 for j, r in enumerate(b.counts) for m in range(len(b.modes))
+                   if r.sum() < int(f["depth"])
+                   and _plus(r, b.modes[m]).tobytes() in rows)
+        assert n_up == len(b.up_a)
+
+
+def _plus(r, m):
+    v = r.copy()
+    v[m] += 1
+    return v
