@@ -485,8 +485,9 @@ def adaptive_leg(args, dev):
 
 # ------------------------------------------------------------- CPU legs --
 def _oracle_worker(args):
-    """One trajectory of the oracle for n_steps steps (single thread)."""
-    wl_name, seed, n_steps = args
+    """One trajectory of the oracle: n_warm untimed steps, then n_steps timed
+    steps from the same start (single thread)."""
+    wl_name, seed, n_steps, n_warm = args
     os.environ["OMP_NUM_THREADS"] = "1"
     from threadpoolctl import threadpool_limits
     from oracle import hops_oracle as O
@@ -496,12 +497,14 @@ def _oracle_worker(args):
     dt = wl["dt"]
     with threadpool_limits(1):
         b = O.OracleBasis(sysp, wl["depth"])
-        n_t = int(np.ceil((n_steps + 2) * dt / (dt / 2))) + 1
+        n_t = int(np.ceil((max(n_steps, n_warm) + 2) * dt / (dt / 2))) + 1
         rng = np.random.default_rng(seed)
         noise = ((rng.normal(size=(b.sys["L"].__len__(), n_t))
                   + 1j * rng.normal(size=(len(b.sys["L"]), n_t))) * 40).astype(np.complex64)
         psi0 = np.zeros(b.nstate, dtype=complex)
         psi0[0] = 1.0
+        if n_warm > 0:
+            O.propagate(b, psi0, noise, dt / 2, n_warm * dt, dt)
         t0 = time.perf_counter()
         O.propagate(b, psi0, noise, dt / 2, n_steps * dt, dt)
         return time.perf_counter() - t0
@@ -511,7 +514,7 @@ def cpu_baseline(wl, sysp, n_steps=4):
     """The oracle port (numpy, one thread) on one trajectory, n_steps steps."""
     name = [k for k, v in __import__("mesohops_b200.workloads", fromlist=["x"]).WORKLOADS.items()
             if v is wl][0]
-    el = _oracle_worker((name, 0, n_steps))
+    el = _oracle_worker((name, 0, n_steps, 1))
     return {"value": round(n_steps / el, 3), "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"1 trajectory x {n_steps} RK4 steps of the same system with the numpy "
                       "oracle (single thread)"}
@@ -528,14 +531,16 @@ def run_reference(args):
     wl = WORKLOADS[args.workload]
     cores = os.cpu_count() or 1
     K = max(1, min(args.steps, 3))
+    W = max(0, args.warmup)
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
-        # each worker builds its basis outside its own timed region; the workers
-        # run concurrently, so the wall time of the step loop is the slowest one
-        el = max(pool.map(_oracle_worker, [(args.workload, s, K) for s in range(cores)]))
+        # each worker builds its basis and runs its warm-up steps outside its
+        # own timed region; the workers run concurrently, so the wall time of
+        # the step loop is the slowest one
+        el = max(pool.map(_oracle_worker, [(args.workload, s, K, W) for s in range(cores)]))
     v = cores * K / el
     line = {"metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": world,
-            "steps": K, "warmup": 1, "ms_per_step": round(el / K * 1e3, 2),
+            "steps": K, "warmup": W, "ms_per_step": round(el / K * 1e3, 2),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "c128", "data": "synthetic (seeded)", "impl": "reference",
             "config": {"workload": wl["desc"] + f"; {cores} trajectories, one per host core"},
