@@ -517,7 +517,7 @@ def cpu_baseline(wl, sysp, n_steps=4):
     el = _oracle_worker((name, 0, n_steps, 1))
     return {"value": round(n_steps / el, 3), "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"1 trajectory x {n_steps} RK4 steps of the same system with the numpy "
-                      "oracle (single thread)"}
+                      "oracle (single thread, after 1 untimed step)"}
 
 
 def run_reference(args):
@@ -545,8 +545,9 @@ def run_reference(args):
             "dtype": "c128", "data": "synthetic (seeded)", "impl": "reference",
             "config": {"workload": wl["desc"] + f"; {cores} trajectories, one per host core"},
             "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{cores} trajectories x {K} RK4 steps (numpy oracle, "
-                                       "one process per core, one thread each)"},
+                             "sample": f"{cores} trajectories x {K} RK4 steps after {W} "
+                                       "untimed ones (numpy oracle, one process per core, "
+                                       "one thread each)"},
             "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
