@@ -5,6 +5,13 @@
 #include <stdint.h>
 #include "../../include/hops_b200.h"
 
+// Host helpers shared by the library's translation units (not part of the C ABI).
+// hops_set_error_text: replace the calling thread's last-error text.
+// hops_check_propagate_args: every argument check of hops_rk4_propagate.
+void hops_set_error_text(const char* msg);
+int hops_check_propagate_args(const hops_structure* st, const hops_batch* bt, int32_t it0,
+                              int32_t di, int32_t n_steps);
+
 namespace hops {
 
 // ---------------------------------------------------------------- complex ----
@@ -93,6 +100,28 @@ struct ScalarLayout {
   __host__ __device__ int upc_f() const { return 4 + 6 * L + 6 * M + 4 * S; }   // M float2
   __host__ __device__ int diagD_f() const { return 4 + 6 * L + 7 * M + 4 * S; } // S float2
   __host__ __device__ int phys_f() const { return 4 + 6 * L + 7 * M + 5 * S; }  // S float2
+};
+
+// Workspace of a batch: B per-trajectory ScalarLayout blocks followed by the
+// stage coefficients in trajectory-fastest layout ([m][b], [s][b], [j][b]) so
+// that the stage kernel reads them coalesced.
+struct BatchLayout {
+  size_t upcT, upcT_f, diagT, diagT_f, czT, czT_f, ncB, scaleB, physT, physT_f, total;  // doubles
+  __host__ __device__ static size_t even(size_t x) { return (x + 1) & ~(size_t)1; }
+  __host__ __device__ BatchLayout(int S, int M, int L, int B) {
+    const ScalarLayout lay(S, M, L);
+    upcT = even((size_t)lay.stride * B);
+    upcT_f = upcT + 2 * (size_t)M * B;
+    diagT = even(upcT_f + (size_t)M * B);
+    diagT_f = diagT + 2 * (size_t)S * B;
+    czT = even(diagT_f + (size_t)S * B);
+    czT_f = czT + 2 * (size_t)L * B;
+    ncB = even(czT_f + (size_t)L * B);
+    scaleB = ncB + B;
+    physT = even(scaleB + B);            // LT term of aux 0, [s][b] complex
+    physT_f = physT + 2 * (size_t)S * B;
+    total = even(physT_f + (size_t)S * B);
+  }
 };
 
 // Stage constants of classic RK4 (integrator_rk.py:29-30).

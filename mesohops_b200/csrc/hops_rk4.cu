@@ -7,7 +7,6 @@
 #include <string.h>
 #include <stdarg.h>
 #include <algorithm>
-#include <mutex>
 #include <vector>
 #include "hops_common.cuh"
 
@@ -78,28 +77,6 @@ template <> struct Prec<float> {
   static __device__ __forceinline__ T hdiag(const hops_structure& st, int s) {
     const double2 v = ld2(st.h_diag, s);
     return mkf((float)v.x, (float)v.y);
-  }
-};
-
-// Workspace of a batch: B per-trajectory ScalarLayout blocks followed by the
-// stage coefficients in trajectory-fastest layout ([m][b], [s][b], [j][b]) so
-// that the stage kernel reads them coalesced.
-struct BatchLayout {
-  size_t upcT, upcT_f, diagT, diagT_f, czT, czT_f, ncB, scaleB, physT, physT_f, total;  // doubles
-  __host__ __device__ static size_t even(size_t x) { return (x + 1) & ~(size_t)1; }
-  __host__ __device__ BatchLayout(int S, int M, int L, int B) {
-    const ScalarLayout lay(S, M, L);
-    upcT = even((size_t)lay.stride * B);
-    upcT_f = upcT + 2 * (size_t)M * B;
-    diagT = even(upcT_f + (size_t)M * B);
-    diagT_f = diagT + 2 * (size_t)S * B;
-    czT = even(diagT_f + (size_t)S * B);
-    czT_f = czT + 2 * (size_t)L * B;
-    ncB = even(czT_f + (size_t)L * B);
-    scaleB = ncB + B;
-    physT = even(scaleB + B);            // LT term of aux 0, [s][b] complex
-    physT_f = physT + 2 * (size_t)S * B;
-    total = even(physT_f + (size_t)S * B);
   }
 };
 
@@ -1219,9 +1196,10 @@ extern "C" int hops_batch_settle(const hops_structure* st, hops_batch* bt, void*
   return HOPS_OK;
 }
 
-extern "C" int hops_rk4_propagate(const hops_structure* st, hops_batch* bt, int32_t it0,
-                                  int32_t di, int32_t n_steps, double tau_over_hbar,
-                                  double* psi_out_dev, void* stream) {
+// Every argument check of hops_rk4_propagate, done before anything is
+// launched (also used by the no-allocation entry point).
+int hops_check_propagate_args(const hops_structure* st, const hops_batch* bt, int32_t it0,
+                              int32_t di, int32_t n_steps) {
   int rc = check_structure(st);
   if (rc) return rc;
   if ((rc = check_batch(st, bt))) return rc;
@@ -1232,6 +1210,14 @@ extern "C" int hops_rk4_propagate(const hops_structure* st, hops_batch* bt, int3
   if (n_steps > 0 && bt->noise2 && last >= bt->n_t2)
     return set_err(HOPS_EINVAL, "noise 2 too short: needs index %ld, has %d samples", last, bt->n_t2);
   if (scalar_smem(st) > 48 * 1024) return set_err(HOPS_ENOTSUP, "too many L operators (%d)", st->n_lop);
+  return HOPS_OK;
+}
+
+extern "C" int hops_rk4_propagate(const hops_structure* st, hops_batch* bt, int32_t it0,
+                                  int32_t di, int32_t n_steps, double tau_over_hbar,
+                                  double* psi_out_dev, void* stream) {
+  int rc = hops_check_propagate_args(st, bt, it0, di, n_steps);
+  if (rc) return rc;
   cudaStream_t s = (cudaStream_t)stream;
   if (bt->precision == HOPS_PREC_C128)
     return propagate_impl<double, double2, double2>(st, bt, it0, di, n_steps, tau_over_hbar, psi_out_dev, s);
@@ -1456,120 +1442,4 @@ extern "C" int hops_flux_errors(hops_flux_task* tasks_dev, int32_t n_tasks, int3
   k_flux_errors<<<n_tasks, 256, smem, (cudaStream_t)stream>>>(tasks_dev, hbar);
   LAUNCH_CHECK();
   return HOPS_OK;
-}
-
-// ======================================================= no-allocation path ==
-// Some callers cannot allocate device memory at the point where they step a
-// trajectory: host codes that hand every byte of the GPU to their own memory
-// pool (a cudaMalloc there fails or fragments the pool), and per-step plugin
-// callbacks that must not synchronise the device (cudaMalloc / cudaFree may).
-// hops_rk4_propagate_noalloc serves them: its stage vectors, accumulator,
-// scalar workspace and status words live in the fixed array below, which
-// every GPU that loads this library holds from module load until exit.
-#define HOPS_NOALLOC_MAX_DEVICES 64
-static __device__ __align__(256) unsigned char g_noalloc_scratch[HOPS_NOALLOC_SCRATCH_BYTES];
-static void* g_noalloc_ptr[HOPS_NOALLOC_MAX_DEVICES];
-static std::mutex g_noalloc_mu;
-
-// Host code only holds a host-side stand-in for g_noalloc_scratch; the device
-// address comes from cudaGetSymbolAddress, looked up once per device with that
-// device current (the first call on each device does it).
-static int noalloc_scratch(void** out) {
-  int dev = 0;
-  CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= HOPS_NOALLOC_MAX_DEVICES)
-    return set_err(HOPS_ENOTSUP, "device %d beyond the no-allocation table", dev);
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p)
-      return set_err(HOPS_ECUDA, "cudaGetSymbolAddress(no-allocation scratch): %s",
-                     cudaGetErrorString(e));
-    g_noalloc_ptr[dev] = p;
-  }
-  *out = g_noalloc_ptr[dev];
-  return HOPS_OK;
-}
-
-template <typename T, typename PT>
-__global__ void k_noalloc_shadow(const PT* phi, T* shadow, size_t E) {
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < E;
-       e += (size_t)gridDim.x * blockDim.x)
-    shadow[e] = cv<T>(phi[e]);
-}
-
-extern "C" size_t hops_noalloc_scratch_bytes(const hops_structure* st, int32_t n_traj,
-                                             int32_t precision) {
-  if (!st || n_traj <= 0) return 0;
-  const size_t E = (size_t)st->n_hier * st->n_state * n_traj;
-  const size_t sv = precision == HOPS_PREC_C128 ? 16 : 8;
-  size_t bytes = 3 * E * sv;                          // acc, y0, y1
-  if (precision == HOPS_PREC_MIXED) bytes += E * sv;  // complex64 copy of phi
-  bytes = (bytes + 255) & ~(size_t)255;
-  bytes += BatchLayout(st->n_state, st->n_mode, st->n_lop, n_traj).total * sizeof(double);
-  return bytes;
-}
-
-extern "C" int hops_rk4_propagate_noalloc(const hops_structure* st, int32_t n_traj,
-                                          int32_t precision, int32_t eom, void* phi_dev,
-                                          double* zmem_dev, const float* noise1_dev,
-                                          int32_t n_t1, const float* noise2_dev, int32_t n_t2,
-                                          int32_t it0, int32_t di, int32_t n_steps,
-                                          double tau_over_hbar, double* psi_out_dev,
-                                          int32_t* status_dev, void* stream) {
-  int rc = check_structure(st);
-  if (rc) return rc;
-  if (n_traj <= 0 || !phi_dev || !zmem_dev || !status_dev)
-    return set_err(HOPS_EINVAL, "no-allocation propagate: bad arguments");
-  const size_t need = hops_noalloc_scratch_bytes(st, n_traj, precision);
-  if (need > (size_t)HOPS_NOALLOC_SCRATCH_BYTES)
-    return set_err(HOPS_EINVAL,
-                   "no-allocation propagate needs %zu bytes of scratch, more than its %u-byte "
-                   "static area; use hops_rk4_propagate with caller-allocated buffers",
-                   need, (unsigned)HOPS_NOALLOC_SCRATCH_BYTES);
-  void* base = nullptr;
-  if ((rc = noalloc_scratch(&base))) return rc;
-  const size_t E = (size_t)st->n_hier * st->n_state * n_traj;
-  const size_t sv = precision == HOPS_PREC_C128 ? 16 : 8;
-  unsigned char* p = static_cast<unsigned char*>(base);
-  hops_batch bt;
-  memset(&bt, 0, sizeof(bt));
-  bt.n_traj = n_traj;
-  bt.precision = precision;
-  bt.eom = eom;
-  bt.phi = phi_dev;
-  bt.acc = p;
-  bt.y0 = p + E * sv;
-  bt.y1 = p + 2 * E * sv;
-  size_t off = 3 * E * sv;
-  if (precision == HOPS_PREC_MIXED) {
-    bt.phi_lo = p + off;
-    off += E * sv;
-  }
-  off = (off + 255) & ~(size_t)255;
-  bt.work = reinterpret_cast<double*>(p + off);
-  bt.zmem = zmem_dev;
-  bt.noise1 = noise1_dev;
-  bt.n_t1 = n_t1;
-  bt.noise2 = noise2_dev;
-  bt.n_t2 = n_t2;
-  bt.status = status_dev;
-  if ((rc = check_batch(st, &bt))) return rc;
-  cudaStream_t s = (cudaStream_t)stream;
-  // The array keeps whatever the previous call left: reset the per-trajectory
-  // scale to 1 and the status words to 0, and rebuild the complex64 copy of
-  // phi in the mixed mode.  Everything else is written before it is read.
-  const ScalarLayout lay(st->n_state, st->n_mode, st->n_lop);
-  const BatchLayout bl(st->n_state, st->n_mode, st->n_lop, n_traj);
-  k_reset<<<(n_traj + 127) / 128, 128, 0, s>>>(bt.work, lay.stride, bl.scaleB, n_traj, bt.status, 1);
-  LAUNCH_CHECK();
-  if (precision == HOPS_PREC_MIXED) {
-    long blocks = (long)((E + 255) / 256);
-    if (blocks > (long)sm_count() * 8) blocks = (long)sm_count() * 8;
-    k_noalloc_shadow<float2, double2><<<(int)blocks, 256, 0, s>>>((const double2*)phi_dev,
-                                                                    (float2*)bt.phi_lo, E);
-    LAUNCH_CHECK();
-  }
-  return hops_rk4_propagate(st, &bt, it0, di, n_steps, tau_over_hbar, psi_out_dev, stream);
 }
