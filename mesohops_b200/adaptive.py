@@ -173,7 +173,10 @@ class FluxRequest:
 
 
 def serve_steps(reqs, device):
-    """Run every StepRequest; the resident ones in ONE persistent launch."""
+    """Run every StepRequest; the resident ones in ONE persistent launch.
+
+    A request whose state turned NaN/Inf gets a TrajectoryError instance in
+    place of its result, so the other requests of the launch go on."""
     out = [None] * len(reqs)
     res = [i for i, r in enumerate(reqs) if r.driver.kernel == "resident"]
     if res:
@@ -190,10 +193,9 @@ def serve_steps(reqs, device):
             dis.append(di)
             hs.append(r.tau / hbar)
         st, phis_o, zms_o = ResidentRunner(device).run_packed(trajs, phis, zms, it0s, dis, 1, hs)
-        if np.any(st != 0):
-            raise TrajectoryError("non-finite state during adaptive propagation")
         for j, i in enumerate(res):
-            out[i] = (phis_o[j], zms_o[j])
+            out[i] = ((phis_o[j], zms_o[j]) if st[j] == 0 else
+                      TrajectoryError("non-finite state during adaptive propagation"))
     for i, r in enumerate(reqs):
         if out[i] is not None:
             continue
@@ -204,10 +206,15 @@ def serve_steps(reqs, device):
         eng.set_state(r.phi.reshape(1, -1),
                       r.zmem_abs[b.modes].reshape(1, -1) if b.n_mode else None)
         eng.propagate(it0, di, 1, r.tau / hbar, tuned=False)
-        eng.check_status()
+        try:
+            eng.check_status()
+        except TrajectoryError as exc:
+            out[i] = exc
+            continue
         phi, z = eng.get_state()
         out[i] = (phi[0], z[0])
-    return [r.driver.finish_step(r, phi, zrel) for r, (phi, zrel) in zip(reqs, out)]
+    return [o if isinstance(o, TrajectoryError) else r.driver.finish_step(r, o[0], o[1])
+            for r, o in zip(reqs, out)]
 
 
 def _pack(arrays):
@@ -297,15 +304,23 @@ def drive(gen, device):
             return stop.value
         if isinstance(req, StepRequest):
             result = serve_steps([req], device)[0]
+            if isinstance(result, TrajectoryError):
+                raise result
         else:
             result = serve_flux([req], device)[0]
 
 
-def drive_many(gens, device):
+def drive_many(gens, device, collect_errors=False):
     """Run many coroutines in lock-step: every round serves all pending step
     requests with one launch and all pending flux requests with one launch.
-    Returns the coroutines' return values."""
+    Returns the coroutines' return values.
+
+    A trajectory whose state turns non-finite has the TrajectoryError thrown
+    into its coroutine; the others go on.  collect_errors: the exception (or
+    any other exception of that coroutine) becomes its value; otherwise the
+    first TrajectoryError is raised once the others have finished."""
     values = [None] * len(gens)
+    failed = []
     pending = {}
     for i, g in enumerate(gens):
         try:
@@ -323,10 +338,22 @@ def drive_many(gens, device):
         nxt = {}
         for i, res in served.items():
             try:
-                nxt[i] = gens[i].send(res)
+                if isinstance(res, TrajectoryError):
+                    nxt[i] = gens[i].throw(res)
+                else:
+                    nxt[i] = gens[i].send(res)
             except StopIteration as stop:
                 values[i] = stop.value
+            except Exception as exc:
+                # collect_errors: any failure of one trajectory's host logic
+                # ends that trajectory only
+                if not (collect_errors or isinstance(exc, TrajectoryError)):
+                    raise
+                values[i] = exc
+                failed.append(exc)
         pending = nxt
+    if failed and not collect_errors:
+        raise failed[0]
     return values
 
 

@@ -69,12 +69,16 @@ def _worker(conn, device, precision):
                         break
                     gens = [v[0].adaptive_step_gen((v[2] + 1) * v[1].dt, v[1].dt, v[2])
                             for _, v in act]
-                    ad.drive_many(gens, device)
-                    for _, v in act:
-                        v[2] += 1
+                    vals = ad.drive_many(gens, device, collect_errors=True)
+                    for (k, v), val in zip(act, vals):
+                        if isinstance(val, Exception):   # this trajectory only
+                            errors.append((k, f"{type(val).__name__}: {val}"))
+                            live.pop(k)
+                        else:
+                            v[2] += 1
             except Exception as exc:
                 tb = traceback.format_exc(limit=3)
-                errors = [(k, f"{type(exc).__name__}: {exc} {tb}") for k in list(live)]
+                errors += [(k, f"{type(exc).__name__}: {exc} {tb}") for k in list(live)]
                 live.clear()
             for k in [k for k, v in live.items() if v[2] >= v[1].n_steps]:
                 h, req, _ = live.pop(k)

@@ -193,6 +193,7 @@ class _Active:
         self.done = 0
         self.psi_dev = None
         self.stream = None
+        self.failed = None      # error text once the request's state went non-finite
 
 
 class HopsServer:
@@ -356,7 +357,12 @@ class HopsServer:
                 n_ticks += 1
                 keep = []
                 for a in active:
-                    if a.done >= a.req.n_steps:
+                    if a.failed is not None:      # this request only; the others go on
+                        results[a.req.rid] = ServedResult(a.req, "error", a.failed,
+                                                          footprint=a.fp)
+                        a.traj = a.psi_dev = None
+                        used -= a.fp
+                    elif a.done >= a.req.n_steps:
                         results[a.req.rid] = self._retire(a, clock())
                         used -= a.fp
                     else:
@@ -431,20 +437,25 @@ class HopsServer:
             n = min(self.chunk, max(a.req.n_steps - a.done for a in ada))
             with torch.cuda.stream(s_ad):
                 for k in range(n):
-                    live = [a for a in ada if a.done + k < a.req.n_steps]
+                    live = [a for a in ada if a.done + k < a.req.n_steps and a.failed is None]
                     gens = [a.traj.adaptive_step_gen((a.done + k + 1) * a.req.dt, a.req.dt,
                                                      a.done + k) for a in live]
-                    _adaptive.drive_many(gens, self.device)
+                    vals = _adaptive.drive_many(gens, self.device, collect_errors=True)
+                    for a, v in zip(live, vals):
+                        if isinstance(v, Exception):
+                            a.failed = f"{type(v).__name__}: {v}"
             for a in ada:
                 plan[id(a)] = min(n, a.req.n_steps - a.done)
         if handle is not None:
             st = runner.collect(handle)
-            if np.any(st != 0):
-                bad = [res[i].req.rid for i in np.nonzero(st)[0]]
-                raise TrajectoryError(f"non-finite state in requests {bad}")
+            for i in np.nonzero(st)[0]:
+                res[i].failed = "TrajectoryError: non-finite state during propagation"
         for a in stm:
             a.stream.synchronize()
-            a.traj._traj.check_status()
+            try:
+                a.traj._traj.check_status()
+            except TrajectoryError as exc:
+                a.failed = f"TrajectoryError: {exc}"
         for a in active:
             a.done += plan.get(id(a), 0)
 
