@@ -324,6 +324,79 @@ int hops_stage_tuning(int32_t nb, int32_t chunk_major);
 int hops_kernel_timing(int enable);
 int hops_kernel_timing_read(double* total_ms, int64_t* n_launches);
 
+/* ===================================================== host-array entry points
+ * For callers that hold only host arrays (any language with a C FFI): the
+ * library derives every table of hops_structure from a minimal description,
+ * owns the device memory of structures and batches, and moves states, noise
+ * and psi(t) between host buffers and the device.  These replace, for such a
+ * caller, the reference's construction of the super-operators
+ * (eom/hops_eom.py:118-218 through eom/eom_hops_ksuper.py:36-230) and the
+ * state I/O of trajectory/hops_trajectory.py:253-336 (initialize) and
+ * :1072-1125 (phi, psi, z_mem read-outs).
+ */
+
+/* Minimal description of one basis; all pointers are HOST pointers, complex
+ * numbers interleaved (re, im) doubles.  Aux 0 must be the zero vector (the
+ * physical wavefunction); the first-level aux, K2_k = -sum_m k_m(a) w_m and the
+ * site-projector form are derived from the connection lists and L. */
+typedef struct hops_structure_desc {
+  int32_t n_hier, n_state, n_mode, n_lop;
+  const int32_t* up_ptr;  /* [n_hier+1] CSR over aux of the k+1 connections */
+  const int32_t* up_aux;  /* [up_ptr[n_hier]] aux a + e_m */
+  const int32_t* up_mode; /* mode m (index into the mode arrays) */
+  const int32_t* dn_ptr;  /* [n_hier+1] CSR over aux of the k-1 connections */
+  const int32_t* dn_aux;  /* [dn_ptr[n_hier]] aux a - e_m */
+  const int32_t* dn_mode; /* mode m */
+  const int32_t* dn_k;    /* k_m(a) >= 1, the depth of aux a in mode m */
+  const int32_t* mode_lop;  /* [n_mode] index of the mode's L operator */
+  const double* mode_g;     /* [n_mode] complex g_m */
+  const double* mode_w;     /* [n_mode] complex w_m (nonzero) */
+  const double* lops;       /* [n_lop][n_state][n_state] complex, dense, row-major */
+  const double* hamiltonian; /* [n_state][n_state] complex, dense, row-major */
+  const double* lt_coef;    /* [n_lop] complex low-temperature coefficients, or NULL */
+} hops_structure_desc;
+
+typedef struct hops_structure_owned hops_structure_owned;  /* opaque */
+
+/* Derive and upload every table (one device allocation owned by the library;
+ * returns after the copy has completed).  Inputs are validated (sizes, index
+ * ranges, w != 0, aux 0 without down connections) before anything is
+ * allocated. */
+int hops_structure_upload(const hops_structure_desc* desc, void* stream,
+                          hops_structure_owned** out);
+/* The structure as the entry points above take it: a host struct of device
+ * pointers (hops_rk4_propagate, hops_dsystem_dt, ...) or its device copy
+ * (hops_task.st, hops_flux_task.st).  Valid until hops_structure_destroy. */
+const hops_structure* hops_structure_host_view(const hops_structure_owned* s);
+const hops_structure* hops_structure_device_view(const hops_structure_owned* s);
+int hops_structure_destroy(hops_structure_owned* s);
+
+/* A batch of n_traj trajectories whose buffers the library allocates (and
+ * frees in hops_batch_destroy); status words start at 0. */
+int hops_batch_create(const hops_structure* st, int32_t n_traj, int32_t precision, int32_t eom,
+                      hops_batch** out);
+int hops_batch_destroy(hops_batch* bt);
+/* phi_host: [n_traj][n_hier*n_state] complex128 in the reference's flat order
+ * (aux-major, hops_trajectory.py:316-320); zmem_host: [n_traj][n_mode] complex128
+ * or NULL for zero memory.  Resets the pending scale and the status words;
+ * returns once the host buffers may be reused. */
+int hops_batch_set_state_host(const hops_structure* st, hops_batch* bt, const double* phi_host,
+                              const double* zmem_host, void* stream);
+/* noise: [n_traj][n_lop][n_t] complex64 per noise (noise2_host may be NULL);
+ * copied into batch-owned device memory. */
+int hops_batch_set_noise_host(hops_batch* bt, const float* noise1_host, int32_t n_t1,
+                              const float* noise2_host, int32_t n_t2, void* stream);
+/* hops_rk4_propagate with psi(t) delivered to psi_out_host ([n_steps][n_traj]
+ * [n_state] complex128, or NULL) and the status words to status_host ([n_traj],
+ * or NULL); returns after both copies completed. */
+int hops_batch_propagate_host(const hops_structure* st, hops_batch* bt, int32_t it0, int32_t di,
+                              int32_t n_steps, double tau_over_hbar, double* psi_out_host,
+                              int32_t* status_host, void* stream);
+/* The normalised state and memory back in host buffers (layouts of
+ * hops_batch_set_state_host; either may be NULL). */
+int hops_batch_get_state_host(const hops_structure* st, hops_batch* bt, double* phi_host,
+                              double* zmem_host, void* stream);
+
 /*
  * No counterpart in the reference.  hops_rk4_propagate without any device
  * allocation, for callers that cannot call cudaMalloc when they step: hosts
@@ -332,11 +405,19 @@ int hops_kernel_timing_read(double* total_ms, int64_t* n_launches);
  * layout and precision, z_mem), the noise, psi_out and one int32 status word
  * per trajectory; the stage vectors, accumulator and scalar workspace live in a
  * static device array of HOPS_NOALLOC_SCRATCH_BYTES that every GPU loading the
- * library keeps until exit.  Problems needing more scratch than that
- * (hops_noalloc_scratch_bytes) are rejected with HOPS_EINVAL.  The first call on
- * each device looks the array up with cudaGetSymbolAddress; make it before any
- * stream capture.  All calls share the array: calls that overlap on the GPU
- * (different streams or threads without ordering) race and corrupt each other.
+ * library keeps until exit (it sits in a CUDA module of its own, so under lazy
+ * module loading -- the CUDA 12 default -- a process holds it on a GPU only
+ * after its first call there).  Problems needing more scratch than that
+ * (hops_noalloc_scratch_bytes) are rejected with HOPS_EINVAL.  Every argument
+ * is checked before anything is launched, so a rejected call changes nothing on
+ * the device.  The status words are never cleared by the call: it only sets the
+ * word of a trajectory whose norm became NaN/Inf to HOPS_ENONFINITE, so a flag
+ * survives later calls until the caller zeroes the words (zero them before the
+ * first call).  The first call on each device (and the first after
+ * cudaDeviceReset or a change of the current context) looks the array up with
+ * cudaGetSymbolAddress; make it before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU (different streams or threads without
+ * ordering) race and corrupt each other.
  */
 #define HOPS_NOALLOC_SCRATCH_BYTES (64u << 20)
 size_t hops_noalloc_scratch_bytes(const hops_structure* st, int32_t n_traj, int32_t precision);

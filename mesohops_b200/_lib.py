@@ -74,6 +74,17 @@ class HopsFluxTask(C.Structure):
     ]
 
 
+class HopsStructureDesc(C.Structure):
+    """Mirror of ``hops_structure_desc`` (all pointer fields are host pointers)."""
+    _fields_ = [
+        ("n_hier", _i), ("n_state", _i), ("n_mode", _i), ("n_lop", _i),
+        ("up_ptr", _p), ("up_aux", _p), ("up_mode", _p),
+        ("dn_ptr", _p), ("dn_aux", _p), ("dn_mode", _p), ("dn_k", _p),
+        ("mode_lop", _p), ("mode_g", _p), ("mode_w", _p), ("lops", _p),
+        ("hamiltonian", _p), ("lt_coef", _p),
+    ]
+
+
 _lib = None
 
 
@@ -117,6 +128,22 @@ def lib():
     L.hops_batch_settle.argtypes = [C.POINTER(HopsStructure), C.POINTER(HopsBatch), _p]
     L.hops_flux_errors_smem_doubles.restype = _i
     L.hops_flux_errors_smem_doubles.argtypes = [_i, _i, _i]
+    L.hops_structure_upload.argtypes = [C.POINTER(HopsStructureDesc), _p, C.POINTER(_p)]
+    L.hops_structure_host_view.restype = C.POINTER(HopsStructure)
+    L.hops_structure_host_view.argtypes = [_p]
+    L.hops_structure_device_view.restype = _p
+    L.hops_structure_device_view.argtypes = [_p]
+    L.hops_structure_destroy.argtypes = [_p]
+    L.hops_batch_create.argtypes = [C.POINTER(HopsStructure), _i, _i, _i,
+                                    C.POINTER(C.POINTER(HopsBatch))]
+    L.hops_batch_destroy.argtypes = [C.POINTER(HopsBatch)]
+    L.hops_batch_set_state_host.argtypes = [C.POINTER(HopsStructure), C.POINTER(HopsBatch), _p,
+                                            _p, _p]
+    L.hops_batch_set_noise_host.argtypes = [C.POINTER(HopsBatch), _p, _i, _p, _i, _p]
+    L.hops_batch_propagate_host.argtypes = [C.POINTER(HopsStructure), C.POINTER(HopsBatch), _i,
+                                            _i, _i, C.c_double, _p, _p, _p]
+    L.hops_batch_get_state_host.argtypes = [C.POINTER(HopsStructure), C.POINTER(HopsBatch), _p,
+                                            _p, _p]
     L.hops_kernel_timing.argtypes = [C.c_int]
     L.hops_kernel_timing_read.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_int64)]
     _lib = L
@@ -144,4 +171,8 @@ def exported_symbols():
             "hops_kernel_timing_read", "hops_noalloc_scratch_bytes",
             "hops_rk4_propagate_noalloc", "hops_stage_tuning", "hops_flux_errors",
             "hops_flux_errors_smem_doubles", "hops_tri_max_depth", "hops_tri_pass1",
-            "hops_tri_pass2", "hops_noise_window_mean", "hops_batch_settle"]
+            "hops_tri_pass2", "hops_noise_window_mean", "hops_batch_settle",
+            "hops_structure_upload", "hops_structure_host_view", "hops_structure_device_view",
+            "hops_structure_destroy", "hops_batch_create", "hops_batch_destroy",
+            "hops_batch_set_state_host", "hops_batch_set_noise_host",
+            "hops_batch_propagate_host", "hops_batch_get_state_host"]
