@@ -11,6 +11,7 @@ files committed next to this script; the GPU box never needs the reference.
     python tests/golden/make_golden.py --ltc-adaptive  # the same with an adaptive basis
     python tests/golden/make_golden.py --dyadic      # DyadicTrajectory
     python tests/golden/make_golden.py --effective-adaptive  # effective noise, adaptive basis
+    python tests/golden/make_golden.py --bench-configs  # the benchmark's ring20 / chain10
 
 Each fixture records the inputs (system, hierarchy depth, noise arrays, psi_0,
 time step) together with the reference outputs (psi_traj, derivative values,
@@ -557,8 +558,89 @@ def main_dyadic():
                adaptive=(1e-3, 1e-3))
 
 
+def _ring20_fft_run(seed):
+    """One trajectory of the benchmark's 20-site ring with the reference's own
+    FFT_FILTER noise of SEED seed: (psi_traj, complex64 correlated noise)."""
+    n = 20
+    rng = np.random.default_rng(2)
+    H = np.diag(rng.uniform(-100, 100, n))
+    for i in range(n):
+        H[i, (i + 1) % n] = H[(i + 1) % n, i] = 80.0
+    sysp = site_system(H, [(60, 60, 295)])
+    psi0 = np.zeros(n, dtype=np.complex128)
+    psi0[0] = 1.0
+    hops = HopsTrajectory(sysp, noise_param={"SEED": seed, "MODEL": "FFT_FILTER",
+                                             "TLEN": 1004.0, "TAU": 2.0},
+                          hierarchy_param={"MAXHIER": 4}, storage_param={})
+    quiet(hops.initialize, psi0)
+    quiet(hops.propagate, 1000.0, 4.0)
+    eta = quiet(hops.noise1.get_noise, list(np.arange(0, 1004.0 + 1e-9, 2.0)))
+    return np.array(hops.storage.data["psi_traj"]), np.array(eta, dtype=np.complex64)
+
+
+def main_bench_configs():
+    """Reference runs of the benchmark configurations themselves.
+
+    c3_ring20: 20-site ring (J = 80, eps ~ U(-100, 100) from default_rng(2)), one DL
+    mode (60, 60, 295 K) per site, depth 4 (10626 aux x 20 states), psi_0 = |0>,
+    dt = 4 fs, 250 steps, FFT_FILTER noise of SEED 0..3 (TLEN 1004, TAU 2); the
+    reference's complex64 correlated noise is stored so that the trajectories can
+    be rerun exactly (as PRE_CALCULATED noise).
+    c2_chain10: 10-site chain (J = 100, eps ~ N(0, 50) from default_rng(1)), DL
+    modes (35, 50, 300 K) + (10, 500, 300 K) per site, depth 6 (230230 aux x 10
+    states), dt = 2 fs, 5 steps, seeded PRE_CALCULATED noise for two
+    trajectories; psi_traj plus a fixed sample of 4096 phi entries and
+    sum |phi|^2 at the end (phi itself is 37 MB)."""
+    from concurrent.futures import ProcessPoolExecutor
+    seeds = [0, 1, 2, 3]
+    with ProcessPoolExecutor(4) as ex:
+        runs = list(ex.map(_ring20_fft_run, seeds))
+    np.savez_compressed(os.path.join(HERE, "c3_ring20.npz"), seeds=np.array(seeds),
+                        psi_traj=np.array([r[0] for r in runs]),
+                        noise1=np.array([r[1] for r in runs]), depth=4, dt=4.0,
+                        tau_noise=2.0, tlen=1004.0, t_max=1000.0)
+    print("c3_ring20", [r[0].shape for r in runs])
+
+    n = 10
+    rng = np.random.default_rng(1)
+    H = np.diag(rng.normal(0, 50, n))
+    for i in range(n - 1):
+        H[i, i + 1] = H[i + 1, i] = 100.0
+    sysp = site_system(H, [(35, 50, 300), (10, 500, 300)])
+    psi0 = np.zeros(n, dtype=np.complex128)
+    psi0[0] = 1.0
+    out = {}
+    for k, seed in enumerate((41, 42)):
+        tlen, tau = 12.0, 1.0
+        n_t = int(np.ceil(tlen / tau)) + 1
+        r = np.random.default_rng(seed)
+        noise = ((r.normal(size=(n, n_t)) + 1j * r.normal(size=(n, n_t))) * 40.0
+                 ).astype(np.complex64)
+        tmp = tempfile.mkdtemp()
+        path = os.path.join(tmp, "noise1.npy")
+        np.save(path, noise)
+        hops = HopsTrajectory(sysp, noise_param={"SEED": path, "MODEL": "PRE_CALCULATED",
+                                                 "TLEN": tlen, "TAU": tau},
+                              hierarchy_param={"MAXHIER": 6}, storage_param={})
+        quiet(hops.initialize, psi0)
+        quiet(hops.propagate, 10.0, 2.0)
+        phi = np.array(hops.phi)
+        idx = np.random.default_rng(7).choice(len(phi), 4096, replace=False)
+        out[f"noise1_{k}"] = noise
+        out[f"psi_traj_{k}"] = np.array(hops.storage.data["psi_traj"])
+        out[f"phi_idx_{k}"] = idx
+        out[f"phi_sample_{k}"] = phi[idx]
+        out[f"phi_norm2_{k}"] = float(np.sum(np.abs(phi) ** 2))
+        out["n_hier"] = hops.n_hier
+    np.savez_compressed(os.path.join(HERE, "c2_chain10.npz"), depth=6, dt=2.0, tau_noise=1.0,
+                        tlen=12.0, t_max=10.0, n_traj=2, **out)
+    print("c2_chain10", out["n_hier"])
+
+
 if __name__ == "__main__":
-    if "--dyadic" in sys.argv:
+    if "--bench-configs" in sys.argv:
+        main_bench_configs()
+    elif "--dyadic" in sys.argv:
         main_dyadic()
     elif "--effective-adaptive" in sys.argv:
         main_effective_adaptive()
