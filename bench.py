@@ -8,6 +8,7 @@ trajectories (4 stage kernels + 4 FP64 stage-scalar kernels).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload ring20|chain10]
   python bench.py --impl reference ...     # CPU reference arm (the oracle port)
+  python bench.py --stage-probe 4,0 [--probe-time] ...   # stage-kernel shapes (profiling)
 
 Multi-GPU: one process per GPU (torchrun); every rank propagates its own 128
 trajectories (different seeds), no data-path collective ("scaling": "weak");
@@ -38,7 +39,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="ring20", choices=["ring20", "chain10"])
+    from mesohops_b200.workloads import WORKLOADS
+    ap.add_argument("--workload", default="ring20", choices=sorted(WORKLOADS),
+                    help="ring20 (the benchmark), chain10; chain120 and dimer for the stage probe")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "complex64", "complex128"],
                     help="batched path: mixed = complex128 state with complex64 stage vectors")
     ap.add_argument("--no-extras", action="store_true",
@@ -52,6 +55,14 @@ def parse():
     ap.add_argument("--adaptive-steps", type=int, default=6)
     ap.add_argument("--workers", type=int, default=-1,
                     help="adaptive worker processes (-1: min(12, cores - 4))")
+    ap.add_argument("--stage-probe", nargs="+", metavar="NB,CM", default=None,
+                    help="profiling mode: run the workload's batched stage kernel in the given "
+                         "shapes (trajectories per warp task / 32, chunk-major order) for "
+                         "--steps steps each after --warmup steps, in argument order (for a "
+                         "profiler to pick out), instead of the benchmark")
+    ap.add_argument("--probe-time", action="store_true",
+                    help="with --stage-probe: time each shape with CUDA events and print "
+                         "{shape: [ms per step, ms per stage launch]}")
     return ap.parse_args()
 
 
@@ -138,6 +149,17 @@ def algorithmic_bytes_per_step(t, B, precision):
     return n * per + 4 * t_idx
 
 
+def workload_config(wl, B, world):
+    """The ``config`` object of both arms (GPU and reference) for a workload."""
+    from math import comb
+    sysp = wl["system"]()
+    n_state = sysp["HAMILTONIAN"].shape[0]
+    n_mode = len(sysp["GW_SYSBATH"])
+    return {"workload": wl["desc"], "n_hier": comb(n_mode + wl["depth"], wl["depth"]),
+            "n_state": n_state, "n_traj_per_gpu": B, "dt_fs": wl["dt"],
+            "parallelism": f"replicas x{world} (trajectory-sharded, no collectives)"}
+
+
 def run_gpu(args):
     import torch
     import torch.distributed as dist
@@ -199,16 +221,15 @@ def run_gpu(args):
               "data": "synthetic (seeded)",
               "gpu_launches": launches}
     t = ens.dstruct.tables
-    result["config"] = {
-        "workload": wl["desc"] + f"; batched ensemble of {B} trajectories per GPU",
-        "n_hier": t["n_hier"], "n_state": t["n_state"], "n_traj_per_gpu": B,
-        "dt_fs": dt, "precision": {
+    result["config"] = workload_config(wl, B, world)
+    assert result["config"]["n_hier"] == t["n_hier"]
+    result["config"].update({
+        "precision": {
             "mixed": "complex64 stage vectors and SpMM, complex128 state, FP64 <L>/norm/z_mem",
             "complex64": "complex64 state, stage vectors and SpMM, FP64 <L>/norm/z_mem",
             "complex128": "complex128 throughout"}[args.precision],
         "l2": f"inputs larger than L2: each stage vector is "
-              f"{t['n_hier'] * t['n_state'] * B * 8 / 1e6:.0f} MB (L2 126 MB)",
-        "parallelism": f"replicas x{world} (trajectory-sharded, no collectives)"}
+              f"{t['n_hier'] * t['n_state'] * B * 8 / 1e6:.0f} MB (L2 126 MB)"})
 
     # ---- roofline of the dominant kernel (the streaming stage kernel) ----
     L = _lib.lib()
@@ -337,26 +358,15 @@ def extras(args, wl, sysp, ens, dev, value, K):
                          "note": "one trajectory per call, complex128 everywhere"}
     out["batched_over_plain"] = round(value / plain_v, 2)
 
-    # accuracy: the batched precision vs complex128 on the same seeds over the
-    # configuration's full run (250 steps)
-    na = wl["n_steps"]
-    res = {}
-    for prec in (args.precision, "complex128"):
-        e = HopsEnsemble(sysp, B, noise_param={"MODEL": "FFT_FILTER", "TLEN": tlen,
-                                               "TAU": dt / 2, "SEED": list(range(B))},
-                         hierarchy_param={"MAXHIER": depth}, precision=prec, device=dev)
-        e.initialize(psi0)
-        psi = torch.empty((na, B, e.n_state), dtype=torch.complex128, device=dev)
-        e.propagate(na * dt, dt, psi_out=psi)
-        res[prec] = psi.cpu().numpy()
-        del e
-    p64, p128 = res[args.precision], res["complex128"]
-    out["accuracy"] = {
-        "precision": args.precision,
-        "max_pop_err_vs_c128": float(np.max(np.abs(np.abs(p64) ** 2 - np.abs(p128) ** 2))),
-        "max_abs_psi_err_vs_c128": float(np.max(np.abs(np.abs(p64) - np.abs(p128)))),
-        "sample": f"{B} trajectories x {na} steps; the complex128 GPU path matches the "
-                  "FP64 CPU oracle to <=1e-10 (tests/test_gpu_parity.py)"}
+    # accuracy over independent noise realisations (seed blocks of B), the
+    # batched complex128 path on the same noise timed as a leg of its own
+    acc, c128_ms = accuracy_leg(args, wl, sysp, dev)
+    out["accuracy"] = acc
+    out["batched_c128"] = {"value": round(B / (c128_ms / 1e3), 2), "unit": UNIT,
+                           "ms_per_step": round(c128_ms, 4),
+                           "note": f"the same {B}-trajectory batch in complex128, CUDA events "
+                                   "over the 250 steps of the first accuracy realisation"}
+    out["batched_c128_over_plain"] = round(out["batched_c128"]["value"] / plain_v, 2)
 
     out["cpu_baseline"] = cpu_baseline(wl, sysp)
     if not args.no_served:
@@ -364,6 +374,101 @@ def extras(args, wl, sysp, ens, dev, value, K):
     if not args.no_adaptive:
         out["adaptive_batch"] = adaptive_leg(args, dev)
     return out
+
+
+def _oracle_psi(job):
+    """psi(t) of one trajectory by the CPU oracle (process-pool worker)."""
+    wl_name, noise, n_steps = job
+    os.environ["OMP_NUM_THREADS"] = "1"
+    from threadpoolctl import threadpool_limits
+    from oracle import hops_oracle as O
+    from mesohops_b200.workloads import WORKLOADS
+    wl = WORKLOADS[wl_name]
+    dt = wl["dt"]
+    with threadpool_limits(1):
+        b = O.OracleBasis(wl["system"](), wl["depth"])
+        psi0 = np.zeros(b.nstate, dtype=complex)
+        psi0[0] = 1.0
+        _, psi, _, _ = O.propagate(b, psi0, noise, dt / 2, n_steps * dt, dt)
+    return psi[1:]
+
+
+def wl_elems(wl):
+    """Aux count of a workload's hierarchy."""
+    from math import comb
+    n_mode = len(wl["system"]()["GW_SYSBATH"])
+    return comb(n_mode + wl["depth"], wl["depth"])
+
+
+def accuracy_leg(args, wl, sysp, dev, n_real=4, n_oracle=2):
+    """Population error of the batched precision over n_real independent noise
+    realisations (seeds r*B .. r*B + B - 1 of FFT_FILTER noise, r < n_real), each
+    over the configuration's full run: against the GPU complex128 path for every
+    trajectory, and against the CPU oracle (the FP64 restatement of the
+    reference) for the n_oracle worst trajectories of each realisation, on the
+    same complex64 noise.  Returns (record, ms per step of the complex128 batch)."""
+    import multiprocessing as mp
+    import torch
+    from mesohops_b200.ensemble import HopsEnsemble
+    B, dt, depth, na = wl["n_traj"], wl["dt"], wl["depth"], wl["n_steps"]
+    name = [k for k, v in __import__("mesohops_b200.workloads", fromlist=["x"]).WORKLOADS.items()
+            if v is wl][0]
+    tlen = (na + 2) * dt
+    psi0 = np.zeros(sysp["HAMILTONIAN"].shape[0], dtype=complex)
+    psi0[0] = 1.0
+    per_real, jobs, picks, c128_ms = [], [], [], None
+    for r in range(n_real):
+        res = {}
+        noise_host = None
+        for prec in (args.precision, "complex128"):
+            e = HopsEnsemble(sysp, B, noise_param={"MODEL": "FFT_FILTER", "TLEN": tlen,
+                                                   "TAU": dt / 2,
+                                                   "SEED": list(range(r * B, r * B + B))},
+                             hierarchy_param={"MAXHIER": depth}, precision=prec, device=dev)
+            e.initialize(psi0)
+            psi = torch.empty((na, B, e.n_state), dtype=torch.complex128, device=dev)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            e.propagate(na * dt, dt, psi_out=psi)
+            e1.record()
+            torch.cuda.synchronize()
+            if prec == "complex128" and r == 0:
+                c128_ms = e0.elapsed_time(e1) / na
+            res[prec] = psi.cpu().numpy()
+            if noise_host is None:
+                noise_host = e.noise.cpu().numpy()
+            del e
+        err = np.abs(np.abs(res[args.precision]) ** 2 - np.abs(res["complex128"]) ** 2)
+        per_traj = err.max(axis=(0, 2))
+        per_real.append(float(per_traj.max()))
+        worst = np.argsort(per_traj)[::-1][:n_oracle]
+        for b in worst:
+            jobs.append((name, noise_host[b], na))
+            picks.append((r, int(b), res[args.precision][:, b], res["complex128"][:, b]))
+    # the oracle runs after the GPU work, in spawned processes; a full run of a
+    # hierarchy of millions of elements would take the oracle hours
+    if res["complex128"].shape[2] * wl_elems(wl) > 5e6:
+        jobs, picks = [], []
+    oracle = []
+    if jobs:
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(min(len(jobs), os.cpu_count() or 1)) as pool:
+            oracle = pool.map(_oracle_psi, jobs)
+    pop_vs_oracle, c128_rel = 0.0, 0.0
+    for (r, b, pm, pc), po in zip(picks, oracle):
+        pop_vs_oracle = max(pop_vs_oracle, float(np.max(np.abs(np.abs(pm) ** 2 - np.abs(po) ** 2))))
+        c128_rel = max(c128_rel, float(np.max(np.abs(pc - po)) / np.max(np.abs(po))))
+    rec = {"precision": args.precision,
+           "max_pop_err_vs_c128": max(per_real),
+           "max_pop_err_per_realisation": per_real,
+           "max_pop_err_vs_oracle": pop_vs_oracle if picks else None,
+           "c128_vs_oracle_max_rel": c128_rel if picks else None,
+           "sample": f"{n_real} noise realisations x {B} trajectories x {na} steps (FFT_FILTER "
+                     f"seeds 0..{n_real * B - 1}); the oracle (FP64 CPU restatement of the "
+                     f"reference) reruns the {n_oracle} worst trajectories of each realisation "
+                     "on the same complex64 noise"}
+    return rec, c128_ms
 
 
 def served_leg(args, dev):
@@ -483,7 +588,65 @@ def adaptive_leg(args, dev):
                     "with one resident launch per step for all of them"}
 
 
+def stage_probe(args):
+    """Fixed stage-kernel shapes on a workload (profiling aid): no JSON line of
+    the benchmark, only "ok" or, with --probe-time, per-shape timings."""
+    import ctypes as C
+    import torch
+    from mesohops_b200 import _lib
+    from mesohops_b200.constants import hbar
+    from mesohops_b200.ensemble import HopsEnsemble
+    from mesohops_b200.workloads import WORKLOADS
+    W = WORKLOADS[args.workload]
+    B, dt = W["n_traj"], W["dt"]
+    shapes = [tuple(int(x) for x in sh.split(",")) for sh in args.stage_probe]
+    n_need = args.warmup + (len(shapes) + 1) * (args.steps + 1) + 4
+    ens = HopsEnsemble(W["system"](), B,
+                       noise_param={"SEED": list(range(B)), "MODEL": "FFT_FILTER",
+                                    "TLEN": n_need * dt, "TAU": dt / 2},
+                       hierarchy_param={"MAXHIER": W["depth"]}, precision=args.precision,
+                       autotune=False)
+    psi0 = np.zeros(ens.n_state, complex)
+    psi0[0] = 1.0
+    ens.initialize(psi0)
+    h = dt / hbar
+    ens.batch.tuning = shapes[0]
+    ens.batch.propagate(0, 1, args.warmup, h)
+    L = _lib.lib()
+    out = {}
+    for sh in shapes:
+        ens.batch.tuning = sh
+        if not args.probe_time:
+            ens.batch.propagate(0, 1, args.steps, h)
+            continue
+        torch.cuda.synchronize()
+        L.hops_kernel_timing(1)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ens.batch.propagate(0, 1, args.steps, h)
+        e1.record()
+        torch.cuda.synchronize()
+        tot = C.c_double(0)
+        nl = C.c_int64(0)
+        L.hops_kernel_timing_read(C.byref(tot), C.byref(nl))
+        L.hops_kernel_timing(0)
+        out[str(sh)] = [round(e0.elapsed_time(e1) / args.steps, 4),
+                        round(tot.value / max(nl.value, 1), 4)]
+    torch.cuda.synchronize()
+    ens.check()
+    print(json.dumps(out) if args.probe_time else "ok", flush=True)
+
+
 # ------------------------------------------------------------- CPU legs --
+def _oracle_noise(b, seed, n_steps, dt):
+    n_l = len(b.sys["L"])
+    n_t = int(np.ceil((n_steps + 2) * dt / (dt / 2))) + 1
+    rng = np.random.default_rng(seed)
+    return ((rng.normal(size=(n_l, n_t)) + 1j * rng.normal(size=(n_l, n_t))) * 40
+            ).astype(np.complex64)
+
+
 def _oracle_worker(args):
     """One trajectory of the oracle: n_warm untimed steps, then n_steps timed
     steps from the same start (single thread)."""
@@ -497,10 +660,7 @@ def _oracle_worker(args):
     dt = wl["dt"]
     with threadpool_limits(1):
         b = O.OracleBasis(sysp, wl["depth"])
-        n_t = int(np.ceil((max(n_steps, n_warm) + 2) * dt / (dt / 2))) + 1
-        rng = np.random.default_rng(seed)
-        noise = ((rng.normal(size=(b.sys["L"].__len__(), n_t))
-                  + 1j * rng.normal(size=(len(b.sys["L"]), n_t))) * 40).astype(np.complex64)
+        noise = _oracle_noise(b, seed, max(n_steps, n_warm), dt)
         psi0 = np.zeros(b.nstate, dtype=complex)
         psi0[0] = 1.0
         if n_warm > 0:
@@ -520,8 +680,55 @@ def cpu_baseline(wl, sysp, n_steps=4):
                       "oracle (single thread, after 1 untimed step)"}
 
 
+def _reference_core(wl_name, seeds, K, W, barrier, out):
+    """One host core of the reference arm: its share of the trajectories.
+
+    Every trajectory runs its W warm-up steps first (untimed); after a barrier
+    with the other cores, each trajectory advances K steps from its warm state,
+    one after the other.  Puts this core's seconds for the timed steps on out."""
+    os.environ["OMP_NUM_THREADS"] = "1"
+    from threadpoolctl import threadpool_limits
+    from oracle import hops_oracle as O
+    from mesohops_b200.workloads import WORKLOADS
+    wl = WORKLOADS[wl_name]
+    dt = wl["dt"]
+    with threadpool_limits(1):
+        b = O.OracleBasis(wl["system"](), wl["depth"])
+        S = b.nstate
+        states = []
+        for sd in seeds:
+            noise = _oracle_noise(b, sd, W + K, dt)
+            phi = np.zeros(b.nhier * S, dtype=np.complex128)
+            phi[0] = 1.0
+            zmem = np.zeros(b.nmode, dtype=np.complex128)
+            states.append([noise, phi, zmem])
+        t = 0.0
+
+        def advance(st, n0, n):
+            noise, phi, zmem = st
+            for k in range(n0, n0 + n):
+                tt = k * dt
+                zr = O.noise_lookup(noise, [tt, tt + dt / 2, tt + dt], dt / 2)
+                phi, zmem = O.rk4_step(b, phi, zmem, zr, np.zeros_like(zr), dt)
+                phi = O.normalize(phi, S)
+            st[1], st[2] = phi, zmem
+
+        for st in states:
+            advance(st, 0, W)
+        barrier.wait()
+        t0 = time.perf_counter()
+        for st in states:
+            advance(st, W, K)
+        t = time.perf_counter() - t0
+    out.put(t)
+
+
 def run_reference(args):
-    """CPU arm: the oracle port on every host core, one trajectory per process."""
+    """CPU arm: the oracle port (the reference algorithm restated in numpy) on
+    every host core, on the same workload as the GPU arm: all of its
+    trajectories, dealt round-robin to one process per core, W untimed
+    warm-up steps and K timed steps each.  The timed region is the slowest
+    core's K-step loop; value = trajectories x K / that time."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -529,25 +736,35 @@ def run_reference(args):
     import multiprocessing as mp
     from mesohops_b200.workloads import WORKLOADS
     wl = WORKLOADS[args.workload]
-    cores = os.cpu_count() or 1
-    K = max(1, min(args.steps, 3))
+    B = wl["n_traj"]
+    cores = max(1, min(os.cpu_count() or 1, B))
+    K = max(1, args.steps)
     W = max(0, args.warmup)
     ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
-        # each worker builds its basis and runs its warm-up steps outside its
-        # own timed region; the workers run concurrently, so the wall time of
-        # the step loop is the slowest one
-        el = max(pool.map(_oracle_worker, [(args.workload, s, K, W) for s in range(cores)]))
-    v = cores * K / el
+    barrier = ctx.Barrier(cores)
+    out = ctx.Queue()
+    procs = [ctx.Process(target=_reference_core,
+                         args=(args.workload, list(range(c, B, cores)), K, W, barrier, out))
+             for c in range(cores)]
+    for p in procs:
+        p.start()
+    times = [out.get() for _ in procs]
+    for p in procs:
+        p.join()
+    el = max(times)
+    v = B * K / el
     line = {"metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": world,
             "steps": K, "warmup": W, "ms_per_step": round(el / K * 1e3, 2),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "c128", "data": "synthetic (seeded)", "impl": "reference",
-            "config": {"workload": wl["desc"] + f"; {cores} trajectories, one per host core"},
+            "config": dict(workload_config(wl, B, world),
+                           precision="complex128 throughout (the reference's arithmetic)",
+                           l2="host caches; no GPU in this arm"),
             "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{cores} trajectories x {K} RK4 steps after {W} "
-                                       "untimed ones (numpy oracle, one process per core, "
-                                       "one thread each)"},
+                             "sample": f"all {B} trajectories of the workload, dealt to {cores} "
+                                       f"processes (one per host core, one thread each); {W} "
+                                       f"untimed warm-up steps, then {K} timed RK4 steps each "
+                                       "(numpy oracle, complex128)"},
             "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -557,5 +774,7 @@ if __name__ == "__main__":
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.stage_probe:
+        stage_probe(a)
     else:
         run_gpu(a)
