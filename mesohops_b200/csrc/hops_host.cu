@@ -67,7 +67,7 @@ struct Packer {
   size_t put(const void* src, size_t bytes) {
     const size_t off = (buf.size() + 255) & ~(size_t)255;
     buf.resize(off + std::max<size_t>(bytes, 16), 0);
-    if (bytes) memcpy(buf.data() + off, src, bytes);
+    if (bytes && src) memcpy(buf.data() + off, src, bytes);   // src NULL: reserve only
     return off;
   }
   size_t cplx(const std::vector<cd>& v) {

@@ -77,8 +77,8 @@ def test_nan_in_one_trajectory_flags_only_it(cuda_device, precision):
     for inject in (False, True):
         ens = _ensemble(f, B, noise, precision)
         ens.propagate(2 * dt, dt)
+        ens.batch.settle()   # both runs: the same state with no pending scale
         if inject:   # host-side write into one trajectory's state (aux 0, state 2)
-            ens.batch.settle()
             ens.batch.phi[0, 2, bad] = float("nan")
             if ens.batch.phi_lo is not None:
                 ens.batch.phi_lo[0, 2, bad] = float("nan")
