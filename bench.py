@@ -48,9 +48,13 @@ def parse():
                     help="skip the plain/accuracy/e2e/CPU/served/adaptive legs (profiling runs)")
     ap.add_argument("--no-served", action="store_true", help="skip the served-stream leg")
     ap.add_argument("--no-adaptive", action="store_true", help="skip the adaptive-batch leg")
-    ap.add_argument("--served-requests", type=int, default=48)
-    ap.add_argument("--served-plain", type=int, default=6)
-    ap.add_argument("--served-budget-gb", type=float, default=32.0)
+    ap.add_argument("--served-requests", type=int, default=512)
+    ap.add_argument("--served-cap-s", type=float, default=120.0,
+                    help="time cap of the served stream; requests unfinished then are "
+                         "reported as cancelled")
+    ap.add_argument("--served-plain", type=int, default=12,
+                    help="completed requests rerun one at a time on the plain path")
+    ap.add_argument("--served-plain-cap-s", type=float, default=60.0)
     ap.add_argument("--adaptive-traj", type=int, default=512)
     ap.add_argument("--adaptive-steps", type=int, default=6)
     ap.add_argument("--workers", type=int, default=-1,
@@ -474,23 +478,21 @@ def accuracy_leg(args, wl, sysp, dev, n_real=4, n_oracle=2):
 def served_leg(args, dev):
     """The served request stream (Poisson arrivals, mixed system and hierarchy
     sizes, adaptive or not): its first ``--served-requests`` requests through
-    HopsServer (continuous batching, admission by HBM footprint), then the
-    first few completed ones again one at a time with the plain complex128
-    path."""
+    HopsServer (continuous batching, admission by the HBM footprint against
+    the device's free memory less a reserve) under a time cap, then the first
+    completed ones again one at a time with the plain complex128 path."""
     import torch
     from mesohops_b200 import serving as sv
     from mesohops_b200.trajectory import HopsTrajectory
     from mesohops_b200.workloads import served_request, served_stream_specs
     specs = served_stream_specs()[:args.served_requests]
     reqs = [served_request(s) for s in specs]
-    free, _ = torch.cuda.mem_get_info(dev)
-    budget = int(min(0.6 * free, args.served_budget_gb * (1 << 30)))
     workers = args.workers if args.workers >= 0 else max(0, min(12, (os.cpu_count() or 2) - 4))
-    srv = sv.HopsServer(device=dev, precision=args.precision, hbm_budget=budget,
+    srv = sv.HopsServer(device=dev, precision=args.precision, hbm_budget=None,
                         chunk_steps=32, realtime=True, adaptive_workers=workers)
-    start_s = srv.pool.start_s if srv.pool is not None else 0.0
+    budget = srv.budget
     try:
-        res = srv.serve(reqs)
+        res = srv.serve(reqs, deadline_s=args.served_cap_s)
     finally:
         srv.close()
     summ = sv.summarize(res, srv.stats["makespan_s"])
@@ -498,10 +500,10 @@ def served_leg(args, dev):
     for r in res:
         if r.status == "done":
             kinds[r.kernel] = kinds.get(r.kernel, 0) + 1
-    # plain: the first completed requests one at a time, complex128, wall clock
+    # plain: completed requests one at a time, complex128, wall clock
     n_plain, steps_plain, t_plain = 0, 0, 0.0
     for r, q in zip(res, reqs):
-        if r.status != "done" or n_plain >= args.served_plain:
+        if r.status != "done" or n_plain >= args.served_plain or t_plain > args.served_plain_cap_s:
             continue
         h = HopsTrajectory(q.system_param, eom_param=q.eom_param, noise_param=q.noise_param,
                            hierarchy_param=q.hierarchy_param, storage_param={},
@@ -520,18 +522,26 @@ def served_leg(args, dev):
         "stream": f"first {len(reqs)} of the 4096-request stream (seed 4): Poisson arrivals "
                   "(mean 2 ms), chains of 2-200 sites, depth 3-8, adaptive by a fair coin",
         "precision": args.precision, "hbm_budget_bytes": budget,
+        "hbm_budget": "free device memory after the worker processes started, less a reserve "
+                      "of max(4 GiB, 5 %)",
+        "time_cap_s": args.served_cap_s,
         "adaptive_worker_processes": workers,
         "completed": summ["completed"], "rejected": summ["rejected"], "errors": summ["errors"],
+        "cancelled_at_cap": summ["cancelled"],
+        "rejected_why": "device footprint (state, stage vectors, tables, noise, psi(t)) above "
+                        "the HBM budget",
         "by_kernel": kinds, "traj_steps": summ["traj_steps"],
         "traj_steps_per_s": round(summ["traj_steps_per_s"], 2),
         "p50_ms": round(summ["p50_ms"], 1) if summ["p50_ms"] is not None else None,
         "p99_ms": round(summ["p99_ms"], 1) if summ["p99_ms"] is not None else None,
         "makespan_s": round(summ["makespan_s"], 2),
-        "plain_c128": {"requests": n_plain, "traj_steps_per_s":
-                       round(steps_plain / t_plain, 2) if t_plain > 0 else None,
-                       "note": "the first completed requests again, one at a time, "
-                               "HopsTrajectory complex128, propagate wall clock"},
-        "latency": "completion minus arrival, wall clock of the serving loop"}
+        "plain_c128": {"requests": n_plain, "traj_steps": steps_plain,
+                       "traj_steps_per_s": round(steps_plain / t_plain, 2) if t_plain > 0 else None,
+                       "note": "the first completed requests again (arrival order, up to "
+                               f"{args.served_plain} or {args.served_plain_cap_s:.0f} s), one at a "
+                               "time, HopsTrajectory complex128, propagate wall clock"},
+        "latency": "completion minus arrival, wall clock of the serving loop, completed "
+                   "requests"}
 
 
 def adaptive_leg(args, dev):

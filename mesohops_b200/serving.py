@@ -90,7 +90,7 @@ class TrajectoryRequest:
 
 
 class ServedResult:
-    """Outcome of one request: status 'done' | 'rejected' | 'error'."""
+    """Outcome of one request: status 'done' | 'rejected' | 'error' | 'cancelled'."""
 
     def __init__(self, req, status, reason="", t_axis=None, psi_traj=None, admitted=None,
                  completed=None, footprint=0, kernel=None):
@@ -202,8 +202,8 @@ class HopsServer:
     def __init__(self, device="cuda:0", precision="mixed", hbm_budget=None, chunk_steps=32,
                  builders=2, realtime=True, fairness_s=1.0, adaptive_workers=0,
                  heavy_hold_s=10.0):
-        """hbm_budget: device bytes the admitted requests may hold (default 80 %
-        of the free memory).  realtime: honour the arrival times (False: every
+        """hbm_budget: device bytes the admitted requests may hold (default: the
+        free memory, once the worker processes run, less a reserve).  realtime: honour the arrival times (False: every
         request is present at t = 0).  fairness_s: once the oldest waiting
         request has waited this long, later ones are not admitted ahead of it.
         adaptive_workers: > 0 runs the adaptive requests in that many worker
@@ -214,10 +214,6 @@ class HopsServer:
         admitted only once they have waited this long (0: no holding)."""
         self.device = torch.device(device)
         self.precision = precision
-        if hbm_budget is None:
-            free, _ = torch.cuda.mem_get_info(self.device)
-            hbm_budget = int(0.8 * free)
-        self.budget = int(hbm_budget)
         self.chunk = int(chunk_steps)
         self.builders = int(builders)
         self.realtime = realtime
@@ -228,6 +224,18 @@ class HopsServer:
         if adaptive_workers > 0:
             from .adaptive_pool import AdaptiveWorkers
             self.pool = AdaptiveWorkers(adaptive_workers, self.device, precision)
+        # the workers' CUDA contexts hold device memory too: the default budget
+        # is taken from what is free once they run
+        if hbm_budget is None:
+            hbm_budget = self.free_budget(self.device)
+        self.budget = int(hbm_budget)
+
+    @staticmethod
+    def free_budget(device, reserve_frac=0.05, reserve_min=4 << 30):
+        """Free device memory less a reserve (5 %, at least 4 GiB) for the
+        allocator's slack and the kernels' scratch."""
+        free, total = torch.cuda.mem_get_info(torch.device(device))
+        return max(0, int(free - max(reserve_min, reserve_frac * total)))
 
     def close(self):
         """Stop the adaptive worker processes (if any)."""
@@ -263,9 +271,10 @@ class HopsServer:
         return traj, psi_dev
 
     # ------------------------------------------------------------------- loop
-    def serve(self, requests):
+    def serve(self, requests, deadline_s=None):
         """Serve the requests (sorted by arrival); returns one ServedResult each,
-        in request order."""
+        in request order.  deadline_s: seconds after which every request not
+        finished yet (waiting, building or running) ends as "cancelled"."""
         reqs = sorted(requests, key=lambda r: r.arrival)
         order = {r.rid: i for i, r in enumerate(requests)}
         results = {}
@@ -291,6 +300,18 @@ class HopsServer:
         try:
             while pending or queue or building or active or pooled:
                 now = clock()
+                if deadline_s is not None and now > deadline_s:
+                    why = f"time cap of {deadline_s:.0f} s reached"
+                    for req in list(pending) + list(queue):
+                        results[req.rid] = ServedResult(req, "cancelled", why)
+                    for _, req, fp, _ in building:
+                        results[req.rid] = ServedResult(req, "cancelled", why, footprint=fp)
+                    for a in active:
+                        results[a.req.rid] = ServedResult(a.req, "cancelled", why, footprint=a.fp)
+                    for rid, (req, fp, _) in pooled.items():
+                        results[rid] = ServedResult(req, "cancelled", why, footprint=fp)
+                    pending, queue, building, active, pooled = deque(), deque(), [], [], {}
+                    break
                 while pending and arrival[pending[0].rid] <= now:
                     queue.append(pending.popleft())
                 light = (bool(pooled) or any(a.kernel != "streaming" for a in active)
@@ -486,6 +507,7 @@ def summarize(results, makespan):
         "completed": len(done),
         "rejected": sum(r.status == "rejected" for r in results),
         "errors": sum(r.status == "error" for r in results),
+        "cancelled": sum(r.status == "cancelled" for r in results),
         "traj_steps": int(steps),
         "traj_steps_per_s": steps / makespan if makespan > 0 else None,
         "p50_ms": float(np.percentile(lat, 50) * 1e3) if len(lat) else None,

@@ -82,6 +82,17 @@ WORKLOADS = {
                           "per site, depth 3 (302621 aux x 120 states), one trajectory, "
                           "dt=4 fs: a single large trajectory like the served stream's "
                           "streaming requests"),
+    "chain128": dict(system=lambda: chain_sites(128), depth=3, n_traj=1, dt=4.0, n_steps=250,
+                     desc="128-site chain (J=50 cm^-1, eps~N(0,100) seed 5), DL (50,50,295 K) "
+                          "per site, depth 3 (366145 aux x 128 states), one trajectory, dt=4 fs"),
+    "chain200": dict(system=lambda: chain_sites(200), depth=3, n_traj=1, dt=4.0, n_steps=250,
+                     desc="200-site chain (J=50 cm^-1, eps~N(0,100) seed 5), DL (50,50,295 K) "
+                          "per site, depth 3 (1373701 aux x 200 states), one trajectory, dt=4 fs: "
+                          "the largest systems of the served stream"),
+    "chain200_uncoupled": dict(
+        system=lambda: chain(200, 0.0, np.random.default_rng(5).normal(0, 100, 200), 50.0, 50.0),
+        depth=3, n_traj=1, dt=4.0, n_steps=250,
+        desc="chain200 with J = 0 (diagonal H): the same hierarchy without the -iH couplings"),
     "dimer": dict(system=dimer, depth=4, n_traj=1, dt=4.0, n_steps=250,
                   desc="2-site dimer H=[[0,50],[50,0]], DL (50,50,295 K) per site, depth 4 "
                        "(15 aux x 2 states), one trajectory, dt=4 fs, 1000 fs"),
