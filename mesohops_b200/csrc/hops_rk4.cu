@@ -253,14 +253,51 @@ __device__ __forceinline__ void acc_store(ST* p, ST v) {
   else *p = v;
 }
 
+// Mixed precision in the stage kernels (complex128 state, complex64 stage
+// vectors): the third stage does not store the accumulated slope in complex64
+// but the partial sum P = phi + h/6 (k1 + 2 k2 + 2 k3) in complex128 -- real
+// parts in the accumulator's buffer, imaginary parts in the buffer of phi's
+// complex64 copy, which no kernel reads between the second stage and the
+// fourth -- and the fourth stage reads P in place of phi and the slope:
+// phi' = P + h/6 k4.  The same bytes move, one complex64 rounding of the
+// slope (the largest, of k1 + 2 k2 + 2 k3) is gone.
+template <typename ST, typename PT>
+constexpr bool psum_mode() { return sizeof(PT) == 16 && sizeof(ST) == 8; }
+
+__device__ __forceinline__ double* psum_re(void* acc) { return static_cast<double*>(acc); }
+__device__ __forceinline__ double* psum_im(void* shadow) { return static_cast<double*>(shadow); }
+
 // rk_finish: the same update with the accumulated slope acc[e] already loaded
 // (accv; read at stages 1-3 only), so that a caller can load the operands of
-// several elements before it stores any of them.
-template <bool GHINT, typename T, typename ST, typename PT>
+// several elements before it stores any of them.  PSUM: the partial-sum form
+// above (the caller passes P as ph at the fourth stage).
+template <bool GHINT, bool PSUM, typename T, typename ST, typename PT>
 __device__ __forceinline__ void rk_finish(int stage, double h, T k, PT ph, ST accv, ST* acc,
                                           ST* yout, PT* phi, ST* shadow, size_t e) {
   using RP = decltype(ph.x);
   const RP hh = (RP)h;
+  if constexpr (PSUM) {
+    if (stage == 2) {
+      PT sum = cv<PT>(cadd(cv<T>(accv), cscale(k, (decltype(k.x))2)));
+      PT hs = cscale(sum, hh);
+      hs.x = hs.x / (RP)6;
+      hs.y = hs.y / (RP)6;
+      const PT pp = cadd(ph, hs);
+      __stcs(psum_re(acc) + e, (double)pp.x);
+      __stcs(psum_im(shadow) + e, (double)pp.y);
+      yout[e] = cv<ST>(cadd(ph, cscale(cv<PT>(k), hh)));
+      return;
+    }
+    if (stage == 3) {
+      PT hs = cscale(cv<PT>(k), hh);
+      hs.x = hs.x / (RP)6;
+      hs.y = hs.y / (RP)6;
+      const PT nw = cadd(ph, hs);
+      phi[e] = nw;
+      shadow[e] = cv<ST>(nw);
+      return;
+    }
+  }
   switch (stage) {
     case 0: {
       acc_store<GHINT>(acc + e, cv<ST>(k));
@@ -291,7 +328,7 @@ template <bool GHINT, typename T, typename ST, typename PT>
 __device__ __forceinline__ void rk_update(int stage, double h, T k, PT ph, ST* acc, ST* yout,
                                           PT* phi, ST* shadow, size_t e) {
   const ST accv = (stage >= 1 && stage <= 3) ? acc_load<GHINT>(acc + e) : ST{};
-  rk_finish<GHINT, T, ST, PT>(stage, h, k, ph, accv, acc, yout, phi, shadow, e);
+  rk_finish<GHINT, false, T, ST, PT>(stage, h, k, ph, accv, acc, yout, phi, shadow, e);
 }
 
 // Asynchronous global -> shared copies (cp.async, no register staging).
@@ -377,8 +414,11 @@ __global__ void __launch_bounds__(wide_threads(NB), NB <= 2 ? 4 : (NB == 4 ? HOP
              (size_t)wib * 2 * CH;
   ST* ys_s = reinterpret_cast<ST*>(wide_smem + (size_t)nwb * 2 * CH * (sizeof(PT) + sizeof(ST))) +
              (size_t)wib * 2 * CH;
-  const bool want_phi = stage != 4;
-  const bool want_acc = stage >= 1 && stage <= 3;
+  constexpr bool PSUM = psum_mode<ST, PT>();
+  // fourth stage of the partial-sum form: P (re, im) in place of phi and acc
+  const bool want_psum = PSUM && stage == 3;
+  const bool want_phi = stage != 4 && !want_psum;
+  const bool want_acc = stage >= 1 && stage <= 3 && !want_psum;
   auto prefetch = [&](unsigned t, unsigned ci, int buf) {
     const unsigned as = chunk_major ? t - ci * n_as : t;
     const size_t row = (size_t)as * B;
@@ -390,6 +430,13 @@ __global__ void __launch_bounds__(wide_threads(NB), NB <= 2 ? 4 : (NB == 4 ? HOP
         cp_async<sizeof(ST)>(ys_s + o, yin + row + b);
         if (want_phi) cp_async<sizeof(PT)>(ph_s + o, phi + row + b);
         if (want_acc) cp_async<sizeof(ST)>(ac_s + o, acc + row + b);
+        if constexpr (PSUM) {
+          if (want_psum) {
+            double* pd = reinterpret_cast<double*>(ph_s + o);
+            cp_async<8>(pd, psum_re(acc) + row + b);
+            cp_async<8>(pd + 1, psum_im(shadow) + row + b);
+          }
+        }
       }
     }
   };
@@ -545,7 +592,7 @@ __global__ void __launch_bounds__(wide_threads(NB), NB <= 2 ? 4 : (NB == 4 ? HOP
       sc[j] = 1.0;
       if (!ok[j]) continue;
       sc[j] = scaleB[bg + lane + 32 * j];
-      if (want_phi) ph[j] = ph_s[o];
+      if (want_phi || want_psum) ph[j] = ph_s[o];
       if (want_acc) accv[j] = ac_s[o];
     }
 #pragma unroll
@@ -558,8 +605,9 @@ __global__ void __launch_bounds__(wide_threads(NB), NB <= 2 ? 4 : (NB == 4 ? HOP
         if constexpr (sizeof(R) == 8) kk = cadd(kk, ld2(ws + bl.physT, s * B + bg + lane + 32 * j));
         else kk = cadd(kk, ld2f(reinterpret_cast<const float*>(ws + bl.physT_f), s * B + bg + lane + 32 * j));
       }
-      const PT p = stage == 4 ? PT{} : cscale(ph[j], (decltype(PT{}.x))sc[j]);
-      rk_finish<true, T, ST, PT>(stage, h, kk, p, accv[j], acc, yout, phi, shadow, e);
+      // P was formed from the scaled state: no scale at the partial-sum stage
+      const PT p = stage == 4 ? PT{} : (want_psum ? ph[j] : cscale(ph[j], (decltype(PT{}.x))sc[j]));
+      rk_finish<true, PSUM, T, ST, PT>(stage, h, kk, p, accv[j], acc, yout, phi, shadow, e);
     }
     t = tn;
     ci = cn;
@@ -590,17 +638,25 @@ __global__ void __launch_bounds__(256) k_narrow(hops_structure st, int B, int st
       const int b = r - s * B;
       const size_t e = (size_t)a * SB + r;
       // the element's own streamed operands first: their DRAM latency then
-      // overlaps the neighbour gather instead of following it
-      const PT ph0 = stage == 4 ? PT{} : phi[e];
-      const ST accv = (stage >= 1 && stage <= 3) ? acc_load<true>(acc + e) : ST{};
+      // overlaps the neighbour gather instead of following it; the fourth
+      // stage of the partial-sum form reads P (already scaled) instead
+      constexpr bool PSUM = psum_mode<ST, PT>();
+      const bool want_psum = PSUM && stage == 3;
+      PT ph0 = PT{};
+      if (want_psum) {
+        if constexpr (PSUM) ph0 = PT{__ldcs(psum_re(acc) + e), __ldcs(psum_im(shadow) + e)};
+      } else if (stage != 4) {
+        ph0 = phi[e];
+      }
+      const ST accv = (stage >= 1 && stage <= 3 && !want_psum) ? acc_load<true>(acc + e) : ST{};
       const double sc = scaleB[b];
       auto y = [&](int x, int sp) { return cv<T>(yin[((size_t)x * S + sp) * B + b]); };
       const CoefT<R> cf{ws, bl, B, b};
       T k = deriv_elem<R, SITE>(st, a, s, y, cf);
       if (stage == 0 || stage == 4) k = cscale(k, (R)sc);
       if (st.lt_coef && a == 0) k = cadd(k, cf.phys(s));  // LT term of psi_0 (already scaled)
-      const PT ph = cscale(ph0, (decltype(PT{}.x))sc);
-      rk_finish<true, T, ST, PT>(stage, h, k, ph, accv, acc, yout, phi, shadow, e);
+      const PT ph = want_psum ? ph0 : cscale(ph0, (decltype(PT{}.x))sc);
+      rk_finish<true, PSUM, T, ST, PT>(stage, h, k, ph, accv, acc, yout, phi, shadow, e);
     }
   }
 }
