@@ -56,7 +56,11 @@ def parse():
                     help="completed requests rerun one at a time on the plain path")
     ap.add_argument("--served-plain-cap-s", type=float, default=60.0)
     ap.add_argument("--adaptive-traj", type=int, default=512)
-    ap.add_argument("--adaptive-steps", type=int, default=6)
+    ap.add_argument("--adaptive-steps", type=int, default=6,
+                    help="early phase of the adaptive leg (the inch-worm integrator's 5 steps "
+                         "and one more)")
+    ap.add_argument("--adaptive-steady-steps", type=int, default=50,
+                    help="steady phase of the adaptive leg, timed on its own")
     ap.add_argument("--workers", type=int, default=-1,
                     help="adaptive worker processes (-1: min(12, cores - 4))")
     ap.add_argument("--stage-probe", nargs="+", metavar="NB,CM", default=None,
@@ -553,7 +557,8 @@ def adaptive_leg(args, dev):
     from mesohops_b200.adaptive_pool import AdaptiveWorkers
     from mesohops_b200.serving import TrajectoryRequest
     from mesohops_b200.workloads import adaptive_chain500
-    n, K = args.adaptive_traj, args.adaptive_steps
+    n, K1, K2 = args.adaptive_traj, args.adaptive_steps, args.adaptive_steady_steps
+    K = K1 + K2
     sysp, psi0, seeds = adaptive_chain500(n)
     dt = 4.0
     workers = args.workers if args.workers >= 0 else max(1, min(12, (os.cpu_count() or 2) - 4))
@@ -573,29 +578,37 @@ def adaptive_leg(args, dev):
             for ev in pool.events(timeout=1.0):
                 errors.extend(ev[2])
         t_init = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        pool.step_idle(K)
-        done = []
-        while any(pool.stepping):
-            for ev in pool.events(timeout=1.0):
-                done.extend(ev[1])
-                errors.extend(ev[2])
-        el = time.perf_counter() - t0
+        done, phases = [], []
+        for k in (K1, K2):
+            if k <= 0:
+                continue
+            t0 = time.perf_counter()
+            pool.step_idle(k)
+            while any(pool.stepping):
+                for ev in pool.events(timeout=1.0):
+                    done.extend(ev[1])
+                    errors.extend(ev[2])
+            phases.append((k, time.perf_counter() - t0))
     finally:
         pool.close()
     sizes = np.array([d[3] * d[4] for d in done]) if done else np.zeros(1)
+    live = n - len(errors)
     return {"workload": "500-site chain (J=50, eps~N(0,100) seed 3), DL (50,50,295 K) per "
                         "site, depth 10, delta_a = delta_s = 1e-3, dt = 4 fs, psi_0 on a "
                         f"seeded site; {n} trajectories (noise seeds 0..{n - 1})",
             "steps": K, "completed": len(done), "errors": len(errors),
-            "traj_steps_per_s": round(len(done) * K / el, 2),
+            "traj_steps_per_s_early": round(live * phases[0][0] / phases[0][1], 2),
+            "traj_steps_per_s_steady": (round(live * phases[1][0] / phases[1][1], 2)
+                                        if len(phases) > 1 else None),
+            "traj_steps_per_s": round(live * K / sum(t for _, t in phases), 2),
             "basis_elems_end": {"min": int(sizes.min()), "median": int(np.median(sizes)),
                                 "max": int(sizes.max())},
             "worker_processes": workers, "init_s": round(t_init, 2),
             "precision": args.precision,
-            "note": f"first {K} steps (inch-worm early integrator included), wall clock of "
-                    "the stepping; each worker process steps its trajectories in lock-step "
-                    "with one resident launch per step for all of them"}
+            "note": f"early phase: the first {K1} steps (inch-worm early integrator); steady "
+                    f"phase: the next {K2} steps, timed on its own; wall clock of the stepping; "
+                    "each worker process steps its trajectories in lock-step with one resident "
+                    "launch per step for all of them"}
 
 
 def stage_probe(args):
