@@ -381,10 +381,11 @@ class AdaptiveHops:
         self.early_steps = ip["EARLY_INTEGRATOR_STEPS"]
         self.inchworm_cap = ip["INCHWORM_CAP"]
         self.early = ip["EARLY_ADAPTIVE_INTEGRATOR"]
-        if self.early not in ("INCH_WORM", "STATIC"):
+        if self.early not in ("INCH_WORM", "STATIC", "STATIC_STATE_INCHWORM_HIERARCHY"):
             raise UnsupportedRequest(self.early, "early time integrator clause of the propagate")
-        if ip["STATIC_BASIS"] is not None:
-            raise UnsupportedRequest("STATIC_BASIS with an adaptive basis",
+        self.static_states, self.static_counts = self._static_basis(ip["STATIC_BASIS"])
+        if self.early == "STATIC_STATE_INCHWORM_HIERARCHY" and self.static_states is None:
+            raise UnsupportedRequest("STATIC_STATE_INCHWORM_HIERARCHY without a STATIC_BASIS",
                                      "mesohops_b200 adaptive propagation")
         self.eom = ep["EQUATION_OF_MOTION"]
         if self.eom == "LINEAR":
@@ -421,6 +422,44 @@ class AdaptiveHops:
         self.noise1_dev = self.noise2_dev = None
         self.noise1_host = self.noise2_host = None
         self.t = 0.0
+
+    def _static_basis(self, sb):
+        """integration_param STATIC_BASIS = [states, aux list] (hops_trajectory.py
+        :293-316): absolute states, and aux given as count vectors over all modes,
+        as (mode, depth) pairs, or as objects with ``todense()`` (the
+        reference's AuxiliaryVector).  Returns (states, count rows) or (None, None)."""
+        if sb is None:
+            return None, None
+        if len(sb) != 2:
+            raise UnsupportedRequest("STATIC_BASIS must be [state list, aux list]",
+                                     "mesohops_b200 adaptive propagation")
+        M = self.system.n_mode
+        states = np.array(sorted(set(int(x) for x in sb[0])), dtype=np.int64)
+        rows = []
+        for a in sb[1]:
+            if hasattr(a, "todense"):
+                v = np.asarray(a.todense(), dtype=np.int64).ravel()
+            else:
+                arr = np.asarray(a, dtype=np.int64)
+                if arr.ndim == 2 or (arr.ndim == 1 and arr.size == 0):
+                    v = np.zeros(M, dtype=np.int64)
+                    for m, k in arr.reshape(-1, 2):
+                        v[m] = k
+                else:
+                    v = arr.ravel()
+            if v.size != M or np.any(v < 0) or v.sum() > self.maxhier:
+                raise UnsupportedRequest("STATIC_BASIS aux outside the hierarchy",
+                                         "mesohops_b200 adaptive propagation")
+            rows.append(v)
+        counts = np.array(rows, dtype=np.int16).reshape(-1, M)
+        return states, counts
+
+    def _union_counts(self, a, b):
+        """Rows of a followed by the rows of b not in a."""
+        allc = np.concatenate([a, b], axis=0)
+        keys = self.keyer.sort_keys(allc)
+        _, first = np.unique(keys, return_index=True)
+        return allc[np.sort(first)]
 
     # ------------------------------------------------------------ basis setup
     def _set_basis(self, states, counts):
@@ -558,8 +597,15 @@ class AdaptiveHops:
         phi = np.zeros(self.basis.n_hier * self.basis.n_state, dtype=np.complex128)
         phi[:self.basis.n_state] = psi0[self.basis.states]
         self.t = 0.0
-        z_step = self._z_step(0.0, self.zmem_abs)
-        states_u, counts_u = yield from self.define_basis_gen(phi, 1.0, z_step)
+        if self.static_states is None:
+            z_step = self._z_step(0.0, self.zmem_abs)
+            states_u, counts_u = yield from self.define_basis_gen(phi, 1.0, z_step)
+        else:
+            # the initial basis joined with the static one instead of a first
+            # basis update
+            states_u = np.array(sorted(set(self.basis.states.tolist())
+                                       | set(self.static_states.tolist())), dtype=np.int64)
+            counts_u = self._union_counts(self.basis.counts, self.static_counts)
         self.phi = self.update_basis(phi, states_u, counts_u)
 
     # ------------------------------------------------------------------ noise
@@ -859,13 +905,21 @@ class AdaptiveHops:
                                    effective=self.traj.effective_noise_integration)
         phi = self._normalize(phi)
         if self.early_counter < self.early_steps:
-            if self.early == "INCH_WORM":
+            if self.early in ("INCH_WORM", "STATIC_STATE_INCHWORM_HIERARCHY"):
+                # STATIC_STATE_INCHWORM_HIERARCHY: the state basis of the early
+                # steps is the static one, the hierarchy inch-worms
+                # (hops_trajectory.py:477-491)
+                fixed = self.early == "STATIC_STATE_INCHWORM_HIERARCHY"
                 z_step = self._z_step(self.t, z)
                 states_u, counts_u = yield from self.define_basis_gen(phi, tau, z_step)
+                if fixed:
+                    states_u = self.static_states
                 n_iter = 0
                 while not self.basis.same_as(states_u, counts_u):
                     states_u, counts_u, phi, z = yield from self._inchworm_gen(
                         states_u, counts_u, tau)
+                    if fixed:
+                        states_u = self.static_states
                     n_iter += 1
                     if n_iter >= self.inchworm_cap:
                         break

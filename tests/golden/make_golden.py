@@ -12,6 +12,7 @@ files committed next to this script; the GPU box never needs the reference.
     python tests/golden/make_golden.py --dyadic      # DyadicTrajectory
     python tests/golden/make_golden.py --effective-adaptive  # effective noise, adaptive basis
     python tests/golden/make_golden.py --bench-configs  # the benchmark's ring20 / chain10
+    python tests/golden/make_golden.py --static-basis   # STATIC_BASIS, adaptive
 
 Each fixture records the inputs (system, hierarchy depth, noise arrays, psi_0,
 time step) together with the reference outputs (psi_traj, derivative values,
@@ -450,6 +451,37 @@ def main_adaptive():
                      delta, delta, noise_seed=seed)
 
 
+def main_static_basis():
+    """Adaptive basis with integration_param STATIC_BASIS (states and aux joined
+    to the initial basis, hops_trajectory.py:293-316), with the INCH_WORM early
+    integrator and with STATIC_STATE_INCHWORM_HIERARCHY (the state basis of the
+    early steps fixed to the static states, :477-491)."""
+    from mesohops.basis.hops_aux import AuxiliaryVector
+    n = 12
+    rng = np.random.default_rng(3)
+    eps = rng.normal(0, 100, n)
+    H = np.diag(eps)
+    for i in range(n - 1):
+        H[i, i + 1] = H[i + 1, i] = 50.0
+    psi0 = np.zeros(n, dtype=np.complex128)
+    psi0[n // 2] = 1.0
+    static_states = [4, 5, 6, 7]
+    static_aux_pairs = [[(6, 1)], [(5, 1), (6, 1)], [(7, 2)]]
+    rows = np.zeros((len(static_aux_pairs), n), dtype=np.int16)
+    for i, pairs in enumerate(static_aux_pairs):
+        for m, k in pairs:
+            rows[i, m] = k
+    for name, early in (("adaptive_static_inchworm", "INCH_WORM"),
+                        ("adaptive_static_state", "STATIC_STATE_INCHWORM_HIERARCHY")):
+        integ = {"INTEGRATOR": "RUNGE_KUTTA", "EARLY_ADAPTIVE_INTEGRATOR": early,
+                 "STATIC_BASIS": [list(static_states),
+                                  [AuxiliaryVector(p, n) for p in static_aux_pairs]]}
+        run_adaptive(name, site_system(H, [(50, 50, 295)]), 4, psi0, 80.0, 4.0, 1e-3, 1e-3,
+                     noise_seed=61, integration=integ,
+                     extra={"static_states": np.array(static_states),
+                            "static_aux": rows, "early_integrator": early})
+
+
 def run_dyadic(name, eom, sparse_input, noise_seed, adaptive=None):
     """DyadicTrajectory (trajectory/hops_dyadic.py) on a 3-site system with a
     ground state: ket and bra excitations, propagation, a bra de-excitation,
@@ -640,6 +672,8 @@ def main_bench_configs():
 if __name__ == "__main__":
     if "--bench-configs" in sys.argv:
         main_bench_configs()
+    elif "--static-basis" in sys.argv:
+        main_static_basis()
     elif "--dyadic" in sys.argv:
         main_dyadic()
     elif "--effective-adaptive" in sys.argv:

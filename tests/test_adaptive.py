@@ -26,7 +26,7 @@ from oracle import hops_oracle as O
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CASES = ["adaptive_dod_full", "adaptive_chain8", "adaptive_chain12", "adaptive_chain8_ltc",
-         "adaptive_chain8_eff"]
+         "adaptive_chain8_eff", "adaptive_static_inchworm", "adaptive_static_state"]
 # the benchmark's 500-site chain at depth 10 (aux keys beyond int64): the oracle
 # would need its 500 dense L-operators, so only the GPU run is compared
 GPU_ONLY_CASES = ["adaptive_chain500"]
@@ -54,6 +54,13 @@ def system_param(f):
 def make_traj(f, tmp_path, device):
     path = str(tmp_path / "noise1.npy")
     np.save(path, f["noise1"])
+    integ = {"INTEGRATOR": "RUNGE_KUTTA",
+             # the fixture with noise finer than dt / 2 was made with
+             # EFFECTIVE_NOISE_INTEGRATION (make_golden.py --effective-adaptive)
+             "EFFECTIVE_NOISE_INTEGRATION": 2 * float(f["tau_noise"]) < float(f["dt"]) - 1e-12}
+    if "static_states" in f:   # make_golden.py --static-basis
+        integ["STATIC_BASIS"] = [f["static_states"].tolist(), list(f["static_aux"])]
+        integ["EARLY_ADAPTIVE_INTEGRATOR"] = str(f["early_integrator"])
     hops = HopsTrajectory(system_param(f),
                           noise_param={"SEED": path, "MODEL": "PRE_CALCULATED",
                                        "TLEN": float(f["tlen"]), "TAU": float(f["tau_noise"])},
@@ -61,11 +68,7 @@ def make_traj(f, tmp_path, device):
                           eom_param={"EQUATION_OF_MOTION": "NORMALIZED NONLINEAR"},
                           storage_param={}, device_param={"DEVICE": device,
                                                           "PRECISION": "complex128"},
-                          # the fixture with noise finer than dt / 2 was made with
-                          # EFFECTIVE_NOISE_INTEGRATION (make_golden.py --effective-adaptive)
-                          integration_param={"INTEGRATOR": "RUNGE_KUTTA",
-                                             "EFFECTIVE_NOISE_INTEGRATION":
-                                             2 * float(f["tau_noise"]) < float(f["dt"]) - 1e-12})
+                          integration_param=integ)
     hops.make_adaptive(float(f["delta_a"]), float(f["delta_s"]),
                        update_step=int(f["update_step"]), f_discard=float(f["f_discard"]),
                        adaptive_noise=False)
