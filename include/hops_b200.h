@@ -136,12 +136,15 @@ typedef struct hops_batch {
   void* y1;
   double* zmem;  /* [B][n_mode] complex noise memory */
   double* work;  /* scalar workspace of hops_scalar_workspace_doubles() doubles */
-  const float* noise1; /* [B][n_lop][n_t1] complex64 */
-  const float* noise2; /* [B][n_lop][n_t2] complex64, or NULL for zero noise 2 */
+  const float* noise1; /* [B][n_lop][n_t1] complex64 (complex128 if noise_c128) */
+  const float* noise2; /* [B][n_lop][n_t2] likewise, or NULL for zero noise 2 */
   int32_t* status;     /* [B] 0 ok, HOPS_ENONFINITE if a norm went NaN/Inf */
   void* phi_lo;        /* HOPS_PREC_MIXED: complex64 copy of phi read by stage 1 */
   int32_t defer_scale; /* 1: hops_rk4_propagate leaves the renormalisation of its
                           last step pending (see there) */
+  int32_t noise_c128;  /* 1: noise1 / noise2 hold complex128 samples (noise with
+                          INTERPOLATE, hops_noise.py:242-279: the cubic spline
+                          through the samples, evaluated at them); 0: complex64 */
 } hops_batch;
 
 /* One trajectory of hops_resident_propagate (array in device memory). */
@@ -149,7 +152,7 @@ typedef struct hops_task {
   const hops_structure* st; /* device pointer to the structure */
   void* phi;                /* [n_hier][n_state]: complex64 for HOPS_PREC_C64, else complex128 */
   double* zmem;             /* [n_mode] complex */
-  const float* noise1;      /* [n_lop][n_t1] complex64 */
+  const float* noise1;      /* [n_lop][n_t1] complex64 (complex128 if noise_c128) */
   const float* noise2;      /* [n_lop][n_t2] complex64 or NULL */
   double* psi_out;          /* [n_steps][n_state] complex128, or NULL */
   void* scratch;            /* 3 * n_hier * n_state stage elements (complex128 for
@@ -164,6 +167,8 @@ typedef struct hops_task {
   int32_t status;   /* written by the kernel: 0 ok, HOPS_ENONFINITE */
   double tau_over_hbar;
   double scale;     /* pending normalisation factor of phi (1 = none) */
+  int32_t noise_c128; /* 1: noise1 / noise2 hold complex128 samples (see hops_batch) */
+  int32_t pad;
 } hops_task;
 
 /* One trajectory of hops_flux_errors (array in device memory). */

@@ -50,7 +50,7 @@ class HopsBatch(C.Structure):
         ("n_traj", _i), ("precision", _i), ("eom", _i), ("n_t1", _i), ("n_t2", _i),
         ("phi", _p), ("acc", _p), ("y0", _p), ("y1", _p),
         ("zmem", _p), ("work", _p), ("noise1", _p), ("noise2", _p), ("status", _p),
-        ("phi_lo", _p), ("defer_scale", _i),
+        ("phi_lo", _p), ("defer_scale", _i), ("noise_c128", _i),
     ]
 
 
@@ -62,6 +62,7 @@ class HopsTask(C.Structure):
         ("n_t1", _i), ("n_t2", _i), ("it0", _i), ("di", _i), ("n_steps", _i),
         ("precision", _i), ("eom", _i), ("status", _i),
         ("tau_over_hbar", C.c_double), ("scale", C.c_double),
+        ("noise_c128", _i), ("pad", _i),
     ]
 
 

@@ -396,6 +396,9 @@ class AdaptiveHops:
                 raise UnsupportedRequest("adaptive basis with off-diagonal L-operator couplings",
                                          "mesohops_b200 adaptive propagation")
         n1, n2 = traj.noise1, traj.noise2
+        if n1.interpolate or n2.interpolate:
+            raise UnsupportedRequest("INTERPOLATE noise with an adaptive basis",
+                                     "mesohops_b200 adaptive propagation")
         if (n2.param["MODEL"] != "ZERO"
                 and abs(n2.param["TAU"] - n1.param["TAU"]) >= precision):
             raise UnsupportedRequest("noise 2 on a different time axis with an adaptive basis",

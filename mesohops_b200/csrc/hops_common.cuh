@@ -148,12 +148,20 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return r;
 }
 
+// Noise sample i of a row stored as complex64 or complex128.
+__device__ __forceinline__ double2 noise_at(const void* p, size_t i, int c128) {
+  if (c128) return reinterpret_cast<const double2*>(p)[i];
+  const float2 v = reinterpret_cast<const float2*>(p)[i];
+  return mk((double)v.x, (double)v.y);
+}
+
 struct StageIO {
   // inputs
   const double* zmem;   // [M] noise memory at the start of the step
-  const float2* noise1;  // [L][n_t1] of this trajectory (complex64)
-  const float2* noise2;  // [L][n_t2] or null
+  const void* noise1;   // [L][n_t1] of this trajectory (complex64, or complex128
+  const void* noise2;   // if noise_c128); noise2 [L][n_t2] or null
   int n_t1, n_t2;
+  int noise_c128;
   int it;               // noise time index of this stage
   int stage;            // 0..3, or 4 = single derivative (no RK bookkeeping)
   int eom;
@@ -230,23 +238,26 @@ __device__ void stage_scalars(const hops_structure& st, const StageIO& io, Get g
       ltc = cmul(cconj(ld2(st.lt_coef, j)), num);
     }
     // compress_zmem: sum of z_mem over the modes of L_j, then + conj(z1).
-    float2 z1 = io.noise1 ? io.noise1[(size_t)j * io.n_t1 + io.it] : mkf(0.f, 0.f);
+    const double2 z1 = io.noise1 ? noise_at(io.noise1, (size_t)j * io.n_t1 + io.it, io.noise_c128)
+                                 : mk(0.0, 0.0);
     double2 zs = mk(0.0, 0.0);
     if (!linear) {
       const double* zsrc = io.stage == 0 || io.stage == 4 ? io.zmem : ws + lay.zst();
       for (int m = 0; m < M; ++m)
         if (st.mode_lop[m] == j) zs = cadd(zs, ld2(zsrc, m));
     }
-    double2 zh = cadd(mk((double)z1.x, -(double)z1.y), zs);
+    double2 zh = cadd(mk(z1.x, -z1.y), zs);
     zhat[j] = zh;
-    float2 z2 = io.noise2 ? io.noise2[(size_t)j * io.n_t2 + io.it] : mkf(0.f, 0.f);
-    double2 cz = (linear || act) ? mk(zh.x + (double)z2.y, zh.y - (double)z2.x) : mk(0.0, 0.0);
+    const double2 z2 = io.noise2 ? noise_at(io.noise2, (size_t)j * io.n_t2 + io.it, io.noise_c128)
+                                 : mk(0.0, 0.0);
+    double2 cz = (linear || act) ? mk(zh.x + z2.y, zh.y - z2.x) : mk(0.0, 0.0);
     cz = cadd(cz, ltc);
     // The LINEAR closure forms conj(z1) - 1j*z2 from complex64 samples without
     // any complex128 term, so the reference rounds it to complex64
     // (hops_eom.py:520,535); the float sum of two floats taken in double and
-    // rounded once is the correctly rounded float sum.
-    if (linear) cz = mk((double)(float)cz.x, (double)(float)cz.y);
+    // rounded once is the correctly rounded float sum.  Complex128 samples
+    // (INTERPOLATE) are not rounded.
+    if (linear && !io.noise_c128) cz = mk((double)(float)cz.x, (double)(float)cz.y);
     reinterpret_cast<double2*>(ws + lay.cz())[j] = cz;
     reinterpret_cast<double2*>(ws + lay.avgL())[j] = num;
   }

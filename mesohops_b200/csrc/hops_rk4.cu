@@ -746,13 +746,18 @@ __global__ void __launch_bounds__(128) k_scalars(hops_structure st, hops_batch b
     io.noise2 = z2s ? reinterpret_cast<const float2*>(z2s) + (size_t)b * L : nullptr;
     io.n_t1 = 1;
     io.n_t2 = 1;
+    io.noise_c128 = 0;
     io.it = 0;
     io.zmem_out = dz_out + (size_t)b * M * 2;
   } else {
-    io.noise1 = bt.noise1 ? reinterpret_cast<const float2*>(bt.noise1) + (size_t)b * L * bt.n_t1 : nullptr;
-    io.noise2 = bt.noise2 ? reinterpret_cast<const float2*>(bt.noise2) + (size_t)b * L * bt.n_t2 : nullptr;
+    const size_t esz = bt.noise_c128 ? 16 : 8;
+    io.noise1 = bt.noise1 ? reinterpret_cast<const char*>(bt.noise1) + (size_t)b * L * bt.n_t1 * esz
+                          : nullptr;
+    io.noise2 = bt.noise2 ? reinterpret_cast<const char*>(bt.noise2) + (size_t)b * L * bt.n_t2 * esz
+                          : nullptr;
     io.n_t1 = bt.n_t1;
     io.n_t2 = bt.n_t2;
+    io.noise_c128 = bt.noise_c128;
     io.it = it;
     io.zmem_out = bt.zmem + (size_t)b * M * 2;
   }
@@ -893,10 +898,11 @@ __global__ void __launch_bounds__(512, 1) k_resident(hops_task* tasks, int mode,
   StageIO io;
   io.zmem = zm;
   io.zmem_out = zm;
-  io.noise1 = reinterpret_cast<const float2*>(tk->noise1);
-  io.noise2 = reinterpret_cast<const float2*>(tk->noise2);
+  io.noise1 = tk->noise1;
+  io.noise2 = tk->noise2;
   io.n_t1 = tk->n_t1;
   io.n_t2 = tk->n_t2;
+  io.noise_c128 = tk->noise_c128;
   io.eom = tk->eom;
   io.h = tk->tau_over_hbar;
   io.ws = ws;
@@ -1424,10 +1430,11 @@ __global__ void __launch_bounds__(256) k_flux_errors(hops_flux_task* tasks, doub
   }
   StageIO io;
   io.zmem = tk->zmem;
-  io.noise1 = reinterpret_cast<const float2*>(tk->z1);
-  io.noise2 = reinterpret_cast<const float2*>(tk->z2);
+  io.noise1 = tk->z1;
+  io.noise2 = tk->z2;
   io.n_t1 = 1;
   io.n_t2 = 1;
+  io.noise_c128 = 0;
   io.it = 0;
   io.stage = 4;
   io.eom = tk->eom;

@@ -42,6 +42,16 @@ def dtypes(prec):
     return torch.complex64, torch.complex64
 
 
+def _noise_pair(noise1, noise2):
+    """Both noises as contiguous tensors of one element type: complex128 when
+    either is complex128 (INTERPOLATE noise), else complex64.  Returns
+    (noise1, noise2, 1 if complex128)."""
+    c128 = any(n is not None and n.dtype == torch.complex128 for n in (noise1, noise2))
+    dt = torch.complex128 if c128 else torch.complex64
+    out = [n.to(dt).contiguous() if n is not None else None for n in (noise1, noise2)]
+    return out[0], out[1], int(c128)
+
+
 def _stream(dev):
     return torch.cuda.current_stream(dev).cuda_stream
 
@@ -116,9 +126,9 @@ class StreamBatch:
         self._pending = False
 
     def set_noise(self, noise1, noise2=None):
-        """noise tensors [B, L, n_t] complex64 on the device (noise2 may be None)."""
-        self.noise1 = noise1.contiguous() if noise1 is not None else None
-        self.noise2 = noise2.contiguous() if noise2 is not None else None
+        """noise tensors [B, L, n_t] on the device, complex64 or (INTERPOLATE)
+        complex128 (noise2 may be None)."""
+        self.noise1, self.noise2, self.cb.noise_c128 = _noise_pair(noise1, noise2)
         self.cb.noise1 = self.noise1.data_ptr() if self.noise1 is not None else None
         self.cb.n_t1 = self.noise1.shape[-1] if self.noise1 is not None else 0
         self.cb.noise2 = self.noise2.data_ptr() if self.noise2 is not None else None
@@ -257,9 +267,8 @@ class ResidentTrajectory:
                 self.zmem[:self.M].cpu().numpy())
 
     def set_noise(self, noise1, noise2=None):
-        """[L, n_t] complex64 device tensors."""
-        self.noise1 = noise1.contiguous() if noise1 is not None else None
-        self.noise2 = noise2.contiguous() if noise2 is not None else None
+        """[L, n_t] device tensors, complex64 or (INTERPOLATE) complex128."""
+        self.noise1, self.noise2, self.noise_c128 = _noise_pair(noise1, noise2)
 
 
 class ResidentRunner:
@@ -301,6 +310,7 @@ class ResidentRunner:
             else:
                 tk.phi = tr.phi.data_ptr()
                 tk.zmem = tr.zmem.data_ptr()
+            tk.noise_c128 = getattr(tr, "noise_c128", 0)
             tk.noise1 = tr.noise1.data_ptr() if tr.noise1 is not None else None
             tk.noise2 = tr.noise2.data_ptr() if tr.noise2 is not None else None
             tk.n_t1 = tr.noise1.shape[-1] if tr.noise1 is not None else 0

@@ -74,7 +74,8 @@ class HopsEnsemble:
             if arr.shape != (self.B, L, n_t):
                 raise UnsupportedRequest("PRE_CALCULATED ensemble noise must be [B, N_L2, n_t]",
                                          "HopsEnsemble", override=True)
-            self.noise = torch.from_numpy(np.ascontiguousarray(arr.astype(np.complex64))).to(self.device)
+            dt = np.complex128 if self.noise_param["INTERPOLATE"] else np.complex64
+            self.noise = torch.from_numpy(np.ascontiguousarray(arr.astype(dt))).to(self.device)
         elif model == "FFT_FILTER":
             seeds = self.seeds if self.seeds is not None else [None] * self.B
             if len(seeds) != self.B:
@@ -84,7 +85,8 @@ class HopsEnsemble:
             alpha = proto._corr()
             raw = np.concatenate([raw_white_noise(s, range(L), n_t, self.noise_param["RAND_MODEL"])
                                   for s in seeds], axis=0)
-            out, _ = filter_on_device(np.tile(alpha, (self.B, 1)), raw, self.device)
+            out, _ = filter_on_device(np.tile(alpha, (self.B, 1)), raw, self.device,
+                                      complex128=bool(self.noise_param["INTERPOLATE"]))
             self.noise = out.reshape(self.B, L, n_t)
         else:
             raise UnsupportedRequest(f"Noise.param[MODEL] {model}", "HopsEnsemble")

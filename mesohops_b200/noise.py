@@ -59,12 +59,12 @@ def raw_white_noise(seed, lops, ntaus, rand_model="SUM_GAUSSIAN"):
     return np.complex64(np.sqrt(-2.0 * np.log(x[:, re])) * np.exp(2.0j * np.pi * x[:, im]))
 
 
-def filter_on_device(alpha, z_raw, device):
+def filter_on_device(alpha, z_raw, device, complex128=False):
     """FP64 circulant-embedding filter on the GPU.
 
     alpha: complex128 [R, n_t] correlation functions; z_raw: complex64
-    [R, 2(n_t-1)].  Returns (complex64 device tensor [R, n_t], number of
-    clipped negative spectral values).
+    [R, 2(n_t-1)].  Returns (complex64 device tensor [R, n_t] -- complex128 if
+    complex128 -- and the number of clipped negative spectral values).
     """
     L = _lib.lib()
     R, n_t = alpha.shape
@@ -72,13 +72,15 @@ def filter_on_device(alpha, z_raw, device):
     a = torch.from_numpy(np.ascontiguousarray(alpha, dtype=np.complex128)).to(dev)
     z = torch.from_numpy(np.ascontiguousarray(z_raw, dtype=np.complex64)).to(dev)
     work = torch.empty(int(L.hops_noise_filter_work_doubles(R, n_t)), dtype=torch.float64, device=dev)
-    out64 = torch.empty((R, n_t), dtype=torch.complex64, device=dev)
+    out = torch.empty((R, n_t), dtype=torch.complex128 if complex128 else torch.complex64,
+                      device=dev)
     nneg = C.c_int64(0)
     stream = torch.cuda.current_stream(dev).cuda_stream
-    rc = L.hops_noise_filter(a.data_ptr(), z.data_ptr(), R, n_t, work.data_ptr(), None,
-                             out64.data_ptr(), C.byref(nneg), stream)
+    rc = L.hops_noise_filter(a.data_ptr(), z.data_ptr(), R, n_t, work.data_ptr(),
+                             out.data_ptr() if complex128 else None,
+                             None if complex128 else out.data_ptr(), C.byref(nneg), stream)
     _lib.check(rc, "hops_noise_filter")
-    return out64, int(nneg.value)
+    return out, int(nneg.value)
 
 
 def window_means(noise, start, k, n_out, real_only=False):
@@ -106,9 +108,13 @@ class HopsNoise:
         if noise_type == 2 and "FLAG_REAL" not in p and p.get("MODEL") != "ZERO":
             p["FLAG_REAL"] = True   # prepare_functions.py:72-77
         self.param = initialize_dict(p, NOISE_DICT_DEFAULT, NOISE_DICT_TYPES, "HopsNoise")
-        if self.param["INTERPOLATE"]:
-            raise UnsupportedRequest("INTERPOLATE = True (cubic noise interpolation)",
-                                     "mesohops_b200 HopsNoise")
+        # INTERPOLATE (hops_noise.py:242-279,379-384): the reference samples a
+        # cubic spline through the correlated noise, and its step check
+        # (hops_trajectory.py:434-447, 579-614) only lets it sample at the
+        # grid times of the noise axis, where the spline returns the samples
+        # themselves; the difference is then only that the samples stay
+        # complex128 instead of being rounded to complex64
+        self.interpolate = bool(self.param["INTERPOLATE"])
         self.system = system
         self.noise_type = noise_type
         n_t = int(np.ceil(self.param["TLEN"] / self.param["TAU"])) + 1
@@ -150,7 +156,8 @@ class HopsNoise:
         return raw_white_noise(seed, range(self.n_lop), self.n_t, self.param["RAND_MODEL"])
 
     def prepare(self, device):
-        """Correlated noise as a complex64 device tensor [n_lop, n_t] (None for ZERO)."""
+        """Correlated noise as a device tensor [n_lop, n_t] (None for ZERO):
+        complex64, or complex128 with INTERPOLATE."""
         if self._dev is not None or self.param["MODEL"] == "ZERO":
             return self._dev
         model = self.param["MODEL"]
@@ -158,14 +165,16 @@ class HopsNoise:
             z = self._uncorrelated()
             if self.param["STORE_RAW_NOISE"]:
                 self.param["Z_UNCORRELATED"] = z
-            noise, self.n_clipped = filter_on_device(self._corr(), z, device)
+            noise, self.n_clipped = filter_on_device(self._corr(), z, device,
+                                                     complex128=self.interpolate)
         elif model == "PRE_CALCULATED":
             seed = self.param["SEED"]
             if isinstance(seed, str):
                 if not os.path.isfile(seed) or seed[-4:] != ".npy":
                     raise UnsupportedRequest(f"Noise.param[SEED] {seed} is not a valid .npy "
                                              "file", "Noise.prepare_noise", True)
-                seed = np.load(seed)
+                # a file's samples are complex64 (hops_noise.py:287)
+                seed = np.complex64(np.load(seed))
             if not isinstance(seed, (list, np.ndarray)):
                 raise UnsupportedRequest(f"Noise.param[SEED] of type {type(seed)}",
                                          "Noise.prepare_noise")
@@ -173,7 +182,8 @@ class HopsNoise:
             if seed.shape != (self.n_lop, self.n_t):
                 raise UnsupportedRequest("Noise.param[SEED] is an array of the wrong length",
                                          "Noise.prepare_noise", True)
-            noise = torch.from_numpy(np.ascontiguousarray(seed.astype(np.complex64))).to(device)
+            dt = np.complex128 if self.interpolate else np.complex64
+            noise = torch.from_numpy(np.ascontiguousarray(seed.astype(dt))).to(device)
         else:
             raise UnsupportedRequest(f"Noise.param[MODEL] {model}", "Noise.prepare_noise")
         if self.param["FLAG_REAL"]:
@@ -188,6 +198,9 @@ class HopsNoise:
         the RK slots of step n are windows 2n, 2n+1, 2n+2.  None for ZERO noise."""
         if self._dev is None:
             return None
+        if self.interpolate:
+            raise UnsupportedRequest("EFFECTIVE_NOISE_INTEGRATION with INTERPOLATE noise",
+                                     "mesohops_b200 HopsNoise")
         k = int(round(tau * 0.5 / self.param["TAU"]))
         start = self.time_index(t0)
         n_out = 2 * int(n_steps) + 1
@@ -210,14 +223,16 @@ class HopsNoise:
         return it
 
     def get_noise(self, t_axis, list_lop=None):
-        """complex64 [len(list_lop), len(t_axis)] samples (hops_noise.py:339-451)."""
+        """[len(list_lop), len(t_axis)] samples (hops_noise.py:339-451):
+        complex64, or complex128 with INTERPOLATE."""
         if list_lop is None:
             list_lop = np.arange(self.n_lop)
+        dt = np.complex128 if self.interpolate else np.complex64
         if self.param["MODEL"] == "ZERO":
-            return np.zeros((len(list_lop), len(t_axis)), dtype=np.complex64)
+            return np.zeros((len(list_lop), len(t_axis)), dtype=dt)
         if self._dev is None:
             self.prepare("cuda")
         h = self.host()
         idx = [self.time_index(t) for t in t_axis]
         return np.ascontiguousarray(h[np.ix_(np.asarray(list_lop, dtype=np.int64), idx)],
-                                    dtype=np.complex64)
+                                    dtype=dt)

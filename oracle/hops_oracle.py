@@ -313,9 +313,11 @@ def normalize(phi, nstate):
     return phi / np.sqrt(np.sum(np.abs(phi[:nstate]) ** 2))
 
 
-def noise_lookup(noise, t_list, tau_noise):
-    """Exact time lookup + complex64 result.  noise/hops_noise.py:437-451,796-825"""
-    out = np.zeros((noise.shape[0], len(t_list)), dtype=np.complex64)
+def noise_lookup(noise, t_list, tau_noise, dtype=np.complex64):
+    """Exact time lookup + complex64 result.  noise/hops_noise.py:437-451,796-825
+    (dtype complex128: INTERPOLATE noise, the cubic spline of hops_noise.py:
+    242-265,379-384 at its own sample times)"""
+    out = np.zeros((noise.shape[0], len(t_list)), dtype=dtype)
     for i, t in enumerate(t_list):
         it = int(round(t / tau_noise))
         if abs(it * tau_noise - t) >= PRECISION:
@@ -339,7 +341,7 @@ def effective_noise(noise, t, tau, tau_noise, real=False):
 
 
 def propagate(basis, psi0, noise1, tau_noise, t_max, dt, noise2=None,
-              eom="NORMALIZED NONLINEAR", effective=False):
+              eom="NORMALIZED NONLINEAR", effective=False, noise_dtype=np.complex64):
     """Run the non-adaptive trajectory loop; returns (t_axis, psi_traj, phi, zmem).
 
     trajectory/hops_trajectory.py:253-336 (phi_0 = [psi_0, 0 ...], z_mem = 0)
@@ -362,8 +364,8 @@ def propagate(basis, psi0, noise1, tau_noise, t_max, dt, noise2=None,
             zr2 = effective_noise(noise2, t, dt, tau_noise)
         else:
             tl = [t, t + dt * 0.5, t + dt]
-            zr = noise_lookup(noise1, tl, tau_noise)
-            zr2 = noise_lookup(noise2, tl, tau_noise)
+            zr = noise_lookup(noise1, tl, tau_noise, noise_dtype)
+            zr2 = noise_lookup(noise2, tl, tau_noise, noise_dtype)
         phi, zmem = rk4_step(basis, phi, zmem, zr, zr2, dt, eom)
         if eom == "NORMALIZED NONLINEAR":
             phi = normalize(phi, S)

@@ -13,6 +13,7 @@ files committed next to this script; the GPU box never needs the reference.
     python tests/golden/make_golden.py --effective-adaptive  # effective noise, adaptive basis
     python tests/golden/make_golden.py --bench-configs  # the benchmark's ring20 / chain10
     python tests/golden/make_golden.py --static-basis   # STATIC_BASIS, adaptive
+    python tests/golden/make_golden.py --interpolate    # INTERPOLATE noise
 
 Each fixture records the inputs (system, hierarchy depth, noise arrays, psi_0,
 time step) together with the reference outputs (psi_traj, derivative values,
@@ -451,6 +452,50 @@ def main_adaptive():
                      delta, delta, noise_seed=seed)
 
 
+def run_interpolate(name, sysp, depth, psi0, t_max, dt, noise_seed, eom):
+    """INTERPOLATE noise: a complex128 SEED array through the reference's cubic
+    spline (hops_noise.py:255-265), sampled at the step times."""
+    tau_noise = dt / 2.0
+    tlen = t_max + dt
+    n_t = int(np.ceil(tlen / tau_noise)) + 1
+    nl = n_unique(sysp)
+    rng = np.random.default_rng(noise_seed)
+    noise = (rng.normal(size=(nl, n_t)) + 1j * rng.normal(size=(nl, n_t))) * 40.0
+    hops = HopsTrajectory(sysp, noise_param={"SEED": noise, "MODEL": "PRE_CALCULATED",
+                                             "TLEN": float(tlen), "TAU": float(tau_noise),
+                                             "INTERPOLATE": True},
+                          hierarchy_param={"MAXHIER": depth},
+                          eom_param={"EQUATION_OF_MOTION": eom}, storage_param={})
+    quiet(hops.initialize, psi0)
+    quiet(hops.propagate, t_max, dt)
+    H = sysp["HAMILTONIAN"]
+    H = H.toarray() if sps.issparse(H) else np.asarray(H)
+    np.savez_compressed(
+        os.path.join(HERE, name + ".npz"),
+        H=np.array(H, dtype=np.complex128), G=np.array([g for g, w in sysp["GW_SYSBATH"]]),
+        W=np.array([w for g, w in sysp["GW_SYSBATH"]]), L=dense_lops(sysp), depth=depth,
+        psi0=np.array(psi0, dtype=np.complex128), t_max=t_max, dt=dt, tau_noise=tau_noise,
+        tlen=tlen, noise1=noise, eom=eom, psi_traj=np.array(hops.storage.data["psi_traj"]),
+        n_hier=hops.n_hier, n_state=hops.n_state)
+    print(name, "steps", len(hops.storage.data["psi_traj"]) - 1)
+
+
+def main_interpolate():
+    n = 6
+    rng = np.random.default_rng(2)
+    H = np.diag(rng.uniform(-100, 100, n))
+    for i in range(n):
+        H[i, (i + 1) % n] = H[(i + 1) % n, i] = 80.0
+    psi0 = np.zeros(n, dtype=np.complex128)
+    psi0[0] = 1.0
+    run_interpolate("interp_ring6", site_system(H, [(60, 60, 295)]), 3, psi0, 100.0, 4.0,
+                    noise_seed=71, eom="NORMALIZED NONLINEAR")
+    H = np.array([[0, 50], [50, 0.0]])
+    run_interpolate("interp_dimer_linear", site_system(H, [(50, 50, 295)]), 3,
+                    np.array([1, 0], dtype=np.complex128), 100.0, 4.0, noise_seed=72,
+                    eom="LINEAR")
+
+
 def main_static_basis():
     """Adaptive basis with integration_param STATIC_BASIS (states and aux joined
     to the initial basis, hops_trajectory.py:293-316), with the INCH_WORM early
@@ -674,6 +719,8 @@ if __name__ == "__main__":
         main_bench_configs()
     elif "--static-basis" in sys.argv:
         main_static_basis()
+    elif "--interpolate" in sys.argv:
+        main_interpolate()
     elif "--dyadic" in sys.argv:
         main_dyadic()
     elif "--effective-adaptive" in sys.argv:
