@@ -150,7 +150,7 @@ def _read(ptr, n, dtype):
 
     class Dev:
         __cuda_array_interface__ = {"shape": (n,), "typestr": np.dtype(dtype).str,
-                                    "data": (int(ptr), True), "version": 3}
+                                    "data": (int(ptr), False), "version": 3}
     return torch.as_tensor(Dev(), device="cuda").cpu().numpy()
 
 
