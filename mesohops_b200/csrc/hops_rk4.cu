@@ -382,8 +382,15 @@ constexpr size_t wide_smem_bytes(int warps) {
 // steps at the register counts the wider tasks take).
 constexpr int wide_threads(int nb) { return nb <= 2 ? 256 : 128; }
 
+// Resident CTAs per SM of a shape.  With FP64 arithmetic the NB = 2 task holds
+// twice the complex accumulators of the single-precision one: at 4 CTAs (64
+// registers) it spilled; 3 CTAs leave it 85 registers.
+constexpr int wide_min_blocks(int nb, int rbytes) {
+  return nb == 1 ? 4 : (nb == 2 ? (rbytes == 8 ? 3 : 4) : (nb == 4 ? HOPS_WIDE_MIN_BLOCKS4 : 2));
+}
+
 template <typename R, typename ST, typename PT, bool SITE, int NB, bool LT>
-__global__ void __launch_bounds__(wide_threads(NB), NB <= 2 ? 4 : (NB == 4 ? HOPS_WIDE_MIN_BLOCKS4 : 2))
+__global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R)))
     k_wide(hops_structure st, int B, int stage, double h, const ST* __restrict__ yin,
            ST* __restrict__ yout, PT* phi, ST* shadow, ST* acc, const double* __restrict__ ws,
            FastDiv divS, FastDiv divAS, int chunk_major) {
