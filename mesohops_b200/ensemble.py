@@ -118,6 +118,14 @@ class HopsEnsemble:
         di = int(round(tau * 0.5 / tau_noise))
         return n, it0, di
 
+    def tune(self, tau):
+        """Run the stage-kernel autotuner for steps of tau now (it restores the
+        state), so that a later propagate call carries no tuning runs."""
+        _, it0, di = self.steps_for(tau, tau)
+        if self.autotune and not self._tuned:
+            self.batch.autotune(it0, di, tau / hbar)
+            self._tuned = True
+
     def propagate(self, t_advance, tau, psi_out=None):
         """Propagate all trajectories; psi_out: optional device tensor [n, B, S] c128."""
         n, it0, di = self.steps_for(t_advance, tau)
