@@ -116,6 +116,10 @@ typedef struct hops_structure {
   const int32_t* l2_ptr;  /* [n_lop * (n_state+1)] CSR of L_j^2 */
   const int32_t* l2_col;
   const double* l2_val;   /* complex */
+  /* every aux a >= n_up_prefix has no up connection (0: not known); task
+     order 3 of the batched stage kernel runs the aux below it state by state */
+  int32_t n_up_prefix;
+  int32_t reserved;
 } hops_structure;
 
 /*
@@ -312,10 +316,13 @@ int hops_noise_window_mean(const float* noise_dev, int64_t rows, int32_t n_t, in
                            void* stream);
 
 /*
- * Shape of the batched stage kernel: 32*nb trajectories per warp task and
- * chunk-major task order (1) or not (0); nb = 0 / chunk_major = -1 restore the
- * automatic choice.  Process-wide setting used by the autotuner; has no
- * counterpart in the reference.
+ * Shape of the batched stage kernel: 32*nb trajectories per warp task and the
+ * task order: 0 = (aux, state) with the trajectory chunks innermost, 1 = chunk
+ * outermost, 2 = chunk outermost then state, aux innermost, 3 = chunk
+ * outermost, then the aux below n_up_prefix state by state, then the rest in
+ * (aux, state) order; nb = 0 / chunk_major = -1 restore the automatic choice.
+ * Process-wide setting used by the autotuner; has no counterpart in the
+ * reference.
  */
 int hops_stage_tuning(int32_t nb, int32_t chunk_major);
 

@@ -41,6 +41,7 @@ class HopsStructure(C.Structure):
         ("dn_coef_site", _p), ("dn_coef_site_f", _p),
         ("up_site", _p), ("dn_site", _p), ("h_diag", _p),
         ("lt_coef", _p), ("l2_ptr", _p), ("l2_col", _p), ("l2_val", _p),
+        ("n_up_prefix", _i), ("reserved", _i),
     ]
 
 

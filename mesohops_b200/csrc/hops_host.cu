@@ -238,9 +238,10 @@ extern "C" int hops_structure_upload(const hops_structure_desc* d, void* stream,
   // ---- aux tables
   std::vector<cd> k_decay(N, cd(0.0, 0.0)), dn_coef(n_dn), dn_coef_site(n_dn);
   std::vector<int32_t> up_site(n_up), dn_site(n_dn), first_of_mode(M, -1);
-  int max_up = 0, max_dn = 0;
+  int max_up = 0, max_dn = 0, n_up_prefix = 0;
   for (int a = 0; a < N; ++a) {
     max_up = std::max(max_up, d->up_ptr[a + 1] - d->up_ptr[a]);
+    if (d->up_ptr[a + 1] > d->up_ptr[a]) n_up_prefix = a + 1;
     max_dn = std::max(max_dn, d->dn_ptr[a + 1] - d->dn_ptr[a]);
     cd s(0.0, 0.0);
     for (int p = d->dn_ptr[a]; p < d->dn_ptr[a + 1]; ++p) s += (double)d->dn_k[p] * W[d->dn_mode[p]];
@@ -315,6 +316,7 @@ extern "C" int hops_structure_upload(const hops_structure_desc* d, void* stream,
   st.site_projector = is_site ? 1 : 0;
   st.max_up = max_up;
   st.max_dn = max_dn;
+  st.n_up_prefix = n_up_prefix;
 #define AT(T, o) reinterpret_cast<T>(base + (o))
   st.k_decay = AT(const double*, o_kd);
   st.k_decay_f = AT(const float*, o_kdf);

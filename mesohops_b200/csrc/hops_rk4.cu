@@ -233,6 +233,14 @@ struct FastDiv {
 };
 
 // ----------------------------------------------------------- stage update ----
+// L2 eviction priorities of the batched stage kernel (HOPS_WIDE_HINTS bit 0:
+// the read-once streams -- phi, acc and the stage outputs -- evict-first;
+// bit 1: the stage input Y, which the neighbour gathers re-read, evict-last).
+// Bit 0 alone is the default: on the 20-site ring it took 5 % off the
+// complex128 stage (3 % mixed, none complex64); bit 1 gained nothing more.
+#ifndef HOPS_WIDE_HINTS
+#define HOPS_WIDE_HINTS 1
+#endif
 // RK4 bookkeeping of one element (integrator_rk.py:66-73).  ph: the state at
 // the start of the step (already scaled) in the state type PT; k in the
 // arithmetic type T; acc, the stage inputs and phi's complex64 copy stored in
@@ -250,6 +258,13 @@ __device__ __forceinline__ ST acc_load(const ST* p) {
 template <bool GHINT, typename ST>
 __device__ __forceinline__ void acc_store(ST* p, ST v) {
   if constexpr (GHINT) __stcs(p, v);
+  else *p = v;
+}
+// store of a stage output or the new state (evict-first when OHINT: the
+// batched stage kernel with HOPS_WIDE_HINTS bit 0)
+template <bool OHINT, typename V>
+__device__ __forceinline__ void out_store(V* p, V v) {
+  if constexpr (OHINT) __stcs(p, v);
   else *p = v;
 }
 
@@ -271,7 +286,7 @@ __device__ __forceinline__ double* psum_im(void* shadow) { return static_cast<do
 // (accv; read at stages 1-3 only), so that a caller can load the operands of
 // several elements before it stores any of them.  PSUM: the partial-sum form
 // above (the caller passes P as ph at the fourth stage).
-template <bool GHINT, bool PSUM, typename T, typename ST, typename PT>
+template <bool GHINT, bool PSUM, typename T, typename ST, typename PT, bool OHINT = false>
 __device__ __forceinline__ void rk_finish(int stage, double h, T k, PT ph, ST accv, ST* acc,
                                           ST* yout, PT* phi, ST* shadow, size_t e) {
   using RP = decltype(ph.x);
@@ -285,7 +300,7 @@ __device__ __forceinline__ void rk_finish(int stage, double h, T k, PT ph, ST ac
       const PT pp = cadd(ph, hs);
       __stcs(psum_re(acc) + e, (double)pp.x);
       __stcs(psum_im(shadow) + e, (double)pp.y);
-      yout[e] = cv<ST>(cadd(ph, cscale(cv<PT>(k), hh)));
+      out_store<OHINT>(yout + e, cv<ST>(cadd(ph, cscale(cv<PT>(k), hh))));
       return;
     }
     if (stage == 3) {
@@ -293,22 +308,22 @@ __device__ __forceinline__ void rk_finish(int stage, double h, T k, PT ph, ST ac
       hs.x = hs.x / (RP)6;
       hs.y = hs.y / (RP)6;
       const PT nw = cadd(ph, hs);
-      phi[e] = nw;
-      shadow[e] = cv<ST>(nw);
+      out_store<OHINT>(phi + e, nw);
+      out_store<OHINT>(shadow + e, cv<ST>(nw));
       return;
     }
   }
   switch (stage) {
     case 0: {
       acc_store<GHINT>(acc + e, cv<ST>(k));
-      yout[e] = cv<ST>(cadd(ph, cscale(cv<PT>(k), hh * (RP)0.5)));
+      out_store<OHINT>(yout + e, cv<ST>(cadd(ph, cscale(cv<PT>(k), hh * (RP)0.5))));
     } break;
     case 1:
     case 2: {
       const T a0 = cv<T>(accv);
       acc_store<GHINT>(acc + e, cv<ST>(cadd(a0, cscale(k, (decltype(k.x))2))));
       const RP c = stage == 1 ? hh * (RP)0.5 : hh;
-      yout[e] = cv<ST>(cadd(ph, cscale(cv<PT>(k), c)));
+      out_store<OHINT>(yout + e, cv<ST>(cadd(ph, cscale(cv<PT>(k), c))));
     } break;
     case 3: {
       PT sum = cv<PT>(cadd(cv<T>(accv), k));
@@ -316,11 +331,11 @@ __device__ __forceinline__ void rk_finish(int stage, double h, T k, PT ph, ST ac
       hs.x = hs.x / (RP)6;
       hs.y = hs.y / (RP)6;
       const PT nw = cadd(ph, hs);
-      phi[e] = nw;
-      if (shadow) shadow[e] = cv<ST>(nw);
+      out_store<OHINT>(phi + e, nw);
+      if (shadow) out_store<OHINT>(shadow + e, cv<ST>(nw));
     } break;
     default:
-      yout[e] = cv<ST>(k);
+      out_store<OHINT>(yout + e, cv<ST>(k));
   }
 }
 
@@ -329,6 +344,31 @@ __device__ __forceinline__ void rk_update(int stage, double h, T k, PT ph, ST* a
                                           PT* phi, ST* shadow, size_t e) {
   const ST accv = (stage >= 1 && stage <= 3) ? acc_load<GHINT>(acc + e) : ST{};
   rk_finish<GHINT, false, T, ST, PT>(stage, h, k, ph, accv, acc, yout, phi, shadow, e);
+}
+
+// L2 cache policies for the hints above.
+__device__ __forceinline__ unsigned long long policy_evict_first() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ unsigned long long policy_evict_last() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+// load of one stage-vector element with an L2 cache policy
+__device__ __forceinline__ double2 ld_pol(const double2* p, unsigned long long pol) {
+  double2 v;
+  asm volatile("ld.global.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;\n"
+               : "=d"(v.x), "=d"(v.y) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float2 ld_pol(const float2* p, unsigned long long pol) {
+  float2 v;
+  asm volatile("ld.global.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;\n"
+               : "=f"(v.x), "=f"(v.y) : "l"(p), "l"(pol));
+  return v;
 }
 
 // Asynchronous global -> shared copies (cp.async, no register staging).
@@ -343,6 +383,18 @@ __device__ __forceinline__ void cp_async(void* sdst, const void* gsrc) {
 }
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+// the same with an L2 cache policy
+template <int BYTES>
+__device__ __forceinline__ void cp_async_pol(void* sdst, const void* gsrc,
+                                             unsigned long long pol) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;\n"
+                 ::"r"(d), "l"(gsrc), "l"(pol) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], %2, %3;\n"
+                 ::"r"(d), "l"(gsrc), "n"(BYTES), "l"(pol) : "memory");
 }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -362,10 +414,24 @@ constexpr size_t wide_smem_bytes(int warps) {
 // Connection lists, coefficients and the site test are warp-uniform and loaded
 // once per neighbour for the whole chunk; every Y load is a coalesced
 // 32-trajectory segment and the NB loads per neighbour are in flight together.
-// chunk_major: the chunk is the outermost task index, so the warps in flight
-// all gather from one chunk's slice of Y, which stays resident in L2 (a slice
-// of 32 trajectories of the 20-site ring is 54 MB in complex64); otherwise each
-// warp walks every chunk of its (a, s).
+// chunk_major (the task order):
+//   0  tasks (a, s), s fastest; each warp walks every chunk of its (a, s);
+//   1  the chunk is the outermost task index, so the warps in flight all
+//      gather from one chunk's slice of Y (a slice of 32 trajectories of the
+//      20-site ring is 54 MB in complex64);
+//   2  chunk outermost, then the state s, the aux a fastest.  With site
+//      projectors an item (a, s) gathers only rows (a +- e_k, s) and the
+//      H-neighbour rows (a, s'), so the warps in flight touch a few state
+//      slices of one chunk (10626 aux x 128 trajectories x 16 B = 22 MB each
+//      on the 20-site ring): the up-gathers, which re-read every leaf row up
+//      to four times, hit L2; the H-neighbour rows, adjacent in memory in
+//      order 0, are read again one slice later;
+//   3  chunk outermost, then the aux below st.n_up_prefix (those with up
+//      connections) in order 2, then the others in order 0.  The gathers of
+//      the interior aux run state by state against one slice of the leaf rows
+//      (8855 leaves x 2 KB = 18 MB per state on the 20-site ring), while the
+//      leaves, 83 % of the items, keep the sequential (aux, state) streaming
+//      and their H rows' locality.
 // The stage is bound by load latency at the occupancy registers allow.  NB <= 2
 // is held to 64 registers (4 CTAs of 256 threads, 32 warps per SM), NB = 4 to
 // 128 (4 CTAs of 128 threads); both measured faster than the registers the
@@ -393,7 +459,8 @@ template <typename R, typename ST, typename PT, bool SITE, int NB, bool LT>
 __global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R)))
     k_wide(hops_structure st, int B, int stage, double h, const ST* __restrict__ yin,
            ST* __restrict__ yout, PT* phi, ST* shadow, ST* acc, const double* __restrict__ ws,
-           FastDiv divS, FastDiv divAS, int chunk_major) {
+           FastDiv divS, FastDiv divAS, FastDiv divH, FastDiv divP, unsigned n_pre_s,
+           int chunk_major) {
   using P = Prec<R>;
   using T = typename P::T;
   const int S = st.n_state;
@@ -413,6 +480,25 @@ __global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R
   // A work item is one (task, chunk).  The streamed operands of the warp's
   // next item are copied into shared memory while the current item gathers
   // its neighbours, so no item waits for its own DRAM reads.
+  [[maybe_unused]] const unsigned long long pol_stream = policy_evict_first();
+  [[maybe_unused]] const unsigned long long pol_keep = policy_evict_last();
+  auto yl = [&](size_t i) -> ST {
+    if constexpr ((HOPS_WIDE_HINTS & 2) != 0) return ld_pol(yin + i, pol_keep);
+    else return yin[i];
+  };
+  // row index a * S + s of task t in chunk ci
+  auto task_as = [&](unsigned t, unsigned ci) -> unsigned {
+    const unsigned r = chunk_major ? t - ci * n_as : t;
+    if (chunk_major == 2) {
+      const unsigned sm = divH.div(r);
+      return (r - sm * (unsigned)st.n_hier) * (unsigned)S + sm;
+    }
+    if (chunk_major == 3 && r < n_pre_s) {  // divP divides by the prefix length
+      const unsigned sm = divP.div(r);
+      return (r - sm * divP.d) * (unsigned)S + sm;
+    }
+    return r;
+  };
   extern __shared__ __align__(16) unsigned char wide_smem[];
   const int nwb = blockDim.x >> 5;
   const int wib = threadIdx.x >> 5;
@@ -427,16 +513,22 @@ __global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R
   const bool want_phi = stage != 4 && !want_psum;
   const bool want_acc = stage >= 1 && stage <= 3 && !want_psum;
   auto prefetch = [&](unsigned t, unsigned ci, int buf) {
-    const unsigned as = chunk_major ? t - ci * n_as : t;
+    const unsigned as = task_as(t, ci);
     const size_t row = (size_t)as * B;
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
       const int b = (int)ci * CH + lane + 32 * j;
       if (b < B) {
         const int o = buf * CH + lane + 32 * j;
-        cp_async<sizeof(ST)>(ys_s + o, yin + row + b);
-        if (want_phi) cp_async<sizeof(PT)>(ph_s + o, phi + row + b);
-        if (want_acc) cp_async<sizeof(ST)>(ac_s + o, acc + row + b);
+        if constexpr ((HOPS_WIDE_HINTS & 2) != 0) cp_async_pol<sizeof(ST)>(ys_s + o, yin + row + b, pol_keep);
+        else cp_async<sizeof(ST)>(ys_s + o, yin + row + b);
+        if constexpr ((HOPS_WIDE_HINTS & 1) != 0) {
+          if (want_phi) cp_async_pol<sizeof(PT)>(ph_s + o, phi + row + b, pol_stream);
+          if (want_acc) cp_async_pol<sizeof(ST)>(ac_s + o, acc + row + b, pol_stream);
+        } else {
+          if (want_phi) cp_async<sizeof(PT)>(ph_s + o, phi + row + b);
+          if (want_acc) cp_async<sizeof(ST)>(ac_s + o, acc + row + b);
+        }
         if constexpr (PSUM) {
           if (want_psum) {
             double* pd = reinterpret_cast<double*>(ph_s + o);
@@ -462,7 +554,7 @@ __global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R
     if (tn < ntask) prefetch(tn, cn, buf ^ 1);
     cp_async_commit();  // one group per item, empty past the last one
 
-    const unsigned as = chunk_major ? t - ci * n_as : t;
+    const unsigned as = task_as(t, ci);
     const int a = (int)divS.div(as);
     const int s = (int)as - a * S;
     const size_t rowa = (size_t)as * B;
@@ -499,7 +591,7 @@ __global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R
 #pragma unroll
           for (int j = 0; j < NB; ++j)
             if (ok[j])
-              k[j] = cfma(cmul(czT[(size_t)jl * B + bg + lane + 32 * j], lv), cv<T>(yin[rb + 32 * j]), k[j]);
+              k[j] = cfma(cmul(czT[(size_t)jl * B + bg + lane + 32 * j], lv), cv<T>(yl(rb + 32 * j)), k[j]);
         }
       }
     }
@@ -508,7 +600,7 @@ __global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R
       const size_t rb = ((size_t)a * S + st.h_col[q]) * B + bg + lane;
 #pragma unroll
       for (int j = 0; j < NB; ++j)
-        if (ok[j]) k[j] = cfma(hv, cv<T>(yin[rb + 32 * j]), k[j]);
+        if (ok[j]) k[j] = cfma(hv, cv<T>(yl(rb + 32 * j)), k[j]);
     }
     int p0 = u0;
     if (SITE) {
@@ -524,8 +616,8 @@ __global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R
 #pragma unroll
         for (int j = 0; j < NB; ++j) {
           if (ok[j]) {
-            ya[j] = yin[ra + 32 * j];
-            yb[j] = yin[rb + 32 * j];
+            ya[j] = yl(ra + 32 * j);
+            yb[j] = yl(rb + 32 * j);
           }
         }
         const T* upa = upcT + (size_t)ma * B + bg + lane;
@@ -550,11 +642,11 @@ __global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R
         const T corr = hit ? P::gwv(st, m) : czero<T>();
 #pragma unroll
         for (int j = 0; j < NB; ++j)
-          if (ok[j]) k[j] = cfma(csub(up[32 * j], corr), cv<T>(yin[rb + 32 * j]), k[j]);
+          if (ok[j]) k[j] = cfma(csub(up[32 * j], corr), cv<T>(yl(rb + 32 * j)), k[j]);
       } else {
 #pragma unroll
         for (int j = 0; j < NB; ++j)
-          if (ok[j]) k[j] = cfma(up[32 * j], cv<T>(yin[rb + 32 * j]), k[j]);
+          if (ok[j]) k[j] = cfma(up[32 * j], cv<T>(yl(rb + 32 * j)), k[j]);
         const int base = st.mode_lop[m] * (S + 1);
         const int q0 = st.l_ptr[base + s], q1 = st.l_ptr[base + s + 1];
         for (int q = q0; q < q1; ++q) {
@@ -562,7 +654,7 @@ __global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R
           const size_t rb2 = ((size_t)u * S + st.l_col[q]) * B + bg + lane;
 #pragma unroll
           for (int j = 0; j < NB; ++j)
-            if (ok[j]) k[j] = csub(k[j], cmul(lv, cv<T>(yin[rb2 + 32 * j])));
+            if (ok[j]) k[j] = csub(k[j], cmul(lv, cv<T>(yl(rb2 + 32 * j))));
         }
       }
     }
@@ -574,7 +666,7 @@ __global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R
         const size_t rb = ((size_t)d * S + s) * B + bg + lane;
 #pragma unroll
         for (int j = 0; j < NB; ++j)
-          if (ok[j]) k[j] = cfma(cf, cv<T>(yin[rb + 32 * j]), k[j]);
+          if (ok[j]) k[j] = cfma(cf, cv<T>(yl(rb + 32 * j)), k[j]);
       } else {
         const int d = st.dn_aux[p], m = st.dn_mode[p];
         const int base = st.mode_lop[m] * (S + 1);
@@ -584,7 +676,7 @@ __global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R
           const size_t rb = ((size_t)d * S + st.lh_col[q]) * B + bg + lane;
 #pragma unroll
           for (int j = 0; j < NB; ++j)
-            if (ok[j]) k[j] = cfma(cf, cv<T>(yin[rb + 32 * j]), k[j]);
+            if (ok[j]) k[j] = cfma(cf, cv<T>(yl(rb + 32 * j)), k[j]);
         }
       }
     }
@@ -614,7 +706,8 @@ __global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R
       }
       // P was formed from the scaled state: no scale at the partial-sum stage
       const PT p = stage == 4 ? PT{} : (want_psum ? ph[j] : cscale(ph[j], (decltype(PT{}.x))sc[j]));
-      rk_finish<true, PSUM, T, ST, PT>(stage, h, kk, p, accv[j], acc, yout, phi, shadow, e);
+      rk_finish<true, PSUM, T, ST, PT, (HOPS_WIDE_HINTS & 1) != 0>(stage, h, kk, p, accv[j], acc,
+                                                                  yout, phi, shadow, e);
     }
     t = tn;
     ci = cn;
@@ -1074,6 +1167,8 @@ static int g_tune_nb = 0, g_tune_cm = -1;
 extern "C" int hops_stage_tuning(int32_t nb, int32_t chunk_major) {
   if (nb != 0 && nb != 1 && nb != 2 && nb != 4 && nb != 8)
     return set_err(HOPS_EINVAL, "nb must be 0 (auto), 1, 2, 4 or 8");
+  if (chunk_major < -1 || chunk_major > 3)
+    return set_err(HOPS_EINVAL, "task order must be -1 (auto) or 0 .. 3");
   g_tune_nb = nb;
   g_tune_cm = chunk_major;
   return HOPS_OK;
@@ -1085,9 +1180,30 @@ static void launch_wide_lt(const hops_structure* st, int B, int stage, double h,
                            int chunk_major, cudaStream_t s) {
   const unsigned n_as = (unsigned)st->n_hier * st->n_state;
   const long nchunk = (B + 32 * NB - 1) / (32 * NB);
+  // prefix of aux with up connections (order 3); 0 leaves order 3 = order 1
+  const int n_pre = st->n_up_prefix > 0 && st->n_up_prefix <= st->n_hier ? st->n_up_prefix : 0;
   constexpr int threads = wide_threads(NB);
-  const int grid = (256 / threads) * grid_for_warps(chunk_major ? (long)n_as * nchunk : (long)n_as);
   constexpr size_t smem = wide_smem_bytes<ST, PT, NB>(threads / 32);
+  // One wave: every CTA is resident from the start, so the warps in flight
+  // work on one contiguous window of the task order (with more CTAs than fit,
+  // the first wave's warps would stride over the whole task range and no task
+  // order would keep a slice of Y in L2).  On the 20-site ring this alone
+  // took 5 % off the complex128 stage against 8 waves of grid-stride CTAs.
+  static int resident = 0;
+  if (resident == 0) {
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(k_wide<R, ST, PT, SITE, NB, LT>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_wide<R, ST, PT, SITE, NB, LT>,
+                                                      threads, smem) != cudaSuccess || nb < 1)
+      nb = 1;
+    resident = nb;
+  }
+  const long task_warps = chunk_major ? (long)n_as * nchunk : (long)n_as;
+  long gl = (task_warps * 32 + threads - 1) / threads;
+  if (gl > (long)sm_count() * resident) gl = (long)sm_count() * resident;
+  const int grid = (int)(gl < 1 ? 1 : gl);
   if (smem > 48 * 1024) {
     // opt in to the large shared-memory carve-out once per device
     static int set_for = -1;
@@ -1101,7 +1217,8 @@ static void launch_wide_lt(const hops_structure* st, int B, int stage, double h,
   }
   k_wide<R, ST, PT, SITE, NB, LT><<<grid, threads, smem, s>>>(
       *st, B, stage, h, (const ST*)yin, (ST*)yout, (PT*)phi, (ST*)shadow, (ST*)acc, ws,
-      FastDiv((unsigned)st->n_state), FastDiv(n_as), chunk_major);
+      FastDiv((unsigned)st->n_state), FastDiv(n_as), FastDiv((unsigned)st->n_hier),
+      FastDiv(n_pre > 0 ? (unsigned)n_pre : 1u), (unsigned)n_pre * st->n_state, chunk_major);
 }
 
 // The low-temperature term is a separate instantiation: the check alone in the
@@ -1125,12 +1242,13 @@ static void launch_stage(const hops_structure* st, int B, int stage, double h, c
   (void)status;
   if (B >= 32) {
     const int nbmax = (B + 31) / 32;
-    // auto (measured on the 20-site ring, 128 trajectories): 128 trajectories
-    // per warp task with FP32 arithmetic, 64 with FP64 arithmetic, natural
-    // task order; the autotuner overrides this per problem class
-    int cm = g_tune_cm >= 0 ? g_tune_cm : 0;
+    // auto (measured on the 20-site ring, 128 trajectories, every precision):
+    // 128 trajectories per warp task, the interior aux state by state
+    // (order 3) when the structure names its up-connected prefix; the
+    // autotuner overrides this per problem class
+    int cm = g_tune_cm >= 0 ? g_tune_cm : (st->n_up_prefix > 0 ? 3 : 0);
     int nb = g_tune_nb;
-    if (nb == 0) nb = sizeof(typename Prec<R>::T) == 8 ? 4 : 2;
+    if (nb == 0) nb = 4;
     if (nb > nbmax) nb = nbmax >= 4 ? 4 : (nbmax >= 2 ? 2 : 1);
     if (nb > 8) nb = 8;
     if (nb == 1) launch_wide<R, ST, PT, SITE, 1>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, cm, s);

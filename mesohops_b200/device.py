@@ -110,6 +110,7 @@ def build_tables(system, basis, state_list=None, mode_list=None, small=None):
         up_site=np.asarray(up_site, dtype=np.int32), dn_site=np.asarray(dn_site, dtype=np.int32),
         max_up=int(up_counts.max()) if len(up_counts) else 0,
         max_dn=int(dn_counts.max()) if len(dn_counts) else 0,
+        n_up_prefix=int(np.flatnonzero(up_counts)[-1]) + 1 if np.any(up_counts) else 0,
     )
     return small
 
@@ -233,6 +234,7 @@ def build_tables_triangular(system, depth, device):
         up_site=mode_site[up_mode.to(torch.int64)].to(torch.int32),
         dn_site=mode_site[dnm].to(torch.int32),
         max_up=M if n_below > 0 else 0, max_dn=min(D, M) if N > 1 else 0,
+        n_up_prefix=int(n_below),
     )
     return small
 
@@ -318,6 +320,7 @@ class DeviceStructure:
         s.n_dn = len(t["dn_aux"])
         s.site_projector = t["site_projector"]
         s.max_up, s.max_dn = t["max_up"], t["max_dn"]
+        s.n_up_prefix = t.get("n_up_prefix", 0)
         dev_parts = []
         self.extra = {}
         for name, (o, a, nbytes) in offs.items():

@@ -177,7 +177,9 @@ class StreamBatch:
         if self.phi_lo is not None:
             saved.append(self.phi_lo.clone())
         nbmax = (self.B + 31) // 32
-        cands = [(nb, cm) for nb in (1, 2, 4, 8) if nb == 1 or nb <= 2 * nbmax for cm in (0, 1)]
+        # task orders 0 and 1 coincide when a warp task covers the whole batch
+        cands = [(nb, cm) for nb in (1, 2, 4, 8) if nb == 1 or nb <= 2 * nbmax
+                 for cm in (0, 1, 2, 3) if cm != 1 or 32 * nb < self.B]
         best, best_ms = None, float("inf")
         for nb, cm in cands:
             L.hops_stage_tuning(nb, cm)

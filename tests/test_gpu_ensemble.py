@@ -112,7 +112,8 @@ def run_forced(f, B, precision, noise, n_steps, tuning):
 
 @pytest.mark.parametrize("name", ["ring6", "chain4_2mode"])
 @pytest.mark.parametrize("B", [40, 64, 96])
-@pytest.mark.parametrize("tuning", [(1, 0), (1, 1), (4, 0), (4, 1), (8, 1)])
+@pytest.mark.parametrize("tuning", [(1, 0), (1, 1), (1, 2), (4, 0), (4, 1), (4, 2), (8, 1),
+                                    (8, 2), (1, 3), (4, 3), (8, 3)])
 def test_stage_kernel_shapes_agree(cuda_device, name, B, tuning):
     """Every stage-kernel shape the autotuner may pick gives the same numbers."""
     f = load_golden(name)
