@@ -143,20 +143,25 @@ def measured_peaks():
 def algorithmic_bytes_per_step(t, B, precision):
     """Compulsory bytes of one RK4 step: every vector touched once per stage.
 
-    Stage 1 reads phi and writes acc, Y2; stages 2-3 read Y, phi, acc and write
-    acc, Y; stage 4 reads Y, phi, acc and writes phi: 17 vector passes, 5 of
-    them on phi (phi is complex128 in the mixed mode, which also writes the
-    complex64 copy of phi read by stage 1: stage 1 then reads that copy for its
-    own element and phi).  Tables per stage: int32 aux + int32 mode per up/down
-    connection, the down coefficient and k_decay per aux.
+    Stage 1 reads phi and writes acc, Y2; stage 2 reads Y, phi, acc and writes
+    acc, Y; stage 3 reads Y, phi, acc and writes the partial sum
+    P = phi + h/6 (k1 + 2 k2 + 2 k3) and Y; stage 4 reads Y and P and writes
+    phi: 16 vector passes, 4 of them on phi.  In the mixed mode phi and P are
+    complex128 and the stage vectors complex64; P's halves take the
+    accumulator's buffer and that of the complex64 copy of phi, which stage 4
+    writes and stage 1 reads for its own element besides phi.  Tables per
+    stage: int32 aux + int32 mode per up/down connection, the down
+    coefficient and k_decay per aux.
     """
     n = t["n_hier"] * t["n_state"] * B
     sv = 16 if precision == "complex128" else 8          # stage vectors
     sp = 8 if precision == "complex64" else 16            # state
     if precision == "mixed":
-        per = 12 * sv + 5 * sp + 2 * sv                    # + shadow write and read
+        # 12 complex64 passes (the copy of phi's write and read among them),
+        # 4 on phi, P (complex128) written and read
+        per = 12 * sv + 4 * sp + 2 * 16
     else:
-        per = 12 * sv + 5 * sp
+        per = 12 * sv + 4 * sp
     sc = 8 if precision != "complex128" else 16
     t_idx = (len(t["up_aux"]) * 8 + len(t["dn_aux"]) * (8 + sc) + t["n_hier"] * sc)
     return n * per + 4 * t_idx
@@ -223,9 +228,11 @@ def run_gpu(args):
     ms = max_over_ranks(e0.elapsed_time(e1), dev)
     ens.check()
     value = B * K * world / (ms / 1e3)
-    # per step 4 x (stage scalars + stage kernel); after the call k_finalize only
-    # (HopsEnsemble defers the renormalisation of its last step)
-    launches = 8 * K + 1
+    # separate launches: per step 4 x (stage scalars + stage kernel); the
+    # persistent step kernel: one launch for the call.  After the call
+    # k_finalize only (HopsEnsemble defers the renormalisation of its last step)
+    persistent = int(getattr(ens.batch, "fusion", 0)) == 2
+    launches = (1 if persistent else 8 * K) + 1
 
     result = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
               "steps": K, "warmup": W, "ms_per_step": round(ms / K, 4),
@@ -247,34 +254,54 @@ def run_gpu(args):
               f"{t['n_hier'] * t['n_state'] * B * (16 if args.precision == 'complex128' else 8) / 1e6:.0f}"
               " MB (L2 126 MB)"})
 
-    # ---- roofline of the dominant kernel (the streaming stage kernel) ----
+    # ---- roofline of the dominant kernel ----
     L = _lib.lib()
     import ctypes as C
     kr = min(K, 20)
-    L.hops_kernel_timing(1)
-    ens.propagate(kr * dt, dt)
-    torch.cuda.synchronize()
-    tot = C.c_double(0)
-    nl = C.c_int64(0)
-    L.hops_kernel_timing_read(C.byref(tot), C.byref(nl))
-    L.hops_kernel_timing(0)
-    avg_ms = tot.value / max(nl.value, 1)
-    bytes_launch = algorithmic_bytes_per_step(t, B, args.precision) / 4.0
     peaks = measured_peaks()
     peak = peaks["hbm_gbs"] if peaks and "hbm_gbs" in peaks else 6650.0
-    achieved = bytes_launch / (avg_ms / 1e3) / 1e9
+    step_bytes = algorithmic_bytes_per_step(t, B, args.precision)
     traffic = None
-    prof = os.path.join(ROOT, "profiles", f"k_wide_{args.workload}_{args.precision}.md")
+    if persistent:
+        # the persistent step kernel: one launch runs the kr steps of a call
+        # (the k_finalize after it is inside the events too, ~0.1 % of them)
+        torch.cuda.synchronize()
+        r0 = torch.cuda.Event(enable_timing=True)
+        r1 = torch.cuda.Event(enable_timing=True)
+        r0.record()
+        ens.propagate(kr * dt, dt)
+        r1.record()
+        torch.cuda.synchronize()
+        avg_ms = r0.elapsed_time(r1)
+        bytes_launch = step_bytes * kr
+        kernel, share = f"k_persist (fused RK4 steps, {kr} steps per launch)", 1.0
+        prof = os.path.join(ROOT, "profiles", f"k_persist_{args.workload}_{args.precision}.md")
+        key = "dram_bytes_per_step:"
+    else:
+        L.hops_kernel_timing(1)
+        ens.propagate(kr * dt, dt)
+        torch.cuda.synchronize()
+        tot = C.c_double(0)
+        nl = C.c_int64(0)
+        L.hops_kernel_timing_read(C.byref(tot), C.byref(nl))
+        L.hops_kernel_timing(0)
+        avg_ms = tot.value / max(nl.value, 1)
+        bytes_launch = step_bytes / 4.0
+        kernel = "k_wide (streaming RK4 stage)"
+        share = round(tot.value / kr / (ms / K), 3)
+        prof = os.path.join(ROOT, "profiles", f"k_wide_{args.workload}_{args.precision}.md")
+        key = "dram_bytes_per_launch:"
+    achieved = bytes_launch / (avg_ms / 1e3) / 1e9
     if os.path.exists(prof):
         for line in open(prof):
-            if line.startswith("dram_bytes_per_launch:"):
-                traffic = int(line.split(":")[1])
+            if line.startswith(key):
+                traffic = int(line.split(":")[1]) * (kr if persistent else 1)
     result["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                           "unit": "GB/s", "frac": round(achieved / peak, 4),
-                          "traffic": traffic, "kernel": "k_wide (streaming RK4 stage)",
+                          "traffic": traffic, "kernel": kernel,
                           "algorithmic_bytes_per_launch": int(bytes_launch),
                           "avg_launch_ms": round(avg_ms, 5),
-                          "stage_share_of_step": round(tot.value / kr / (ms / K), 3),
+                          "stage_share_of_step": share,
                           "peak_source": "of measured" if peaks else "of fallback"}
     result["clocks"] = clocks
 
@@ -663,12 +690,17 @@ def stage_probe(args):
     psi0[0] = 1.0
     ens.initialize(psi0)
     h = dt / hbar
-    ens.batch.tuning = shapes[0]
+    # NB,ORDER[,FUSION]: fusion 1 = separate launches (default), 2 = persistent step kernel
+    def use(sh):
+        ens.batch.tuning = sh[:2]
+        ens.batch.fusion = sh[2] if len(sh) > 2 else 1
+
+    use(shapes[0])
     ens.batch.propagate(0, 1, args.warmup, h)
     L = _lib.lib()
     out = {}
     for sh in shapes:
-        ens.batch.tuning = sh
+        use(sh)
         if not args.probe_time:
             ens.batch.propagate(0, 1, args.steps, h)
             continue

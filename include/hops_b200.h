@@ -38,6 +38,7 @@ extern "C" {
 #define HOPS_ECUDA 2        /* a CUDA runtime / driver call failed */
 #define HOPS_ENOTSUP 3      /* request outside what the library implements */
 #define HOPS_ENONFINITE 5   /* a trajectory produced NaN/Inf (status word set) */
+#define HOPS_ETIMEOUT 6     /* a wait inside a kernel ran out of time (status word set) */
 
 #define HOPS_PREC_C128 0    /* complex128 state and arithmetic */
 #define HOPS_PREC_C64 1     /* complex64 state/SpMM, FP64 <L>, norm, z_mem */
@@ -325,6 +326,29 @@ int hops_noise_window_mean(const float* noise_dev, int64_t rows, int32_t n_t, in
  * reference.
  */
 int hops_stage_tuning(int32_t nb, int32_t chunk_major);
+
+/*
+ * Step fusion of hops_rk4_propagate for batches of >= 32 trajectories:
+ * 1 = a scalar launch and a stage launch per RK4 stage (8 per step);
+ * 2 = one cooperative persistent launch per call that runs every stage of
+ * every step with grid barriers in between (used with the 128-trajectory
+ * task shape, nb = 0 or 4); 0 = automatic.  A grid barrier that waits longer
+ * than its time limit sets HOPS_ETIMEOUT in the status word of the
+ * trajectories and the kernel returns.  Process-wide setting used by the
+ * autotuner; the reference integrates one trajectory in Python
+ * (integrator/integrator_rk.py:33-77).
+ */
+int hops_step_fusion(int32_t mode);
+
+/*
+ * Self-test of the step kernel's grid barrier (failure detection without a
+ * GPU fault): a cooperative launch of n_ctas (<= SM count) CTAs, each but
+ * `absent` (-1: none) passing n_sync barriers on bar (4 uint32 of device
+ * memory, zeroed here); out[c] = 1 passed, 0 failed, 2 absent.  With an
+ * absent CTA every other CTA gives up after limit_ns and bar[2] = 1.
+ */
+int hops_grid_barrier_test(uint32_t* bar, int32_t* out, int32_t n_ctas, int32_t n_sync,
+                           int32_t absent, int64_t limit_ns, void* stream);
 
 
 /*

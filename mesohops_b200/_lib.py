@@ -15,6 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libhops_b200.so")
 
 HOPS_OK, HOPS_EINVAL, HOPS_ECUDA, HOPS_ENOTSUP, HOPS_ENONFINITE = 0, 1, 2, 3, 5
+HOPS_ETIMEOUT = 6
 PREC_C128, PREC_C64, PREC_MIXED = 0, 1, 2
 EOM_CODES = {"NORMALIZED NONLINEAR": 0, "NONLINEAR": 1, "LINEAR": 2}
 
@@ -122,6 +123,8 @@ def lib():
     L.hops_rk4_propagate_noalloc.argtypes = [C.POINTER(HopsStructure), _i, _i, _i, _p, _p, _p,
                                              _i, _p, _i, _i, _i, _i, C.c_double, _p, _p, _p]
     L.hops_stage_tuning.argtypes = [_i, _i]
+    L.hops_step_fusion.argtypes = [_i]
+    L.hops_grid_barrier_test.argtypes = [_p, _p, _i, _i, _i, C.c_int64, _p]
     L.hops_flux_errors.argtypes = [_p, _i, _i, C.c_double, _p]
     L.hops_tri_max_depth.restype = _i
     L.hops_tri_max_depth.argtypes = []
@@ -171,7 +174,9 @@ def exported_symbols():
             "hops_rk4_propagate", "hops_resident_propagate", "hops_resident_scalar_doubles",
             "hops_noise_filter", "hops_noise_filter_work_doubles", "hops_kernel_timing",
             "hops_kernel_timing_read", "hops_noalloc_scratch_bytes",
-            "hops_rk4_propagate_noalloc", "hops_stage_tuning", "hops_flux_errors",
+            "hops_rk4_propagate_noalloc", "hops_stage_tuning", "hops_step_fusion",
+            "hops_grid_barrier_test",
+            "hops_flux_errors",
             "hops_flux_errors_smem_doubles", "hops_tri_max_depth", "hops_tri_pass1",
             "hops_tri_pass2", "hops_noise_window_mean", "hops_batch_settle",
             "hops_structure_upload", "hops_structure_host_view", "hops_structure_device_view",

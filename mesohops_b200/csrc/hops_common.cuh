@@ -106,7 +106,9 @@ struct ScalarLayout {
 // stage coefficients in trajectory-fastest layout ([m][b], [s][b], [j][b]) so
 // that the stage kernel reads them coalesced.
 struct BatchLayout {
-  size_t upcT, upcT_f, diagT, diagT_f, czT, czT_f, ncB, scaleB, physT, physT_f, total;  // doubles
+  // bar: 16 bytes (four uint32: arrivals, generation, error, spare) of the
+  // grid barrier of the persistent step kernel
+  size_t upcT, upcT_f, diagT, diagT_f, czT, czT_f, ncB, scaleB, physT, physT_f, bar, total;  // doubles
   __host__ __device__ static size_t even(size_t x) { return (x + 1) & ~(size_t)1; }
   __host__ __device__ BatchLayout(int S, int M, int L, int B) {
     const ScalarLayout lay(S, M, L);
@@ -120,7 +122,8 @@ struct BatchLayout {
     scaleB = ncB + B;
     physT = even(scaleB + B);            // LT term of aux 0, [s][b] complex
     physT_f = physT + 2 * (size_t)S * B;
-    total = even(physT_f + (size_t)S * B);
+    bar = even(physT_f + (size_t)S * B);
+    total = bar + 2;
   }
 };
 

@@ -268,16 +268,23 @@ __device__ __forceinline__ void out_store(V* p, V v) {
   else *p = v;
 }
 
-// Mixed precision in the stage kernels (complex128 state, complex64 stage
-// vectors): the third stage does not store the accumulated slope in complex64
-// but the partial sum P = phi + h/6 (k1 + 2 k2 + 2 k3) in complex128 -- real
-// parts in the accumulator's buffer, imaginary parts in the buffer of phi's
-// complex64 copy, which no kernel reads between the second stage and the
-// fourth -- and the fourth stage reads P in place of phi and the slope:
-// phi' = P + h/6 k4.  The same bytes move, one complex64 rounding of the
-// slope (the largest, of k1 + 2 k2 + 2 k3) is gone.
+// Partial-sum form of the stage kernels: the third stage does not store the
+// accumulated slope k1 + 2 k2 + 2 k3 but the partial sum
+// P = phi + h/6 (k1 + 2 k2 + 2 k3) in the state's precision, and the fourth
+// stage reads P in place of phi and the slope: phi' = P + h/6 k4.  With the
+// stage vectors in the state's precision (complex128, complex64) P takes the
+// accumulator's buffer and the fourth stage skips the read of phi: 16 vector
+// passes per step instead of 17.  Mixed precision (complex128 state,
+// complex64 stage vectors) splits P -- real parts in the accumulator's
+// buffer, imaginary parts in the buffer of phi's complex64 copy, which no
+// kernel reads between the second stage and the fourth: the same bytes move
+// as with the slope, and one complex64 rounding of the largest slope term is
+// gone.  The sum is rounded as phi + h/6 (k1 + 2 k2 + 2 k3) + h/6 k4 instead
+// of phi + h/6 (k1 + 2 k2 + 2 k3 + k4): a difference in the last bit.
 template <typename ST, typename PT>
-constexpr bool psum_mode() { return sizeof(PT) == 16 && sizeof(ST) == 8; }
+constexpr bool psum_mode() { return true; }
+template <typename ST, typename PT>
+constexpr bool psum_split() { return sizeof(PT) == 16 && sizeof(ST) == 8; }
 
 __device__ __forceinline__ double* psum_re(void* acc) { return static_cast<double*>(acc); }
 __device__ __forceinline__ double* psum_im(void* shadow) { return static_cast<double*>(shadow); }
@@ -291,25 +298,29 @@ __device__ __forceinline__ void rk_finish(int stage, double h, T k, PT ph, ST ac
                                           ST* yout, PT* phi, ST* shadow, size_t e) {
   using RP = decltype(ph.x);
   const RP hh = (RP)h;
+  // h / 6 rounded once: the reference divides h (k1 + 2 k2 + 2 k3 + k4) by 6
+  // (integrator_rk.py:75); the product with h/6 differs in the last bit and
+  // spares every element an IEEE division
+  const RP h6 = (RP)(h / 6.0);
   if constexpr (PSUM) {
     if (stage == 2) {
       PT sum = cv<PT>(cadd(cv<T>(accv), cscale(k, (decltype(k.x))2)));
-      PT hs = cscale(sum, hh);
-      hs.x = hs.x / (RP)6;
-      hs.y = hs.y / (RP)6;
+      const PT hs = cscale(sum, h6);
       const PT pp = cadd(ph, hs);
-      __stcs(psum_re(acc) + e, (double)pp.x);
-      __stcs(psum_im(shadow) + e, (double)pp.y);
+      if constexpr (psum_split<ST, PT>()) {
+        __stcs(psum_re(acc) + e, (double)pp.x);
+        __stcs(psum_im(shadow) + e, (double)pp.y);
+      } else {
+        acc_store<GHINT>(acc + e, cv<ST>(pp));
+      }
       out_store<OHINT>(yout + e, cv<ST>(cadd(ph, cscale(cv<PT>(k), hh))));
       return;
     }
     if (stage == 3) {
-      PT hs = cscale(cv<PT>(k), hh);
-      hs.x = hs.x / (RP)6;
-      hs.y = hs.y / (RP)6;
+      const PT hs = cscale(cv<PT>(k), h6);
       const PT nw = cadd(ph, hs);
       out_store<OHINT>(phi + e, nw);
-      out_store<OHINT>(shadow + e, cv<ST>(nw));
+      if (psum_split<ST, PT>() || shadow) out_store<OHINT>(shadow + e, cv<ST>(nw));
       return;
     }
   }
@@ -327,9 +338,7 @@ __device__ __forceinline__ void rk_finish(int stage, double h, T k, PT ph, ST ac
     } break;
     case 3: {
       PT sum = cv<PT>(cadd(cv<T>(accv), k));
-      PT hs = cscale(sum, hh);
-      hs.x = hs.x / (RP)6;
-      hs.y = hs.y / (RP)6;
+      const PT hs = cscale(sum, h6);
       const PT nw = cadd(ph, hs);
       out_store<OHINT>(phi + e, nw);
       if (shadow) out_store<OHINT>(shadow + e, cv<ST>(nw));
@@ -455,12 +464,17 @@ constexpr int wide_min_blocks(int nb, int rbytes) {
   return nb == 1 ? 4 : (nb == 2 ? (rbytes == 8 ? 3 : 4) : (nb == 4 ? HOPS_WIDE_MIN_BLOCKS4 : 2));
 }
 
+// The work items of one stage, run by the calling CTA's warps (the body of
+// k_wide and of the stage phases of the persistent step kernel).  wide_smem:
+// the CTA's wide_smem_bytes of shared memory.  The persistent kernel passes
+// pointers without __restrict__: its Y and stage coefficients are rewritten
+// within the kernel, so they must not be read through the read-only path.
 template <typename R, typename ST, typename PT, bool SITE, int NB, bool LT>
-__global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R)))
-    k_wide(hops_structure st, int B, int stage, double h, const ST* __restrict__ yin,
-           ST* __restrict__ yout, PT* phi, ST* shadow, ST* acc, const double* __restrict__ ws,
-           FastDiv divS, FastDiv divAS, FastDiv divH, FastDiv divP, unsigned n_pre_s,
-           int chunk_major) {
+__device__ __forceinline__ void wide_items(const hops_structure& st, int B, int stage, double h,
+                                           const ST* yin, ST* yout, PT* phi, ST* shadow, ST* acc,
+                                           const double* ws, FastDiv divS, FastDiv divAS,
+                                           FastDiv divH, FastDiv divP, unsigned n_pre_s,
+                                           int chunk_major, unsigned char* wide_smem) {
   using P = Prec<R>;
   using T = typename P::T;
   const int S = st.n_state;
@@ -499,7 +513,6 @@ __global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R
     }
     return r;
   };
-  extern __shared__ __align__(16) unsigned char wide_smem[];
   const int nwb = blockDim.x >> 5;
   const int wib = threadIdx.x >> 5;
   PT* ph_s = reinterpret_cast<PT*>(wide_smem) + (size_t)wib * 2 * CH;
@@ -531,9 +544,13 @@ __global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R
         }
         if constexpr (PSUM) {
           if (want_psum) {
-            double* pd = reinterpret_cast<double*>(ph_s + o);
-            cp_async<8>(pd, psum_re(acc) + row + b);
-            cp_async<8>(pd + 1, psum_im(shadow) + row + b);
+            if constexpr (psum_split<ST, PT>()) {
+              double* pd = reinterpret_cast<double*>(ph_s + o);
+              cp_async<8>(pd, psum_re(acc) + row + b);
+              cp_async<8>(pd + 1, psum_im(shadow) + row + b);
+            } else {
+              cp_async<sizeof(PT)>(ph_s + o, reinterpret_cast<const PT*>(acc) + row + b);
+            }
           }
         }
       }
@@ -716,6 +733,18 @@ __global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R
   cp_async_wait<0>();
 }
 
+template <typename R, typename ST, typename PT, bool SITE, int NB, bool LT>
+__global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R)))
+    k_wide(hops_structure st, int B, int stage, double h, const ST* __restrict__ yin,
+           ST* __restrict__ yout, PT* phi, ST* shadow, ST* acc, const double* __restrict__ ws,
+           FastDiv divS, FastDiv divAS, FastDiv divH, FastDiv divP, unsigned n_pre_s,
+           int chunk_major) {
+  extern __shared__ __align__(16) unsigned char wide_smem[];
+  wide_items<R, ST, PT, SITE, NB, LT>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, divS,
+                                      divAS, divH, divP, n_pre_s, chunk_major, wide_smem);
+}
+
+
 // -------------------------------------------------- narrow stage kernel ----
 // B < 32 trajectories: one warp per aux a (warp-uniform connection lists),
 // lanes over the S*B elements (state s, trajectory b) of that aux.
@@ -744,7 +773,10 @@ __global__ void __launch_bounds__(256) k_narrow(hops_structure st, int B, int st
       const bool want_psum = PSUM && stage == 3;
       PT ph0 = PT{};
       if (want_psum) {
-        if constexpr (PSUM) ph0 = PT{__ldcs(psum_re(acc) + e), __ldcs(psum_im(shadow) + e)};
+        if constexpr (psum_split<ST, PT>())
+          ph0 = PT{__ldcs(psum_re(acc) + e), __ldcs(psum_im(shadow) + e)};
+        else if constexpr (PSUM)
+          ph0 = __ldcs(reinterpret_cast<const PT*>(acc) + e);
       } else if (stage != 4) {
         ph0 = phi[e];
       }
@@ -800,16 +832,19 @@ __device__ void publish(const hops_structure& st, const BatchLayout& bl, double*
   }
 }
 
+// The stage scalars of trajectory b, computed by the calling CTA (all its
+// threads; shm: the CTA's scalar shared memory, scalar_smem / scalar_smem_rows
+// bytes).  Used by k_scalars (one CTA per trajectory) and by the persistent
+// step kernel.
 template <typename R, typename ST, typename PT>
-__global__ void __launch_bounds__(128) k_scalars(hops_structure st, hops_batch bt, int stage, int it,
-                                                 double h, const void* yin, int recompute_scale,
-                                                 double* psi_prev, const float* z1s,
-                                                 const float* z2s, double* dz_out, int stage_rows) {
+__device__ __forceinline__ void scalars_cta(const hops_structure& st, const hops_batch& bt, int b,
+                                            int stage, int it, double h, const void* yin,
+                                            int recompute_scale, double* psi_prev,
+                                            const float* z1s, const float* z2s, double* dz_out,
+                                            int stage_rows, double* shm) {
   using T = typename Prec<R>::T;
-  extern __shared__ double shm[];
   double* red = shm;
   double* sh = shm + 32;
-  const int b = blockIdx.x;
   const int S = st.n_state, M = st.n_mode, L = st.n_lop, B = bt.n_traj;
   const ScalarLayout lay(S, M, L);
   const BatchLayout bl(S, M, L, B);
@@ -889,6 +924,186 @@ __global__ void __launch_bounds__(128) k_scalars(hops_structure st, hops_batch b
   }
   publish(st, bl, bt.work, B, b, ws);
 }
+
+template <typename R, typename ST, typename PT>
+__global__ void __launch_bounds__(128) k_scalars(hops_structure st, hops_batch bt, int stage, int it,
+                                                 double h, const void* yin, int recompute_scale,
+                                                 double* psi_prev, const float* z1s,
+                                                 const float* z2s, double* dz_out, int stage_rows) {
+  extern __shared__ double shm[];
+  scalars_cta<R, ST, PT>(st, bt, blockIdx.x, stage, it, h, yin, recompute_scale, psi_prev, z1s,
+                         z2s, dz_out, stage_rows, shm);
+}
+
+// --------------------------------------------- persistent step kernel ----
+// One cooperative launch runs every RK4 step of a call: for each stage the
+// stage scalars of every trajectory (CTA b mod gridDim, as k_scalars), a grid
+// barrier, the stage's work items (wide_items), a grid barrier.  It replaces
+// the 8 launches per step of the separate kernels and the gaps between them.
+//
+// Grid barrier: bar[0] counts arrivals, bar[1] is the generation, bar[2] the
+// error word.  The last CTA to arrive resets the count and bumps the
+// generation; the others wait on the generation with a time limit (limit_ns
+// of %globaltimer; HOPS_BARRIER_NS in the step kernel), after which they set
+// the error word and return; a CTA that sees the error word set returns too.
+// The host zeroes bar before the launch.  A cooperative launch guarantees
+// that every CTA is resident, so the barrier cannot wait on a CTA that never
+// runs.  The longest phase between two barriers is one stage (~0.5 ms on the
+// 20-site ring at 128 trajectories, tens of ms for the largest batches).
+#ifndef HOPS_BARRIER_NS
+#define HOPS_BARRIER_NS 2000000000ull
+#endif
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Relaxed (not acquire) load for the polling: an acquire at gpu scope
+// invalidates the SM's L1, and a CTA polling with acquires kept emptying the
+// L1 of the CTAs still working on its SM (1.7x the instructions and half the
+// L1 hit rate of the separate launches).  One fence after the wait acquires.
+__device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+// false: the barrier failed (time limit, or another CTA's failure)
+__device__ __forceinline__ bool grid_sync(unsigned* bar, unsigned& gen,
+                                          unsigned long long limit_ns = HOPS_BARRIER_NS) {
+  __shared__ unsigned ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned ok = 1;
+    __threadfence();  // this CTA's writes before the arrival
+    const unsigned g = gen;
+    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicExch(bar + 1, g + 1u);
+    } else {
+      const unsigned long long t0 = global_ns();
+      unsigned ns = 32;
+      while (ld_relaxed_u32(bar + 1) == g) {
+        if (ld_relaxed_u32(bar + 2) != 0u) {
+          ok = 0;
+          break;
+        }
+        if (global_ns() - t0 > limit_ns) {
+          atomicExch(bar + 2, 1u);
+          ok = 0;
+          break;
+        }
+        __nanosleep(ns);
+        if (ns < 1024) ns <<= 1;
+      }
+    }
+    __threadfence();  // acquire: the other CTAs' writes before the barrier are seen
+    if (ld_relaxed_u32(bar + 2) != 0u) ok = 0;
+    ok_s = ok;
+  }
+  ++gen;
+  __syncthreads();
+  return ok_s != 0u;
+}
+
+// Self-test of the grid barrier: every CTA but `absent` passes n_sync
+// barriers; out[c] = 1 if CTA c passed them all, 0 if one failed (time limit
+// or another CTA's failure), 2 for the absent CTA, which returns at once.
+__global__ void k_barrier_test(unsigned* bar, int32_t* out, int n_sync, int absent,
+                               unsigned long long limit_ns) {
+  if ((int)blockIdx.x == absent) {
+    if (threadIdx.x == 0) out[blockIdx.x] = 2;
+    return;
+  }
+  unsigned gen = 0;
+  bool ok = true;
+  for (int i = 0; i < n_sync && ok; ++i) ok = grid_sync(bar, gen, limit_ns);
+  if (threadIdx.x == 0) out[blockIdx.x] = ok ? 1 : 0;
+}
+
+#ifndef HOPS_PERSIST_NOINLINE
+#define HOPS_PERSIST_NOINLINE 0
+#endif
+#if HOPS_PERSIST_NOINLINE
+// The stage phase as a call: the callee gets the register budget of the
+// kernel, the caller's few live values are saved across it.
+template <typename R, typename ST, typename PT, bool SITE, int NB, bool LT>
+__device__ __noinline__ void wide_phase(const hops_structure& st, const hops_batch& bt, int i,
+                                        double h, FastDiv divS, FastDiv divAS, FastDiv divH,
+                                        FastDiv divP, unsigned n_pre_s, int chunk_major,
+                                        unsigned char* smem) {
+  ST* shadow = bt.precision == HOPS_PREC_MIXED ? static_cast<ST*>(bt.phi_lo) : nullptr;
+  const void* yin = i == 0 ? (shadow ? static_cast<const void*>(shadow) : bt.phi)
+                           : (i == 1 ? bt.y0 : (i == 2 ? bt.y1 : bt.y0));
+  void* yout = i == 0 ? bt.y0 : (i == 1 ? bt.y1 : (i == 2 ? bt.y0 : nullptr));
+  wide_items<R, ST, PT, SITE, NB, LT>(st, bt.n_traj, i, h, static_cast<const ST*>(yin),
+                                      static_cast<ST*>(yout), static_cast<PT*>(bt.phi), shadow,
+                                      static_cast<ST*>(bt.acc), bt.work, divS, divAS, divH, divP,
+                                      n_pre_s, chunk_major, smem);
+}
+#define HOPS_PERSIST_PARAM const __grid_constant__
+#else
+#define HOPS_PERSIST_PARAM
+#endif
+
+// The step loop keeps one counter q = 4 n + i live across the stage phase;
+// everything else is recomputed from the kernel parameters, so the stage
+// phase has (nearly) the register budget of k_wide.
+template <typename R, typename ST, typename PT, bool SITE, int NB, bool LT>
+__global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R)))
+    k_persist(HOPS_PERSIST_PARAM hops_structure st, HOPS_PERSIST_PARAM hops_batch bt, int it0,
+              int di, int n_steps, double h, double* psi_out, int stage_rows, FastDiv divS,
+              FastDiv divAS, FastDiv divH, FastDiv divP, unsigned n_pre_s, int chunk_major) {
+  extern __shared__ __align__(16) unsigned char pers_smem[];
+  for (int q = 0; q < 4 * n_steps; ++q) {
+    const int n = q >> 2, i = q & 3;
+    const int B = bt.n_traj;
+    unsigned* bar = reinterpret_cast<unsigned*>(
+        bt.work + BatchLayout(st.n_state, st.n_mode, st.n_lop, B).bar);
+    unsigned gen = 2u * (unsigned)q;
+    {
+      ST* shadow = bt.precision == HOPS_PREC_MIXED ? static_cast<ST*>(bt.phi_lo) : nullptr;
+      const int it = it0 + 2 * n * di + rk_noise_slot(i) * di;
+      // stage 0 gathers from the state (or its complex64 copy in mixed mode)
+      const void* yin = i == 0 ? (shadow ? static_cast<const void*>(shadow) : bt.phi)
+                               : (i == 1 ? bt.y0 : (i == 2 ? bt.y1 : bt.y0));
+      const int recompute = (i == 0 && n > 0 && bt.eom == HOPS_EOM_NORMALIZED_NONLINEAR) ? 1 : 0;
+      double* psi_prev = (i == 0 && n > 0 && psi_out)
+                             ? psi_out + (size_t)(n - 1) * (size_t)B * st.n_state * 2
+                             : nullptr;
+      for (int b = blockIdx.x; b < B; b += gridDim.x) {
+        scalars_cta<R, ST, PT>(st, bt, b, i, it, h, yin, recompute, psi_prev, nullptr, nullptr,
+                               nullptr, stage_rows, reinterpret_cast<double*>(pers_smem));
+        __syncthreads();  // the next trajectory reuses the shared memory
+      }
+    }
+    bool ok = grid_sync(bar, gen);
+    if (ok) {
+#if HOPS_PERSIST_NOINLINE
+      wide_phase<R, ST, PT, SITE, NB, LT>(st, bt, i, h, divS, divAS, divH, divP, n_pre_s,
+                                          chunk_major, pers_smem);
+#else
+      ST* shadow = bt.precision == HOPS_PREC_MIXED ? static_cast<ST*>(bt.phi_lo) : nullptr;
+      const void* yin = i == 0 ? (shadow ? static_cast<const void*>(shadow) : bt.phi)
+                               : (i == 1 ? bt.y0 : (i == 2 ? bt.y1 : bt.y0));
+      void* yout = i == 0 ? bt.y0 : (i == 1 ? bt.y1 : (i == 2 ? bt.y0 : nullptr));
+      wide_items<R, ST, PT, SITE, NB, LT>(st, B, i, h, static_cast<const ST*>(yin),
+                                          static_cast<ST*>(yout), static_cast<PT*>(bt.phi),
+                                          shadow, static_cast<ST*>(bt.acc), bt.work, divS, divAS,
+                                          divH, divP, n_pre_s, chunk_major, pers_smem);
+#endif
+      bar = reinterpret_cast<unsigned*>(
+          bt.work + BatchLayout(st.n_state, st.n_mode, st.n_lop, bt.n_traj).bar);
+      ok = grid_sync(bar, gen);
+    }
+    if (!ok) {  // every trajectory of this CTA ends with the timeout status
+      if (threadIdx.x == 0)
+        for (int b = blockIdx.x; b < bt.n_traj; b += gridDim.x) bt.status[b] = HOPS_ETIMEOUT;
+      return;
+    }
+  }
+}
+
 
 // Normalisation after the last step of a call: records 1/||psi_0|| per
 // trajectory and writes the last psi_0.
@@ -1163,6 +1378,40 @@ static int grid_for_warps(long warps) {
 // Stage-kernel shape: trajectories per chunk (32 * nb) and chunk-major order.
 // 0 = choose automatically; set by hops_stage_tuning (the autotuner).
 static int g_tune_nb = 0, g_tune_cm = -1;
+// Step fusion: 0 = automatic (separate launches), 1 = separate scalar and
+// stage launches, 2 = the persistent step kernel (batches of >= 32
+// trajectories at 128 trajectories per task); set by hops_step_fusion.  The
+// persistent kernel is exact (bit for bit the numbers of the separate
+// launches) but slower on the 20-site ring at 128 trajectories: 4.1 against
+// 2.0 ms per complex128 step, 2.5 against 1.7 mixed, 1.6 against 1.3
+// complex64.  Its stage phases run 2.1x slower than k_wide's with the scalar
+// phase's code in the same kernel (1.23x without it); the scalar phase,
+// serial between two barriers, takes ~0.1 ms per stage against ~0.02 ms
+// for k_scalars; the barriers themselves cost ~1 us.
+static int g_fusion = 0;
+
+extern "C" int hops_grid_barrier_test(uint32_t* bar, int32_t* out, int32_t n_ctas,
+                                      int32_t n_sync, int32_t absent, int64_t limit_ns,
+                                      void* stream) {
+  if (!bar || !out || n_ctas < 1 || n_ctas > sm_count() || n_sync < 0 || limit_ns <= 0)
+    return set_err(HOPS_EINVAL, "grid barrier test: bad arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  CUDA_TRY(cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), s));
+  unsigned* b = bar;
+  int32_t* o = out;
+  int ns = n_sync, ab = absent;
+  unsigned long long lim = (unsigned long long)limit_ns;
+  void* args[] = {&b, &o, &ns, &ab, &lim};
+  CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_barrier_test, dim3(n_ctas), dim3(128), args,
+                                       0, s));
+  return HOPS_OK;
+}
+
+extern "C" int hops_step_fusion(int32_t mode) {
+  if (mode < 0 || mode > 2) return set_err(HOPS_EINVAL, "step fusion must be 0 (auto), 1 or 2");
+  g_fusion = mode;
+  return HOPS_OK;
+}
 
 extern "C" int hops_stage_tuning(int32_t nb, int32_t chunk_major) {
   if (nb != 0 && nb != 1 && nb != 2 && nb != 4 && nb != 8)
@@ -1235,6 +1484,70 @@ static void launch_wide(const hops_structure* st, int B, int stage, double h, co
                                                chunk_major, s);
 }
 
+// Persistent step kernel (k_persist) for the 128-trajectory task shape.
+template <typename R, typename ST, typename PT, bool SITE, bool LT>
+static int launch_persist_lt(const hops_structure* st, hops_batch* bt, int it0, int di,
+                             int n_steps, double h, double* psi_out, int stage_rows,
+                             size_t scal_smem, int chunk_major, cudaStream_t s) {
+  constexpr int NB = 4;
+  const int B = bt->n_traj;
+  const unsigned n_as = (unsigned)st->n_hier * st->n_state;
+  const long nchunk = (B + 32 * NB - 1) / (32 * NB);
+  const int n_pre = st->n_up_prefix > 0 && st->n_up_prefix <= st->n_hier ? st->n_up_prefix : 0;
+  constexpr int threads = wide_threads(NB);
+  const size_t smem = std::max(wide_smem_bytes<ST, PT, NB>(threads / 32), scal_smem);
+  auto kern = k_persist<R, ST, PT, SITE, NB, LT>;
+  // occupancy at the largest shared memory any structure asks for (48 KB
+  // scalars at most, wide_smem_bytes otherwise): one value per instantiation
+  static int resident = 0;
+  static int set_for = -1;
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  const size_t smem_max = std::max(wide_smem_bytes<ST, PT, NB>(threads / 32), (size_t)48 * 1024);
+  if (set_for != dev) {
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
+    set_for = dev;
+  }
+  if (resident == 0) {
+    int nb = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, threads, smem_max));
+    resident = nb < 1 ? 1 : nb;
+  }
+  const long task_warps = chunk_major ? (long)n_as * nchunk : (long)n_as;
+  long gl = (task_warps * 32 + threads - 1) / threads;
+  if (gl > (long)sm_count() * resident) gl = (long)sm_count() * resident;
+  int grid = (int)(gl < 1 ? 1 : gl);
+  const BatchLayout bl(st->n_state, st->n_mode, st->n_lop, B);
+  CUDA_TRY(cudaMemsetAsync(bt->work + bl.bar, 0, 4 * sizeof(unsigned), s));
+  hops_structure stv = *st;
+  hops_batch btv = *bt;
+  FastDiv divS((unsigned)st->n_state), divAS(n_as), divH((unsigned)st->n_hier),
+      divP(n_pre > 0 ? (unsigned)n_pre : 1u);
+  unsigned n_pre_s = (unsigned)n_pre * st->n_state;
+  void* args[] = {&stv, &btv, &it0, &di, &n_steps, &h, &psi_out, &stage_rows, &divS, &divAS,
+                  &divH, &divP, &n_pre_s, &chunk_major};
+  CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(threads), args, smem, s));
+  return HOPS_OK;
+}
+
+template <typename R, typename ST, typename PT>
+static int launch_persist(const hops_structure* st, hops_batch* bt, int it0, int di, int n_steps,
+                          double h, double* psi_out, int stage_rows, size_t scal_smem,
+                          int chunk_major, cudaStream_t s) {
+  if (st->site_projector) {
+    if (st->lt_coef)
+      return launch_persist_lt<R, ST, PT, true, true>(st, bt, it0, di, n_steps, h, psi_out,
+                                                      stage_rows, scal_smem, chunk_major, s);
+    return launch_persist_lt<R, ST, PT, true, false>(st, bt, it0, di, n_steps, h, psi_out,
+                                                     stage_rows, scal_smem, chunk_major, s);
+  }
+  if (st->lt_coef)
+    return launch_persist_lt<R, ST, PT, false, true>(st, bt, it0, di, n_steps, h, psi_out,
+                                                     stage_rows, scal_smem, chunk_major, s);
+  return launch_persist_lt<R, ST, PT, false, false>(st, bt, it0, di, n_steps, h, psi_out,
+                                                    stage_rows, scal_smem, chunk_major, s);
+}
+
 template <typename R, typename ST, typename PT, bool SITE>
 static void launch_stage(const hops_structure* st, int B, int stage, double h, const void* yin,
                          void* yout, void* phi, void* shadow, void* acc, const double* ws,
@@ -1303,7 +1616,16 @@ static int propagate_impl(const hops_structure* st, hops_batch* bt, int32_t it0,
   const bool normalized = bt->eom == HOPS_EOM_NORMALIZED_NONLINEAR;
   const size_t psi_stride = (size_t)B * S * 2;
   void* shadow = bt->precision == HOPS_PREC_MIXED ? bt->phi_lo : nullptr;
-  for (int n = 0; n < n_steps; ++n) {
+  // the persistent step kernel: 128 trajectories per task (or the automatic
+  // shape) and fusion switched on
+  const int cm = g_tune_cm >= 0 ? g_tune_cm : (st->n_up_prefix > 0 ? 3 : 0);
+  const bool persist = g_fusion == 2 && B >= 32 && (g_tune_nb == 0 || g_tune_nb == 4);
+  if (persist && n_steps > 0) {
+    int rc = launch_persist<R, ST, PT>(st, bt, it0, di, n_steps, h, psi_out, stage_rows, smem,
+                                       cm, s);
+    if (rc) return rc;
+  }
+  for (int n = 0; n < (persist ? 0 : n_steps); ++n) {
     for (int i = 0; i < 4; ++i) {
       const int slot = i == 0 ? 0 : (i == 3 ? 2 : 1);
       const int it = it0 + 2 * n * di + slot * di;

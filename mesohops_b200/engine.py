@@ -57,7 +57,7 @@ def _stream(dev):
 
 
 # Autotuned stage-kernel shapes per problem class:
-# (n_hier, n_state, n_mode, B, precision, site projector) -> (nb, chunk_major)
+# (n_hier, n_state, n_mode, B, precision, site projector) -> ((nb, chunk_major), fusion)
 _TUNE_CACHE = {}
 
 
@@ -97,6 +97,8 @@ class StreamBatch:
         b.defer_scale = 0
         self.cb = b
         self._pending = False
+        self.tuning = None      # (nb, task order) of the stage kernel, None = automatic
+        self.fusion = 0         # hops_step_fusion mode: 0 automatic, 1 separate, 2 persistent
         self.reset()
 
     @property
@@ -160,6 +162,7 @@ class StreamBatch:
         fewer than 32 trajectories use the narrow kernel and need no tuning.
         """
         self.tuning = None
+        self.fusion = 0
         if self.B < 32:
             return None
         # timing only: run from noise index 0 and stay inside the noise axis
@@ -169,7 +172,7 @@ class StreamBatch:
             return None
         key = self.tune_key()
         if key in _TUNE_CACHE:
-            self.tuning = _TUNE_CACHE[key]
+            self.tuning, self.fusion = _TUNE_CACHE[key]
             return self.tuning
         L = _lib.lib()
         pending = self._pending
@@ -177,12 +180,15 @@ class StreamBatch:
         if self.phi_lo is not None:
             saved.append(self.phi_lo.clone())
         nbmax = (self.B + 31) // 32
-        # task orders 0 and 1 coincide when a warp task covers the whole batch
-        cands = [(nb, cm) for nb in (1, 2, 4, 8) if nb == 1 or nb <= 2 * nbmax
+        # task orders 0 and 1 coincide when a warp task covers the whole batch.
+        # The persistent step kernel (fusion 2) is not a candidate: on the
+        # 20-site ring it ran 1.2-2.1x slower than the separate launches
+        cands = [(nb, cm, 1) for nb in (1, 2, 4, 8) if nb == 1 or nb <= 2 * nbmax
                  for cm in (0, 1, 2, 3) if cm != 1 or 32 * nb < self.B]
         best, best_ms = None, float("inf")
-        for nb, cm in cands:
+        for nb, cm, fu in cands:
             L.hops_stage_tuning(nb, cm)
+            L.hops_step_fusion(fu)
             self.propagate(it0, di, 1, tau_over_hbar, tuned=False)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
@@ -192,14 +198,15 @@ class StreamBatch:
             torch.cuda.synchronize(self.dev)
             ms = e0.elapsed_time(e1)
             if ms < best_ms:
-                best, best_ms = (nb, cm), ms
+                best, best_ms = (nb, cm, fu), ms
             for dst, src in zip((self.phi, self.zmem, self.work, self.status, self.phi_lo), saved):
                 dst.copy_(src)
         L.hops_stage_tuning(0, -1)
+        L.hops_step_fusion(0)
         self._pending = pending
-        _TUNE_CACHE[key] = best
-        self.tuning = best
-        return best
+        self.tuning, self.fusion = best[:2], best[2]
+        _TUNE_CACHE[key] = (self.tuning, self.fusion)
+        return self.tuning
 
     def propagate(self, it0, di, n_steps, tau_over_hbar, psi_out=None, tuned=True):
         """n_steps RK4 steps; psi_out: optional device tensor [n_steps, B, S] complex128."""
@@ -207,6 +214,7 @@ class StreamBatch:
         if tuned:
             nb, cm = getattr(self, "tuning", None) or (0, -1)
             L.hops_stage_tuning(nb, cm)
+            L.hops_step_fusion(int(getattr(self, "fusion", 0)))
         ptr = psi_out.data_ptr() if psi_out is not None else None
         rc = L.hops_rk4_propagate(C.byref(self.st.cstruct), C.byref(self.cb), int(it0), int(di),
                                   int(n_steps), float(tau_over_hbar), ptr, _stream(self.dev))
@@ -216,6 +224,9 @@ class StreamBatch:
 
     def check_status(self):
         st = self.status.cpu().numpy()
+        if np.any(st == _lib.HOPS_ETIMEOUT):
+            raise TrajectoryError("a grid barrier of the step kernel timed out in trajectories "
+                                  f"{np.nonzero(st == _lib.HOPS_ETIMEOUT)[0].tolist()}")
         if np.any(st != 0):
             raise TrajectoryError(f"non-finite state in trajectories {np.nonzero(st)[0].tolist()}")
 

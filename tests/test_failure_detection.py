@@ -154,3 +154,36 @@ def test_server_ends_only_the_failing_requests(cuda_device, workers):
         r = by_id[c.rid]
         assert r.status == "done", (c.rid, r.reason)
         assert np.max(np.abs(r.psi_traj - c.psi_traj)) <= 1e-12
+
+
+@pytest.mark.gpu
+def test_grid_barrier_wait_runs_out_and_reports(cuda_device):
+    """The persistent step kernel's grid barrier: with every CTA present it
+    passes; with one CTA that never arrives (a flag nothing sets) the others
+    give up after the time limit, return, and the error word and their result
+    say so -- no hang, no fault, the context stays usable."""
+    import time
+    import torch
+    from mesohops_b200 import _lib
+    L = _lib.lib()
+    bar = torch.zeros(4, dtype=torch.int32, device="cuda")
+    n = 8
+    out = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    _lib.check(L.hops_grid_barrier_test(bar.data_ptr(), out.data_ptr(), n, 5, -1,
+                                        2_000_000_000, s), "barrier test")
+    torch.cuda.synchronize()
+    assert out.tolist() == [1] * n and int(bar[2]) == 0
+    limit_ns = 20_000_000
+    t0 = time.perf_counter()
+    _lib.check(L.hops_grid_barrier_test(bar.data_ptr(), out.data_ptr(), n, 5, 3, limit_ns, s),
+               "barrier test")
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    res = out.tolist()
+    assert res[3] == 2 and all(r == 0 for i, r in enumerate(res) if i != 3)
+    assert int(bar[2]) == 1
+    assert dt < 5.0
+    # the context is still usable
+    x = torch.ones(1024, device="cuda")
+    assert float(x.sum()) == 1024.0

@@ -91,8 +91,9 @@ def test_ensemble_derivative_matches_oracle(cuda_device):
 
 
 
-def run_forced(f, B, precision, noise, n_steps, tuning):
-    """Ensemble run with a fixed stage-kernel shape (nb, chunk_major)."""
+def run_forced(f, B, precision, noise, n_steps, tuning, fusion=1):
+    """Ensemble run with a fixed stage-kernel shape (nb, chunk_major) and step
+    fusion (1: separate launches, 2: the persistent step kernel)."""
     import torch
     from mesohops_b200 import HopsEnsemble
     ens = HopsEnsemble(golden_system(f), B,
@@ -102,6 +103,7 @@ def run_forced(f, B, precision, noise, n_steps, tuning):
                        autotune=False)
     ens.initialize(f["psi0"])
     ens.batch.tuning = tuning
+    ens.batch.fusion = fusion
     dt = float(f["dt"])
     psi = torch.empty((n_steps, B, ens.n_state), dtype=torch.complex128, device="cuda")
     ens.propagate(n_steps * dt, dt, psi_out=psi)
@@ -122,6 +124,24 @@ def test_stage_kernel_shapes_agree(cuda_device, name, B, tuning):
     ref = run_forced(f, B, "complex128", noise, n_steps, (2, 0))
     got = run_forced(f, B, "complex128", noise, n_steps, tuning)
     assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("name", ["ring6", "chain4_2mode"])
+@pytest.mark.parametrize("B", [40, 128, 700])
+@pytest.mark.parametrize("precision", ["complex128", "mixed", "complex64"])
+@pytest.mark.parametrize("order", [0, 3])
+def test_persistent_step_kernel_matches_separate_launches(cuda_device, name, B, precision, order):
+    """The persistent step kernel (one cooperative launch per call, grid
+    barriers between the scalar and stage phases) gives the numbers of the
+    separate scalar and stage launches bit for bit -- including batches with
+    more trajectories than CTAs (700 on the 6-site ring: 126 CTAs, each
+    computing the scalars of several trajectories) and several chunks."""
+    f = load_golden(name)
+    n_steps = 6
+    noise = ensemble_noise(f, B, 5)
+    ref = run_forced(f, B, precision, noise, n_steps, (4, order), fusion=1)
+    got = run_forced(f, B, precision, noise, n_steps, (4, order), fusion=2)
+    assert np.array_equal(got, ref)
 
 
 @pytest.mark.parametrize("precision", ["complex128", "mixed"])
