@@ -317,7 +317,8 @@ int hops_noise_window_mean(const float* noise_dev, int64_t rows, int32_t n_t, in
                            void* stream);
 
 /*
- * Shape of the batched stage kernel: 32*nb trajectories per warp task and the
+ * Shape of the batched stage kernel (batches of >= 32 trajectories): 32*nb
+ * trajectories per warp task and the
  * task order: 0 = (aux, state) with the trajectory chunks innermost, 1 = chunk
  * outermost, 2 = chunk outermost then state, aux innermost, 3 = chunk
  * outermost, then the aux below n_up_prefix state by state, then the rest in
