@@ -33,7 +33,8 @@ from .constants import hbar, precision
 from .device import DeviceStructure, _state_mode_tables, build_tables
 from .engine import ResidentRunner, ResidentTrajectory, StreamBatch
 from .exceptions import TrajectoryError, UnsupportedRequest
-from .hierarchy import AuxBasis, AuxKeyer, apply_static_filters, triangular_counts
+from .hierarchy import (AuxBasis, AuxKeyer, apply_static_filters, insert_mode, remove_mode,
+                        triangular_counts, tuples_of)
 
 # Resident kernel when the four stage vectors fit one CTA's shared memory.
 RESIDENT_MAX_BYTES = 200 * 1024
@@ -733,23 +734,31 @@ class AdaptiveHops:
         # modes); the terms of one candidate are summed in that order
         iu, mu = np.nonzero(Eu.T)
         idn, md = np.nonzero(Ed.T)
-        n_abs = self.system.n_mode
-        cand = np.concatenate([b.counts[idx_stable[iu]], b.counts[idx_stable[idn]]], axis=0)
-        cand[np.arange(len(iu)), b.modes[mu]] += 1
-        cand[len(iu) + np.arange(len(idn)), b.modes[md]] -= 1
+        # candidate i: the stable aux par[i] with mode mod[i] added (sgn +1) or
+        # removed (sgn -1); keyed from its sorted mode tuple
+        par = np.concatenate([idx_stable[iu], idx_stable[idn]])
+        mod = np.concatenate([b.modes[mu], b.modes[md]]).astype(np.int64)
+        sgn = np.concatenate([np.ones(len(iu), np.int64), -np.ones(len(idn), np.int64)])
         vals = np.concatenate([Eu[mu, iu], Ed[md, idn]])
         order = np.argsort(np.concatenate([2 * iu, 2 * idn + 1]), kind="stable")
-        cand, vals = cand[order].reshape(-1, n_abs), vals[order]
+        par, mod, sgn, vals = par[order], mod[order], sgn[order], vals[order]
         if len(vals) == 0:
             return []
-        keys = self.keyer.sort_keys(cand)
+        tup = b.aux.tup[par]
+        up = sgn > 0
+        tup[up] = insert_mode(tup[up], mod[up])
+        tup[~up] = remove_mode(tup[~up], mod[~up])
+        keys = self.keyer.keys_from_tuples(tup, b.depth[par] + sgn)
         _, first, inv = np.unique(keys, return_index=True, return_inverse=True)
         sums = np.zeros(len(first))
         np.add.at(sums, inv.ravel(), vals)
         seq = np.argsort(first)                     # first-occurrence order
-        sums, rows = sums[seq], cand[first[seq]]
+        sums, pick = sums[seq], first[seq]
         thresh = error_thresh(np.sort(sums), bound_sq, offset=discarded)
-        return list(rows[sums > thresh])
+        pick = pick[sums > thresh]
+        rows = b.counts[par[pick]].copy()
+        rows[np.arange(len(pick)), mod[pick]] += sgn[pick].astype(rows.dtype)
+        return list(rows)
 
     # ----------------------------------------------------------------- states
     def _state_gen(self, phi, dt, z_step, idx_stable_aux, bound_aux):
@@ -769,19 +778,19 @@ class AdaptiveHops:
         F_up = np.zeros((M, N), dtype=bool)
         V = np.asarray(bound_aux, dtype=np.int16).reshape(-1, self.system.n_mode)
         if len(V) and M:
+            TV, dV = tuples_of(V, self.maxhier)
             # aux one step up from each boundary aux along every basis mode
-            low = V[V.sum(axis=1) < self.maxhier]
+            low = np.nonzero(dV < self.maxhier)[0]
             if len(low):
-                ups = np.repeat(low[:, None, :], M, axis=1)
-                ups[:, np.arange(M), b.modes] += 1
-                idx = b.aux.index_of(ups.reshape(-1, self.system.n_mode)).reshape(len(low), M)
+                ups = insert_mode(np.repeat(TV[low], M, axis=0), np.tile(b.modes, len(low)))
+                keys = self.keyer.keys_from_tuples(ups, np.repeat(dV[low] + 1, M))
+                idx = b.aux.index_of_keys(keys).reshape(len(low), M)
                 vi, mi = np.nonzero(idx >= 0)
                 F_down[mi, idx[vi, mi]] = True
             # aux one step down from each boundary aux along its own modes
             vi, mabs = np.nonzero(V)
-            downs = V[vi].copy()
-            downs[np.arange(len(vi)), mabs] -= 1
-            idx = b.aux.index_of(downs)
+            downs = remove_mode(TV[vi], mabs)
+            idx = b.aux.index_of_keys(self.keyer.keys_from_tuples(downs, dV[vi] - 1))
             ok = idx >= 0
             rel = np.array([b.rel_mode[int(m)] for m in mabs[ok]], dtype=np.int64)
             F_up[rel, idx[ok]] = True

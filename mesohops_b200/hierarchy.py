@@ -93,7 +93,11 @@ class AuxKeyer:
         """keys_from_counts for every depth at once (int64 keys): each row's
         rank is a difference of running sums of its per-position binomial
         terms."""
-        row_t, c, i, start = self._tuples(counts, depth)
+        return self._keys_int64_from(*self._tuples(counts, depth), depth)
+
+    def _keys_int64_from(self, row_t, c, i, start, depth):
+        """The int64 keys of rows given as their sorted mode tuples laid end to
+        end (the layout of _tuples)."""
         k = depth[row_t]
         n = self.M + k - 1
         b = c + i
@@ -125,6 +129,27 @@ class AuxKeyer:
         arr = np.zeros((counts.shape[0], self.D + 1), dtype=w)
         arr[:, 0] = depth
         arr[row_t, 1 + i] = c
+        return np.ascontiguousarray(arr).view(f"S{arr.itemsize * (self.D + 1)}").ravel()
+
+    def keys_from_tuples(self, tup, depth):
+        """sort_keys of aux given as sorted mode tuples: tup [N, W] with W at
+        least the largest depth; the entries of row r beyond depth[r] are
+        ignored.  Equal to sort_keys of the same aux as count rows."""
+        depth = np.asarray(depth, dtype=np.int64)
+        tup = np.asarray(tup, dtype=np.int64).reshape(len(depth), -1)
+        if depth.size and depth.max() > self.D:
+            raise AuxError("aux deeper than MAXHIER")
+        mask = np.arange(tup.shape[1])[None, :] < depth[:, None]
+        if self.use_int64:
+            row_t, i = np.nonzero(mask)
+            start = np.zeros(len(depth) + 1, dtype=np.int64)
+            np.cumsum(depth, out=start[1:])
+            return self._keys_int64_from(row_t, tup[row_t, i], i, start, depth)
+        w = ">u2" if self.M < (1 << 16) else ">u4"
+        arr = np.zeros((len(depth), self.D + 1), dtype=w)
+        arr[:, 0] = depth
+        k = min(tup.shape[1], self.D)
+        arr[:, 1:1 + k] = np.where(mask[:, :k], tup[:, :k], 0)
         return np.ascontiguousarray(arr).view(f"S{arr.itemsize * (self.D + 1)}").ravel()
 
     def _rank(self, tup, k):
@@ -202,6 +227,42 @@ def apply_static_filters(counts, filters, n_mode):
     return counts[keep]
 
 
+_PAD = np.iinfo(np.int64).max   # mode-tuple padding, above every mode index
+
+
+def tuples_of(counts, width):
+    """Sorted mode tuples of count rows, padded with _PAD to ``width``, and the
+    rows' depths."""
+    counts = np.asarray(counts)
+    depth = counts.sum(axis=1).astype(np.int64)
+    row_t, c, i, _ = AuxKeyer._tuples(counts, depth)
+    tup = np.full((len(counts), max(int(width), 1)), _PAD, dtype=np.int64)
+    tup[row_t, i] = c
+    return tup, depth
+
+
+def insert_mode(tup, m):
+    """The sorted tuples tup [n, W] with mode m[i] inserted into row i (row i
+    must have a free slot)."""
+    m = np.asarray(m, dtype=np.int64)[:, None]
+    pos = (tup <= m).sum(axis=1, keepdims=True)
+    ar = np.arange(tup.shape[1])[None, :]
+    right = np.full_like(tup, _PAD)
+    right[:, 1:] = tup[:, :-1]
+    return np.where(ar < pos, tup, np.where(ar == pos, m, right))
+
+
+def remove_mode(tup, m):
+    """The sorted tuples tup [n, W] with one occurrence of mode m[i] (which row
+    i must hold) removed from row i."""
+    m = np.asarray(m, dtype=np.int64)[:, None]
+    pos = (tup < m).sum(axis=1, keepdims=True)
+    ar = np.arange(tup.shape[1])[None, :]
+    left = np.full_like(tup, _PAD)
+    left[:, :-1] = tup[:, 1:]
+    return np.where(ar < pos, tup, left)
+
+
 class AuxBasis:
     """A sorted aux list with its up/down connection tables.
 
@@ -212,10 +273,14 @@ class AuxBasis:
 
     def __init__(self, counts, keyer, maxhier, modes=None):
         counts = np.asarray(counts)
-        keys = keyer.sort_keys(counts)
+        # sorted mode tuple of every aux (padded with _PAD beyond its depth),
+        # from which its key is formed
+        tup, depth = tuples_of(counts, maxhier)
+        keys = keyer.keys_from_tuples(tup, depth)
         order = np.argsort(keys, kind="stable")
         self.counts = counts[order]
         self.keys = keys[order]
+        self.tup = tup[order]
         if len(self.keys) == 0 or self.counts[0].sum() != 0:
             raise AuxError("Zero Vector not contained in list_aux!")
         self.keyer = keyer
@@ -223,34 +288,54 @@ class AuxBasis:
         self.n_hier = len(self.counts)
         n_mode_abs = self.counts.shape[1]
         self.modes = np.arange(n_mode_abs) if modes is None else np.asarray(modes, dtype=np.int64)
-        self.depth = self.counts.sum(axis=1).astype(np.int64)
+        self.depth = depth[order]
         self._build_connections()
 
     def index_of(self, counts):
         """Indices of the given aux (count rows) in this basis, -1 if absent."""
-        k = self.keyer.sort_keys(counts)
+        return self.index_of_keys(self.keyer.sort_keys(counts))
+
+    def index_of_keys(self, k):
+        """Indices of the aux with the given sort keys in this basis, -1 if absent."""
         pos = np.searchsorted(self.keys, k)
         pos = np.minimum(pos, self.n_hier - 1)
         found = self.keys[pos] == k
         return np.where(found, pos, -1).astype(np.int64)
 
     def _build_connections(self):
-        """k+1 / k-1 connections along the basis modes (hops_hierarchy.py:470-523)."""
+        """k+1 / k-1 connections along the basis modes (hops_hierarchy.py:470-523).
+
+        The candidate a + e_m of every aux below MAXHIER and basis mode m is
+        its sorted mode tuple with m inserted in order; the candidates are
+        keyed from those tuples (keys_from_tuples) and looked up in the
+        basis's sorted keys, without forming their count rows."""
         ups_a, ups_u, ups_m = [], [], []
         below = np.nonzero(self.depth < self.maxhier)[0]
-        n_abs = self.counts.shape[1]
-        # modes per batch: keep the stacked candidate rows near 4M count entries
-        per = max(1, int(4_000_000 // max(1, len(below) * n_abs)))
-        for c0 in range(0, len(self.modes) if len(below) else 0, per):
-            rels = np.arange(c0, min(c0 + per, len(self.modes)))
-            up = np.repeat(self.counts[below][None], len(rels), axis=0)
-            up[np.arange(len(rels)), :, self.modes[rels]] += 1
-            idx = self.index_of(up.reshape(-1, n_abs)).reshape(len(rels), len(below))
-            for i, rel in enumerate(rels):
-                ok = idx[i] >= 0
-                ups_a.append(below[ok])
-                ups_u.append(idx[i][ok])
-                ups_m.append(np.full(ok.sum(), rel, dtype=np.int64))
+        nm = len(self.modes)
+        if len(below) and nm:
+            T = self.tup[below]
+            D = T.shape[1]
+            dep1 = self.depth[below] + 1
+            Tsh = np.full_like(T, _PAD)          # the tuple shifted one place right
+            Tsh[:, 1:] = T[:, :-1]
+            ar = np.arange(D)
+            # modes per batch: keep the candidate tuples near 4M entries
+            per = max(1, int(4_000_000 // max(1, len(below) * D)))
+            for c0 in range(0, nm, per):
+                rels = np.arange(c0, min(c0 + per, nm))
+                mabs = self.modes[rels].astype(np.int64)
+                pos = (T[:, None, :] <= mabs[None, :, None]).sum(axis=2)
+                cand = np.where(ar < pos[..., None], T[:, None, :],
+                                np.where(ar == pos[..., None], mabs[None, :, None],
+                                         Tsh[:, None, :]))
+                keys = self.keyer.keys_from_tuples(cand.reshape(-1, D),
+                                                   np.repeat(dep1, len(rels)))
+                p = np.minimum(np.searchsorted(self.keys, keys), self.n_hier - 1)
+                idx = np.where(self.keys[p] == keys, p, -1).reshape(len(below), len(rels))
+                ii, jj = np.nonzero(idx >= 0)
+                ups_a.append(below[ii])
+                ups_u.append(idx[ii, jj])
+                ups_m.append(rels[jj])
         if ups_a:
             a = np.concatenate(ups_a)
             u = np.concatenate(ups_u)
