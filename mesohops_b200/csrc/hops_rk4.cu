@@ -7,6 +7,7 @@
 #include <string.h>
 #include <stdarg.h>
 #include <algorithm>
+#include <utility>
 #include <vector>
 #include "hops_common.cuh"
 
@@ -47,6 +48,60 @@ extern "C" int hops_device_query(int device, int* sm_count, int* smem_optin) {
   CUDA_TRY(cudaDeviceGetAttribute(sm_count, cudaDevAttrMultiProcessorCount, device));
   CUDA_TRY(cudaDeviceGetAttribute(smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
   return HOPS_OK;
+}
+
+// ------------------------------------------- programmatic dependent launch ----
+// The scalar and stage kernels of a propagate call form a chain in one stream
+// (k_scalars -> stage kernel -> k_scalars ...).  With HOPS_PDL they are
+// launched with programmatic stream serialisation: each kernel lets its
+// dependent launch at once (griddepcontrol.launch_dependents) and waits for
+// its predecessor's completion and memory (griddepcontrol.wait) before it
+// reads anything, so the dependent's launch and CTA placement overlap the
+// running kernel instead of following it.  A dependent launches only once
+// every CTA of its predecessor is resident and has triggered, and no kernel
+// waits on its dependent, so the waits always end.
+#ifndef HOPS_PDL
+#define HOPS_PDL 1
+#endif
+// the stage kernels: let the next k_scalars launch at once, then wait
+__device__ __forceinline__ void pdl_enter() {
+#if HOPS_PDL
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
+}
+// k_scalars waits at entry and lets the next stage kernel launch only at its
+// end, so that the stage kernel's one-wave grid is placed all at once rather
+// than partly beside the scalar CTAs
+__device__ __forceinline__ void pdl_wait() {
+#if HOPS_PDL
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
+}
+__device__ __forceinline__ void pdl_trigger() {
+#if HOPS_PDL
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
+}
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_chain(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                                cudaStream_t s, Args&&... args) {
+#if HOPS_PDL
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+#else
+  kern<<<grid, block, smem, s>>>(std::forward<Args>(args)...);
+  return cudaGetLastError();
+#endif
 }
 
 // ------------------------------------------------------------- precision ----
@@ -740,6 +795,7 @@ __global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R
            FastDiv divS, FastDiv divAS, FastDiv divH, FastDiv divP, unsigned n_pre_s,
            int chunk_major) {
   extern __shared__ __align__(16) unsigned char wide_smem[];
+  pdl_enter();
   wide_items<R, ST, PT, SITE, NB, LT>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, divS,
                                       divAS, divH, divP, n_pre_s, chunk_major, wide_smem);
 }
@@ -755,6 +811,7 @@ __global__ void __launch_bounds__(256) k_narrow(hops_structure st, int B, int st
                                                 ST* acc, const double* __restrict__ ws,
                                                 FastDiv divB) {
   using T = typename Prec<R>::T;
+  pdl_enter();
   const int S = st.n_state;
   const int SB = S * B;
   const BatchLayout bl(S, st.n_mode, st.n_lop, B);
@@ -931,8 +988,10 @@ __global__ void __launch_bounds__(128) k_scalars(hops_structure st, hops_batch b
                                                  double* psi_prev, const float* z1s,
                                                  const float* z2s, double* dz_out, int stage_rows) {
   extern __shared__ double shm[];
+  pdl_wait();
   scalars_cta<R, ST, PT>(st, bt, blockIdx.x, stage, it, h, yin, recompute_scale, psi_prev, z1s,
                          z2s, dz_out, stage_rows, shm);
+  pdl_trigger();
 }
 
 // --------------------------------------------- persistent step kernel ----
@@ -1464,7 +1523,7 @@ static void launch_wide_lt(const hops_structure* st, int B, int stage, double h,
       set_for = dev;
     }
   }
-  k_wide<R, ST, PT, SITE, NB, LT><<<grid, threads, smem, s>>>(
+  launch_chain(k_wide<R, ST, PT, SITE, NB, LT>, dim3(grid), dim3(threads), smem, s,
       *st, B, stage, h, (const ST*)yin, (ST*)yout, (PT*)phi, (ST*)shadow, (ST*)acc, ws,
       FastDiv((unsigned)st->n_state), FastDiv(n_as), FastDiv((unsigned)st->n_hier),
       FastDiv(n_pre > 0 ? (unsigned)n_pre : 1u), (unsigned)n_pre * st->n_state, chunk_major);
@@ -1570,9 +1629,9 @@ static void launch_stage(const hops_structure* st, int B, int stage, double h, c
     else launch_wide<R, ST, PT, SITE, 8>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, cm, s);
   } else {
     const int grid = grid_for_warps(st->n_hier);
-    k_narrow<R, ST, PT, SITE><<<grid, 256, 0, s>>>(*st, B, stage, h, (const ST*)yin, (ST*)yout,
-                                                   (PT*)phi, (ST*)shadow, (ST*)acc, ws,
-                                                   FastDiv((unsigned)B));
+    launch_chain(k_narrow<R, ST, PT, SITE>, dim3(grid), dim3(256), 0, s, *st, B, stage, h,
+                 (const ST*)yin, (ST*)yout, (PT*)phi, (ST*)shadow, (ST*)acc, ws,
+                 FastDiv((unsigned)B));
   }
 }
 
@@ -1635,8 +1694,9 @@ static int propagate_impl(const hops_structure* st, hops_batch* bt, int32_t it0,
       void* yout = i == 0 ? bt->y0 : (i == 1 ? bt->y1 : (i == 2 ? bt->y0 : nullptr));
       const int recompute = (i == 0 && n > 0 && normalized) ? 1 : 0;
       double* psi_prev = (i == 0 && n > 0 && psi_out) ? psi_out + (size_t)(n - 1) * psi_stride : nullptr;
-      k_scalars<R, ST, PT><<<B, 128, smem, s>>>(*st, *bt, i, it, h, yin, recompute, psi_prev,
-                                                nullptr, nullptr, nullptr, stage_rows);
+      launch_chain(k_scalars<R, ST, PT>, dim3(B), dim3(128), smem, s, *st, *bt, i, it, h, yin,
+                   recompute, psi_prev, (const float*)nullptr, (const float*)nullptr,
+                   (double*)nullptr, stage_rows);
       LAUNCH_CHECK();
       int rc = run_stage<R, ST, PT>(st, B, i, h, yin, yout, bt->phi, shadow, bt->acc, bt->work,
                                     bt->status, s);
