@@ -804,8 +804,18 @@ __global__ void __launch_bounds__(wide_threads(NB), wide_min_blocks(NB, sizeof(R
 // -------------------------------------------------- narrow stage kernel ----
 // B < 32 trajectories: one warp per aux a (warp-uniform connection lists),
 // lanes over the S*B elements (state s, trajectory b) of that aux.
-template <typename R, typename ST, typename PT, bool SITE>
-__global__ void __launch_bounds__(256) k_narrow(hops_structure st, int B, int stage, double h,
+// MINB: resident CTAs per SM the kernel is compiled for.  Complex128 stage
+// vectors on aux of >= 64 elements (large single trajectories) run with
+// MINB = 5 (48 registers, 40 warps per SM), everything else with MINB = 4
+// (64 registers).  Stage launch, ms, MINB 4 / 5 / 6: 120-site chain depth 3
+// complex128 1.054 / 1.019 / 1.029, mixed 0.969 / 0.954 / 0.994; 200-site
+// chain complex128 8.84 / 8.45 / 8.56, mixed 7.90 / 7.99 / 8.24; the
+// one-trajectory 20-site ring (20 elements per aux) is unaffected.
+#ifndef HOPS_NARROW_BIG_MINB
+#define HOPS_NARROW_BIG_MINB 5
+#endif
+template <typename R, typename ST, typename PT, bool SITE, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_narrow(hops_structure st, int B, int stage, double h,
                                                 const ST* __restrict__ yin,
                                                 ST* __restrict__ yout, PT* phi, ST* shadow,
                                                 ST* acc, const double* __restrict__ ws,
@@ -1629,9 +1639,14 @@ static void launch_stage(const hops_structure* st, int B, int stage, double h, c
     else launch_wide<R, ST, PT, SITE, 8>(st, B, stage, h, yin, yout, phi, shadow, acc, ws, cm, s);
   } else {
     const int grid = grid_for_warps(st->n_hier);
-    launch_chain(k_narrow<R, ST, PT, SITE>, dim3(grid), dim3(256), 0, s, *st, B, stage, h,
-                 (const ST*)yin, (ST*)yout, (PT*)phi, (ST*)shadow, (ST*)acc, ws,
-                 FastDiv((unsigned)B));
+    if (st->n_state * B >= 64 && sizeof(ST) == 16)
+      launch_chain(k_narrow<R, ST, PT, SITE, HOPS_NARROW_BIG_MINB>, dim3(grid), dim3(256), 0, s, *st, B, stage, h,
+                   (const ST*)yin, (ST*)yout, (PT*)phi, (ST*)shadow, (ST*)acc, ws,
+                   FastDiv((unsigned)B));
+    else
+      launch_chain(k_narrow<R, ST, PT, SITE, 4>, dim3(grid), dim3(256), 0, s, *st, B, stage, h,
+                   (const ST*)yin, (ST*)yout, (PT*)phi, (ST*)shadow, (ST*)acc, ws,
+                   FastDiv((unsigned)B));
   }
 }
 
