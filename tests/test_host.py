@@ -68,6 +68,35 @@ def test_sort_keys_order_and_equality_are_the_ranks(M, D):
                               exact[np.unique(sk, return_index=True)[1]], kind="stable")])
 
 
+@pytest.mark.parametrize("M,D", [(7, 4), (500, 10)])
+def test_tuple_keys_equal_count_row_keys(M, D):
+    """keys_from_tuples of sorted mode tuples -- and of tuples with one mode
+    inserted or removed (how the adaptive basis keys its neighbour candidates)
+    -- equal sort_keys of the corresponding count rows, for int64 ranks and
+    for byte keys."""
+    k = H.AuxKeyer(M, D)
+    rng = np.random.default_rng(4)
+    c = np.zeros((300, M), dtype=np.int16)
+    for r in range(1, len(c)):
+        np.add.at(c[r], rng.integers(0, min(M, 15), rng.integers(1, D + 1)), 1)
+    tup, depth = H.tuples_of(c, D)
+    assert np.array_equal(k.keys_from_tuples(tup, depth), k.sort_keys(c))
+    # insert a mode into every row below D
+    low = np.nonzero(depth < D)[0]
+    m = rng.integers(0, M, len(low))
+    up = c[low].copy()
+    up[np.arange(len(low)), m] += 1
+    assert np.array_equal(k.keys_from_tuples(H.insert_mode(tup[low], m), depth[low] + 1),
+                          k.sort_keys(up))
+    # remove one of its modes from every row above depth 0
+    hi = np.nonzero(depth > 0)[0]
+    mm = np.array([rng.choice(np.nonzero(c[r])[0]) for r in hi])
+    dn = c[hi].copy()
+    dn[np.arange(len(hi)), mm] -= 1
+    assert np.array_equal(k.keys_from_tuples(H.remove_mode(tup[hi], mm), depth[hi] - 1),
+                          k.sort_keys(dn))
+
+
 def test_missing_zero_aux_raises():
     c = np.array([[1, 0], [0, 1]])
     with pytest.raises(AuxError):
