@@ -85,12 +85,16 @@ def build_tables(system, basis, state_list=None, mode_list=None, small=None):
     counts = basis.counts
     # K2_k diagonal (eom_hops_ksuper.py:78-87): -aux . W over the aux's own modes
     k_decay = -(counts[:, modes].astype(np.float64) @ W) if M else np.zeros(basis.n_hier)
-    # connections are along basis.modes; remap to the relative mode list
-    rel_of_basis_mode = {int(m): i for i, m in enumerate(modes)}
-    up_m = np.array([rel_of_basis_mode[int(basis.modes[m])] for m in basis.up_m], dtype=np.int32)
-    dn_m = np.array([rel_of_basis_mode[int(basis.modes[m])] for m in basis.dn_m], dtype=np.int32)
+    # connections are along basis.modes (a subset of the sorted mode list);
+    # remap to the relative mode list
+    bm = np.asarray(basis.modes, dtype=np.int64)
+    rel = np.searchsorted(modes, bm).astype(np.int32)
+    if len(bm) and (rel.max() >= len(modes) or np.any(modes[rel] != bm)):
+        raise ValueError("the basis modes are not in the mode list")
+    up_m = rel[np.asarray(basis.up_m, dtype=np.int64)]
+    dn_m = rel[np.asarray(basis.dn_m, dtype=np.int64)]
     dn_coef = basis.dn_k.astype(np.float64) * W[dn_m] if len(dn_m) else np.zeros(0, complex)
-    first = [(a, rel_of_basis_mode[int(basis.modes[m])]) for (a, m) in basis.first_level()]
+    first = [(a, int(rel[m])) for (a, m) in basis.first_level()]
     first_aux = np.array([a for a, _ in first], dtype=np.int32)
     first_mode = np.array([m for _, m in first], dtype=np.int32)
     mode_site = small["mode_site"]
