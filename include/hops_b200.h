@@ -22,6 +22,9 @@
  *   hops_noise_filter        <- noise/hops_noise.py:630-716 (_construct_correlated_noise)
  *                               with hops_noise.py:167-192,232-247 (alpha, complex64)
  *   hops_noise_window_mean   <- integrator/integrator_rk.py:115-128 (effective noise)
+ *   hops_noise_draw          <- noise/hops_noise.py:558-628 (_generate_noise_samples with
+ *                               PCG64(SEED).jumped(lop) streams, _construct_indexing)
+ *                               and hops_noise.py:522-553 (complex64 raw noise)
  */
 #ifndef HOPS_B200_H
 #define HOPS_B200_H
@@ -315,6 +318,25 @@ size_t hops_noise_filter_work_doubles(int32_t n_lop, int32_t n_t);
 int hops_noise_window_mean(const float* noise_dev, int64_t rows, int32_t n_t, int32_t start,
                            int32_t k, int32_t n_out, int32_t real_only, float* out_dev,
                            void* stream);
+
+/* Raw (uncorrelated) white noise of the FFT_FILTER model drawn on the device:
+ * replaces noise/hops_noise.py:558-628 (one PCG64(SEED).jumped(lop) stream per
+ * L-operator, numpy's Generator.normal for RAND_MODEL "SUM_GAUSSIAN" = model 0
+ * or Generator.random with the Box-Muller transform for "BOX_MULLER" = model 1,
+ * draws placed by _construct_indexing) and the complex64 assembly of
+ * hops_noise.py:522-553.  seed_states_dev: device uint64 [n_traj][4], each
+ * trajectory's un-jumped PCG64 state (state high and low 64 bits, increment
+ * high and low 64 bits: numpy's PCG64(SEED).state); lops_dev: device int32
+ * [n_lop], the absolute L-operator index (>= 0) of each row; z_dev: complex64
+ * [n_traj * n_lop][2(n_t-1)] out, row b*n_lop + j for trajectory b and
+ * L-operator lops[j].  SUM_GAUSSIAN draws equal numpy's bit for bit (a tail
+ * draw, about 3e-4 of them, goes through log1p, whose last bit may differ
+ * between math libraries: after the rounding to complex64 that changes a
+ * sample with probability ~1e-8); BOX_MULLER uses the device's log and sincos,
+ * so a sample can differ from numpy's in its last complex64 bit.  The output
+ * is the z_dev input of hops_noise_filter.  Requires n_t >= 2. */
+int hops_noise_draw(const uint64_t* seed_states_dev, int32_t n_traj, const int32_t* lops_dev,
+                    int32_t n_lop, int32_t n_t, int32_t model, float* z_dev, void* stream);
 
 /*
  * Shape of the batched stage kernel (batches of >= 32 trajectories): 32*nb

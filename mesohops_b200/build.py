@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import os
 import subprocess
+from concurrent.futures import ThreadPoolExecutor
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -32,7 +33,8 @@ def needs_build():
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = sources() + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh")]
+    deps = sources() + [os.path.join(CSRC, f) for f in os.listdir(CSRC)
+                        if f.endswith((".cuh", ".h"))]
     deps.append(os.path.join(HERE, "..", "include", "hops_b200.h"))
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
@@ -42,14 +44,18 @@ def build(verbose=False, force=False):
     if not force and not needs_build():
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     for src in sources():
         obj = os.path.join(LIBDIR, os.path.basename(src)[:-3] + ".o")
-        cmd = [_nvcc(), *ARCH, *FLAGS, "-c", src, "-o", obj]
-        if verbose:
-            print(" ".join(cmd))
-        subprocess.check_call(cmd)
+        cmds.append([_nvcc(), *ARCH, *FLAGS, "-c", src, "-o", obj])
         objs.append(obj)
+    # one nvcc per translation unit, all at once
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for cmd in cmds:
+            if verbose:
+                print(" ".join(cmd))
+        for f in [ex.submit(subprocess.check_call, c) for c in cmds]:
+            f.result()
     tmp = LIB + ".tmp"
     cmd = [_nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcufft", "-lcudart"]
     if verbose:

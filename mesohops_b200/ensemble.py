@@ -83,8 +83,8 @@ class HopsEnsemble:
             proto = HopsNoise({k: v for k, v in self.noise_param.items() if k != "T_AXIS"},
                               self.system)
             alpha = proto._corr()
-            raw = np.concatenate([raw_white_noise(s, range(L), n_t, self.noise_param["RAND_MODEL"])
-                                  for s in seeds], axis=0)
+            raw = raw_white_noise(seeds, range(L), n_t, self.noise_param["RAND_MODEL"],
+                                  self.device)
             out, _ = filter_on_device(np.tile(alpha, (self.B, 1)), raw, self.device,
                                       complex128=bool(self.noise_param["INTERPOLATE"]))
             self.noise = out.reshape(self.B, L, n_t)

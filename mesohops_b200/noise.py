@@ -2,10 +2,12 @@
 
 Models: FFT_FILTER (correlated complex Gaussian noise), PRE_CALCULATED (a
 given correlated trajectory) and ZERO.  The raw white noise is drawn on the
-host with numpy's PCG64(SEED).jumped(lop) stream, exactly as the reference does
-(hops_noise.py:558-628), so a SEED gives the same raw draws; the circulant-
-embedding filter (hops_noise.py:630-716) runs in FP64 on the GPU through
-``hops_noise_filter``.  The correlated noise is stored as complex64
+GPU (``hops_noise_draw``) from the reference's PCG64(SEED).jumped(lop) streams
+with numpy's normal (or uniform, for BOX_MULLER) sampler restated, so a SEED
+gives the reference's raw draws (hops_noise.py:558-628); only the seed hashing
+(numpy's PCG64(SEED).state, one per trajectory) stays on the host.  The
+circulant-embedding filter (hops_noise.py:630-716) runs in FP64 on the GPU
+through ``hops_noise_filter``.  The correlated noise is stored as complex64
 (hops_noise.py:247), one row per unique L-operator.
 """
 from __future__ import annotations
@@ -37,40 +39,58 @@ def raw_slot_index(ntaus):
     return re, im
 
 
-def raw_white_noise(seed, lops, ntaus, rand_model="SUM_GAUSSIAN"):
-    """Uncorrelated complex64 draws [len(lops), 2(ntaus-1)] (hops_noise.py:453-590)."""
-    if rand_model not in ("SUM_GAUSSIAN", "BOX_MULLER"):
+RAND_MODELS = {"SUM_GAUSSIAN": 0, "BOX_MULLER": 1}
+
+
+def seed_states(seeds):
+    """uint64 [len(seeds)][4]: each trajectory's un-jumped PCG64 generator as
+    numpy seeds it (state high, state low, increment high, increment low).
+    SEED None takes fresh entropy, as the reference's PCG64(seed=None) does."""
+    out = np.empty((len(seeds), 4), dtype=np.uint64)
+    m = (1 << 64) - 1
+    for i, seed in enumerate(seeds):
+        st = np.random.PCG64(seed=seed).state["state"]
+        out[i] = (st["state"] >> 64, st["state"] & m, st["inc"] >> 64, st["inc"] & m)
+    return out
+
+
+def raw_white_noise(seeds, lops, ntaus, rand_model, device):
+    """Uncorrelated complex64 draws on the device, [len(seeds) * len(lops),
+    2(ntaus-1)]: row b * len(lops) + j is trajectory b's noise for L-operator
+    lops[j] (hops_noise.py:453-628, drawn by ``hops_noise_draw``)."""
+    if rand_model not in RAND_MODELS:
         raise UnsupportedRequest(f"Noise.param[RAND_MODEL] {rand_model}", "Noise._prepare_rand")
-    re, im = raw_slot_index(ntaus)
-    x = np.empty((len(lops), 4 * (ntaus - 1)), dtype=np.float64)
-    # jumped() leaves its generator untouched, so one seeded PCG64 serves every
-    # L-operator of the trajectory (SEED None: fresh entropy per row, as the
-    # reference constructs one generator per row)
-    base = np.random.PCG64(seed=seed) if seed is not None else None
-    for i, lop in enumerate(lops):
-        bg = (base if base is not None else np.random.PCG64(seed=None)).jumped(int(lop))
-        gen = np.random.Generator(bg)
-        if rand_model == "SUM_GAUSSIAN":
-            x[i] = gen.normal(loc=0, size=4 * (ntaus - 1))
-        else:
-            x[i] = gen.random(size=4 * (ntaus - 1))
-    if rand_model == "SUM_GAUSSIAN":
-        return np.complex64(x[:, re] + 1j * x[:, im])
-    return np.complex64(np.sqrt(-2.0 * np.log(x[:, re])) * np.exp(2.0j * np.pi * x[:, im]))
+    lops = [int(x) for x in lops]
+    if any(x < 0 for x in lops):
+        raise UnsupportedRequest("negative L-operator index", "Noise._prepare_rand")
+    dev = torch.device(device)
+    z = torch.empty((len(seeds) * len(lops), 2 * (ntaus - 1)), dtype=torch.complex64, device=dev)
+    if z.numel() == 0:
+        return z
+    st = torch.from_numpy(seed_states(seeds).view(np.int64)).to(dev)
+    lp = torch.tensor(lops, dtype=torch.int32, device=dev)
+    rc = _lib.lib().hops_noise_draw(st.data_ptr(), len(seeds), lp.data_ptr(), len(lops),
+                                    int(ntaus), RAND_MODELS[rand_model], z.data_ptr(),
+                                    torch.cuda.current_stream(dev).cuda_stream)
+    _lib.check(rc, "hops_noise_draw")
+    return z
 
 
 def filter_on_device(alpha, z_raw, device, complex128=False):
     """FP64 circulant-embedding filter on the GPU.
 
     alpha: complex128 [R, n_t] correlation functions; z_raw: complex64
-    [R, 2(n_t-1)].  Returns (complex64 device tensor [R, n_t] -- complex128 if
+    [R, 2(n_t-1)], a host array or a device tensor.  Returns (complex64 device tensor [R, n_t] -- complex128 if
     complex128 -- and the number of clipped negative spectral values).
     """
     L = _lib.lib()
     R, n_t = alpha.shape
     dev = torch.device(device)
     a = torch.from_numpy(np.ascontiguousarray(alpha, dtype=np.complex128)).to(dev)
-    z = torch.from_numpy(np.ascontiguousarray(z_raw, dtype=np.complex64)).to(dev)
+    if isinstance(z_raw, torch.Tensor):
+        z = z_raw.to(device=dev, dtype=torch.complex64).contiguous()
+    else:
+        z = torch.from_numpy(np.ascontiguousarray(z_raw, dtype=np.complex64)).to(dev)
     work = torch.empty(int(L.hops_noise_filter_work_doubles(R, n_t)), dtype=torch.float64, device=dev)
     out = torch.empty((R, n_t), dtype=torch.complex128 if complex128 else torch.complex64,
                       device=dev)
@@ -140,7 +160,7 @@ class HopsNoise:
                 alpha[j] += fn(t, *params[i])
         return alpha
 
-    def _uncorrelated(self):
+    def _uncorrelated(self, device):
         seed = self.param["SEED"]
         shape = (self.n_lop, 2 * (self.n_t - 1))
         if isinstance(seed, str):
@@ -153,7 +173,8 @@ class HopsNoise:
                 raise UnsupportedRequest("Noise.param[SEED] is an array of the wrong length",
                                          "Noise._prepare_rand", True)
             return seed
-        return raw_white_noise(seed, range(self.n_lop), self.n_t, self.param["RAND_MODEL"])
+        return raw_white_noise([seed], range(self.n_lop), self.n_t, self.param["RAND_MODEL"],
+                               device)
 
     def prepare(self, device):
         """Correlated noise as a device tensor [n_lop, n_t] (None for ZERO):
@@ -162,9 +183,10 @@ class HopsNoise:
             return self._dev
         model = self.param["MODEL"]
         if model == "FFT_FILTER":
-            z = self._uncorrelated()
+            z = self._uncorrelated(device)
             if self.param["STORE_RAW_NOISE"]:
-                self.param["Z_UNCORRELATED"] = z
+                self.param["Z_UNCORRELATED"] = (z.cpu().numpy() if isinstance(z, torch.Tensor)
+                                                else z)
             noise, self.n_clipped = filter_on_device(self._corr(), z, device,
                                                      complex128=self.interpolate)
         elif model == "PRE_CALCULATED":

