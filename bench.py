@@ -417,12 +417,51 @@ def extras(args, wl, sysp, ens, dev, value, K):
                     "note": f"the same {B}-trajectory batch in {prec}, CUDA events over the "
                             f"{wl['n_steps']} steps of the first accuracy realisation"}
 
+    out["noise_setup"] = noise_setup_leg(ens, dev)
     out["cpu_baseline"] = cpu_baseline(wl, sysp)
     if not args.no_served:
         out["served"] = served_leg(args, dev)
     if not args.no_adaptive:
         out["adaptive_batch"] = adaptive_leg(args, dev)
     return out
+
+
+def noise_setup_leg(ens, dev, reps=3, host_sample=8):
+    """Set-up of the batch's FFT_FILTER noise: the raw draws on the device
+    (hops_noise_draw) and the FP64 filter, CUDA events over `reps` runs each,
+    beside numpy's host draws of the same rows (the reference's generator, a
+    sample of `host_sample` trajectories scaled to the batch); the sample's
+    device rows are checked equal to numpy's bit for bit."""
+    import torch
+    from mesohops_b200.noise import HopsNoise, filter_on_device, raw_white_noise
+    from oracle import hops_oracle as O
+    B, L, n_t = ens.B, ens.system.n_lop, ens.n_t
+    seeds = list(range(B))
+    model = ens.noise_param["RAND_MODEL"]
+    alpha = np.tile(HopsNoise({k: v for k, v in ens.noise_param.items() if k != "T_AXIS"},
+                              ens.system)._corr(), (B, 1))
+    raw_white_noise(seeds, range(L), n_t, model, dev)
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    e[0].record()
+    for _ in range(reps):
+        z = raw_white_noise(seeds, range(L), n_t, model, dev)
+    e[1].record()
+    for _ in range(reps):
+        filter_on_device(alpha, z, dev)
+    e[2].record()
+    torch.cuda.synchronize()
+    nb = min(host_sample, B)
+    t0 = time.perf_counter()
+    host = np.concatenate([O.raw_draws(s, range(L), n_t, model) for s in seeds[:nb]], axis=0)
+    host_s = (time.perf_counter() - t0) * B / nb
+    same = bool(np.array_equal(z[:nb * L].cpu().numpy(), host))
+    return {"rows": B * L, "samples_per_row": 2 * (n_t - 1), "rand_model": model,
+            "device_draws_ms": round(e[0].elapsed_time(e[1]) / reps, 3),
+            "device_filter_ms": round(e[1].elapsed_time(e[2]) / reps, 3),
+            "host_numpy_draws_ms": round(host_s * 1e3, 1),
+            "host_sample": f"{nb} of {B} trajectories, scaled to {B}",
+            "device_draws_equal_numpy": same}
 
 
 def _oracle_psi(job):
