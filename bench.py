@@ -427,25 +427,31 @@ def extras(args, wl, sysp, ens, dev, value, K):
 
 
 def noise_setup_leg(ens, dev, reps=3, host_sample=8):
-    """Set-up of the batch's FFT_FILTER noise: the raw draws on the device
+    """Set-up of the batch's FFT_FILTER noise: the seed hashing on the host
+    (numpy's PCG64(SEED).state per trajectory), the raw draws on the device
     (hops_noise_draw) and the FP64 filter, CUDA events over `reps` runs each,
     beside numpy's host draws of the same rows (the reference's generator, a
     sample of `host_sample` trajectories scaled to the batch); the sample's
     device rows are checked equal to numpy's bit for bit."""
     import torch
-    from mesohops_b200.noise import HopsNoise, filter_on_device, raw_white_noise
+    from mesohops_b200.noise import HopsNoise, draw_from_states, filter_on_device, seed_states
     from oracle import hops_oracle as O
     B, L, n_t = ens.B, ens.system.n_lop, ens.n_t
     seeds = list(range(B))
     model = ens.noise_param["RAND_MODEL"]
     alpha = np.tile(HopsNoise({k: v for k, v in ens.noise_param.items() if k != "T_AXIS"},
                               ens.system)._corr(), (B, 1))
-    raw_white_noise(seeds, range(L), n_t, model, dev)
+    t0 = time.perf_counter()
+    states = seed_states(seeds)
+    hash_ms = (time.perf_counter() - t0) * 1e3
+    st = torch.from_numpy(states.view(np.int64)).to(dev)
+    lp = torch.arange(L, dtype=torch.int32, device=dev)
+    draw_from_states(st, lp, n_t, model)
     torch.cuda.synchronize()
     e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
     e[0].record()
     for _ in range(reps):
-        z = raw_white_noise(seeds, range(L), n_t, model, dev)
+        z = draw_from_states(st, lp, n_t, model)
     e[1].record()
     for _ in range(reps):
         filter_on_device(alpha, z, dev)
@@ -457,7 +463,8 @@ def noise_setup_leg(ens, dev, reps=3, host_sample=8):
     host_s = (time.perf_counter() - t0) * B / nb
     same = bool(np.array_equal(z[:nb * L].cpu().numpy(), host))
     return {"rows": B * L, "samples_per_row": 2 * (n_t - 1), "rand_model": model,
-            "device_draws_ms": round(e[0].elapsed_time(e[1]) / reps, 3),
+            "host_seed_states_ms": round(hash_ms, 3),
+            "device_draws_ms": round(e[0].elapsed_time(e[1]) / reps, 4),
             "device_filter_ms": round(e[1].elapsed_time(e[2]) / reps, 3),
             "host_numpy_draws_ms": round(host_s * 1e3, 1),
             "host_sample": f"{nb} of {B} trajectories, scaled to {B}",

@@ -5,7 +5,14 @@
 // The reference gives L-operator l of a trajectory the stream
 // PCG64(SEED).jumped(l) and draws 4(n_t-1) numbers from it with numpy's
 // Generator.normal (SUM_GAUSSIAN) or Generator.random (BOX_MULLER).  Here one
-// thread owns one (trajectory, L-operator) row and replays that stream:
+// warp owns one (trajectory, L-operator) row and replays that stream 32 words
+// at a time: lane i holds word base + i (its own copy of the generator, moved
+// 32 steps per batch by one affine map of the state), so the stream's serial
+// recurrence is spread over the lanes.  A normal draw takes one word about
+// 99 % of the time; the warp emits the run of such draws up to the first
+// word that needs more (found by a ballot) in one store, then resolves that
+// draw with the next words of the stream (shuffled from their lanes) exactly as
+// the sequential sampler does:
 //   * PCG64 is O'Neill's permuted congruential generator with 128-bit state,
 //     multiplier 0x2360ed051fc65da44385df649fccf645, XSL-RR output taken after
 //     the step; jumped(l) advances the state by l * 0x9e3779b97f4a7c15f39cc0605cedc835
@@ -54,20 +61,8 @@ struct ZigTable {
   unsigned long long ki[256];
 };
 
-struct Pcg {
-  u128 s, inc;
-};
-
-__device__ __forceinline__ uint64_t pcg_next(Pcg& g) {
-  g.s = g.s * kPcgMult + g.inc;
-  const uint64_t x = (uint64_t)(g.s >> 64) ^ (uint64_t)g.s;
-  const unsigned rot = (unsigned)(g.s >> 122);
-  return (x >> rot) | (x << ((64u - rot) & 63u));
-}
-
-// State after `delta` steps: s_{n+delta} = A s_n + C with A = mult^delta and
-// C = inc (mult^delta - 1) / (mult - 1), both built by squaring.
-__device__ u128 pcg_advance(u128 s, u128 inc, u128 delta) {
+// Affine map of `delta` steps: s -> mult * s + C with mult = mult^delta.
+__device__ void pcg_skip(u128 inc, u128 delta, u128& mult, u128& plus) {
   u128 acc_mult = 1, acc_plus = 0, cur_mult = kPcgMult, cur_plus = inc;
   while (delta) {
     if (delta & 1) {
@@ -78,34 +73,18 @@ __device__ u128 pcg_advance(u128 s, u128 inc, u128 delta) {
     cur_mult *= cur_mult;
     delta >>= 1;
   }
-  return acc_mult * s + acc_plus;
+  mult = acc_mult;
+  plus = acc_plus;
 }
 
-__device__ __forceinline__ double next_double(Pcg& g) {
-  return (double)(pcg_next(g) >> 11) * (1.0 / 9007199254740992.0);
+__device__ __forceinline__ uint64_t xsl_rr(u128 s) {
+  const uint64_t x = (uint64_t)(s >> 64) ^ (uint64_t)s;
+  const unsigned rot = (unsigned)(s >> 122);
+  return (x >> rot) | (x << ((64u - rot) & 63u));
 }
 
-__device__ double zig_normal(Pcg& g, const ZigTable& z) {
-  for (;;) {
-    uint64_t r = pcg_next(g);
-    const int idx = (int)(r & 0xff);
-    r >>= 8;
-    const uint64_t field = (r >> 1) & kMask52;
-    double x = __dmul_rn((double)field, z.wi[idx]);
-    if (r & 1) x = -x;
-    if (field < z.ki[idx]) return x;  // about 99 % of draws
-    if (idx == 0) {
-      for (;;) {
-        const double xx = __dmul_rn(-kZigInvR, log1p(-next_double(g)));
-        const double yy = -log1p(-next_double(g));
-        if (__dadd_rn(yy, yy) > __dmul_rn(xx, xx))
-          return ((field >> 8) & 1) ? -__dadd_rn(kZigR, xx) : __dadd_rn(kZigR, xx);
-      }
-    }
-    const double height =
-        __dadd_rn(__dmul_rn(__dadd_rn(z.fi[idx - 1], -z.fi[idx]), next_double(g)), z.fi[idx]);
-    if (height < exp(__dmul_rn(__dmul_rn(-0.5, x), x))) return x;
-  }
+__device__ __forceinline__ double uniform53(uint64_t w) {
+  return (double)(w >> 11) * (1.0 / 9007199254740992.0);
 }
 
 // Time slot of the draw pair starting at even draw d (see the header comment).
@@ -115,12 +94,25 @@ __device__ __forceinline__ long draw_slot(long d, long n1) {
   return 2 * n1 - (d >> 2);
 }
 
-// rows = n_traj * n_lop; row = b * n_lop + j uses trajectory b's generator
-// jumped lops[j] times and writes z[row][0 .. 2(n_t-1)).
-__global__ void __launch_bounds__(128) k_raw_draws(const unsigned long long* __restrict__ states,
+// The lanes' 32 consecutive words of one stream.
+struct WarpStream {
+  u128 t;        // this lane's state right after producing its word
+  u128 a32, c32; // the 32-step map
+  uint64_t w;    // this lane's word of the current batch
+  __device__ __forceinline__ void next() {
+    t = a32 * t + c32;
+    w = xsl_rr(t);
+  }
+  __device__ __forceinline__ uint64_t word(int j) const { return __shfl_sync(0xffffffffu, w, j); }
+};
+
+// rows = n_traj * n_lop; warp `row` = b * n_lop + j uses trajectory b's
+// generator jumped lops[j] times and writes the row's 4 (n_t - 1) draws as
+// z[row][0 .. 2(n_t-1)) (complex64: real part of slot k at float 2k).
+__global__ void __launch_bounds__(256) k_raw_draws(const unsigned long long* __restrict__ states,
                                                    const int32_t* __restrict__ lops, int n_traj,
                                                    int n_lop, int n_t, int model,
-                                                   float2* __restrict__ z) {
+                                                   float* __restrict__ z) {
   __shared__ ZigTable tab;
   for (int i = threadIdx.x; i < 256; i += blockDim.x) {
     tab.wi[i] = c_wi[i];
@@ -128,31 +120,116 @@ __global__ void __launch_bounds__(128) k_raw_draws(const unsigned long long* __r
     tab.ki[i] = c_ki[i];
   }
   __syncthreads();
-  const long row = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= (long)n_traj * n_lop) return;
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const long row = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= (long)n_traj * n_lop) return;  // whole warps only
   const long b = row / n_lop;
   const int lop = lops[row - b * n_lop];
   const unsigned long long* st = states + 4 * b;
-  Pcg g;
-  g.inc = ((u128)st[2] << 64) | st[3];
-  g.s = pcg_advance(((u128)st[0] << 64) | st[1], g.inc, (u128)(uint64_t)lop * kPcgJump);
+  const u128 inc = ((u128)st[2] << 64) | st[3];
+  u128 m, c;
+  // the row's stream: PCG64(SEED).jumped(lop); lane i starts at word i
+  pcg_skip(inc, (u128)(uint64_t)lop * kPcgJump, m, c);
+  const u128 s0 = m * (((u128)st[0] << 64) | st[1]) + c;
+  WarpStream ws;
+  pcg_skip(inc, (u128)(lane + 1), m, c);
+  ws.t = m * s0 + c;
+  ws.w = xsl_rr(ws.t);
+  pcg_skip(inc, (u128)32, ws.a32, ws.c32);
+
   const long n1 = n_t - 1;
-  float2* out = z + row * 2 * n1;
-  for (long d = 0; d < 4 * n1; d += 2) {
-    double a, c;
-    if (model == 0) {
-      a = zig_normal(g, tab);
-      c = zig_normal(g, tab);
-    } else {
-      const double u = next_double(g);
-      const double phi = next_double(g);
-      const double rad = sqrt(__dmul_rn(-2.0, log(u)));
-      double sn, cs;
-      sincos(__dmul_rn(kTwoPi, phi), &sn, &cs);
-      a = __dmul_rn(rad, cs);
-      c = __dmul_rn(rad, sn);
+  const long total = 4 * n1;
+  float* out = z + row * 4 * n1;
+  if (model == 1) {
+    // BOX_MULLER: one uniform per draw; the even lane of each pair writes the slot
+    for (long base = 0; base < total; base += 32) {
+      const double u = uniform53(ws.w);
+      const double ph = __shfl_down_sync(FULL, u, 1);
+      const long d = base + lane;
+      if (!(lane & 1) && d < total) {
+        const double rad = sqrt(__dmul_rn(-2.0, log(u)));
+        double sn, cs;
+        sincos(__dmul_rn(kTwoPi, ph), &sn, &cs);
+        reinterpret_cast<float2*>(out)[draw_slot(d, n1)] =
+            make_float2(__double2float_rn(__dmul_rn(rad, cs)), __double2float_rn(__dmul_rn(rad, sn)));
+      }
+      ws.next();
     }
-    out[draw_slot(d, n1)] = make_float2(__double2float_rn(a), __double2float_rn(c));
+    return;
+  }
+  auto put = [&](long d, double v) {
+    out[2 * draw_slot(d & ~1L, n1) + (d & 1)] = __double2float_rn(v);
+  };
+  long done = 0;  // draws written
+  int pos = 0;    // word of the batch where the next draw starts (warp-uniform)
+  while (done < total) {
+    const int idx = (int)(ws.w & 0xff);
+    const uint64_t r8 = ws.w >> 8;
+    const uint64_t field = (r8 >> 1) & kMask52;
+    double x = __dmul_rn((double)field, tab.wi[idx]);
+    if (r8 & 1) x = -x;
+    const bool fast = field < tab.ki[idx];
+    const unsigned slow = __ballot_sync(FULL, !fast) & (FULL << pos);
+    const int k = slow ? __ffs(slow) - 1 : 32;
+    if (lane >= pos && lane < k && done + (lane - pos) < total) put(done + (lane - pos), x);
+    done += k - pos;
+    if (k == 32) {
+      ws.next();
+      pos = 0;
+      continue;
+    }
+    if (done >= total) break;
+    // the draw starting at word k needs the words after it
+    const int kidx = __shfl_sync(FULL, idx, k);
+    const double kx = __shfl_sync(FULL, x, k);
+    const uint64_t kfield = __shfl_sync(FULL, field, k);
+    int j = k + 1;
+    bool have = false;
+    double v = 0.0;
+    if (kidx != 0) {
+      if (j == 32) {
+        ws.next();
+        j = 0;
+      }
+      const double u = uniform53(ws.word(j++));
+      const double height =
+          __dadd_rn(__dmul_rn(__dadd_rn(tab.fi[kidx - 1], -tab.fi[kidx]), u), tab.fi[kidx]);
+      if (height < exp(__dmul_rn(__dmul_rn(-0.5, kx), kx))) {
+        v = kx;
+        have = true;
+      }
+    } else {
+      // tail beyond r (Marsaglia): pairs of uniforms until one is accepted
+      for (;;) {
+        if (j == 32) {
+          ws.next();
+          j = 0;
+        }
+        const double u1 = uniform53(ws.word(j++));
+        if (j == 32) {
+          ws.next();
+          j = 0;
+        }
+        const double u2 = uniform53(ws.word(j++));
+        const double xx = __dmul_rn(-kZigInvR, log1p(-u1));
+        const double yy = -log1p(-u2);
+        if (__dadd_rn(yy, yy) > __dmul_rn(xx, xx)) {
+          v = ((kfield >> 8) & 1) ? -__dadd_rn(kZigR, xx) : __dadd_rn(kZigR, xx);
+          have = true;
+          break;
+        }
+      }
+    }
+    if (have) {
+      if (lane == 0) put(done, v);
+      ++done;
+    }
+    if (j == 32) {
+      ws.next();
+      j = 0;
+    }
+    pos = j;
   }
 }
 
@@ -177,12 +254,12 @@ extern "C" int hops_noise_draw(const uint64_t* seed_states_dev, int32_t n_traj,
     return rerr(1, "hops_noise_draw: bad arguments (n_traj=%d n_lop=%d n_t=%d model=%d)", n_traj,
                 n_lop, n_t, model);
   const long rows = (long)n_traj * n_lop;
-  const int threads = 128;
-  const long blocks = (rows + threads - 1) / threads;
+  const int threads = 256;  // 8 rows (warps) per CTA
+  const long blocks = (rows * 32 + threads - 1) / threads;
   if (blocks > 0x7fffffffL) return rerr(1, "hops_noise_draw: %ld rows", rows);
   k_raw_draws<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
       reinterpret_cast<const unsigned long long*>(seed_states_dev), lops_dev, n_traj, n_lop, n_t,
-      model, reinterpret_cast<float2*>(z_dev));
+      model, z_dev);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return rerr(2, "hops_noise_draw: %s", cudaGetErrorString(e));
   return 0;

@@ -64,14 +64,24 @@ def raw_white_noise(seeds, lops, ntaus, rand_model, device):
     if any(x < 0 for x in lops):
         raise UnsupportedRequest("negative L-operator index", "Noise._prepare_rand")
     dev = torch.device(device)
-    z = torch.empty((len(seeds) * len(lops), 2 * (ntaus - 1)), dtype=torch.complex64, device=dev)
-    if z.numel() == 0:
-        return z
+    if not seeds or not lops:
+        return torch.empty((len(seeds) * len(lops), 2 * (ntaus - 1)), dtype=torch.complex64,
+                           device=dev)
     st = torch.from_numpy(seed_states(seeds).view(np.int64)).to(dev)
     lp = torch.tensor(lops, dtype=torch.int32, device=dev)
-    rc = _lib.lib().hops_noise_draw(st.data_ptr(), len(seeds), lp.data_ptr(), len(lops),
+    return draw_from_states(st, lp, ntaus, rand_model)
+
+
+def draw_from_states(states, lops, ntaus, rand_model):
+    """The device draws of ``raw_white_noise`` from seed states already on the
+    device (int64 view of ``seed_states``, [n_traj, 4]) and an int32 device
+    tensor of L-operator indices."""
+    n_traj, n_lop = int(states.shape[0]), int(lops.numel())
+    z = torch.empty((n_traj * n_lop, 2 * (ntaus - 1)), dtype=torch.complex64,
+                    device=states.device)
+    rc = _lib.lib().hops_noise_draw(states.data_ptr(), n_traj, lops.data_ptr(), n_lop,
                                     int(ntaus), RAND_MODELS[rand_model], z.data_ptr(),
-                                    torch.cuda.current_stream(dev).cuda_stream)
+                                    torch.cuda.current_stream(states.device).cuda_stream)
     _lib.check(rc, "hops_noise_draw")
     return z
 

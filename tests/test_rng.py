@@ -128,3 +128,30 @@ def test_device_draws_ring_batch_bitwise(cuda_device):
     z = raw_white_noise(seeds, range(20), n_t, "SUM_GAUSSIAN", cuda_device).cpu().numpy()
     ref = np.concatenate([O.raw_draws(s, range(20), n_t) for s in seeds], axis=0)
     assert np.count_nonzero(z != ref) == 0
+
+
+@pytest.mark.gpu
+def test_device_box_muller_batch_within_one_ulp(cuda_device):
+    from mesohops_b200.noise import raw_white_noise
+    seeds, lops, n_t = [5, 6, 7], [0, 2, 9], 300
+    z = raw_white_noise(seeds, lops, n_t, "BOX_MULLER", cuda_device).cpu().numpy()
+    ref = np.concatenate([O.raw_draws(s, lops, n_t, "BOX_MULLER") for s in seeds], axis=0)
+    for part in (np.real, np.imag):
+        a = part(z).astype(np.float32).view(np.int32).astype(np.int64)
+        b = part(ref).astype(np.float32).view(np.int32).astype(np.int64)
+        assert np.abs(a - b).max() <= 1
+    assert np.count_nonzero(z != ref) <= z.size // 1000
+
+
+@pytest.mark.gpu
+def test_device_draws_unseeded_and_empty(cuda_device):
+    """SEED None: fresh entropy per trajectory (the reference seeds PCG64(None)),
+    so rows differ and the draws are standard complex Gaussians (variance 1 per
+    part); an empty L-operator list gives an empty array without a launch."""
+    from mesohops_b200.noise import raw_white_noise
+    z = raw_white_noise([None, None], [0, 1], 2001, "SUM_GAUSSIAN", cuda_device).cpu().numpy()
+    assert not np.array_equal(z[0], z[2]) and not np.array_equal(z[0], z[1])
+    assert abs(np.var(z.real) - 1.0) < 0.05 and abs(np.var(z.imag) - 1.0) < 0.05
+    assert abs(np.mean(z)) < 0.05
+    e = raw_white_noise([1, 2], [], 50, "SUM_GAUSSIAN", cuda_device)
+    assert tuple(e.shape) == (0, 98)
