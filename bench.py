@@ -439,8 +439,8 @@ def noise_setup_leg(ens, dev, reps=3, host_sample=8):
     B, L, n_t = ens.B, ens.system.n_lop, ens.n_t
     seeds = list(range(B))
     model = ens.noise_param["RAND_MODEL"]
-    alpha = np.tile(HopsNoise({k: v for k, v in ens.noise_param.items() if k != "T_AXIS"},
-                              ens.system)._corr(), (B, 1))
+    alpha = HopsNoise({k: v for k, v in ens.noise_param.items() if k != "T_AXIS"},
+                      ens.system)._corr()
     t0 = time.perf_counter()
     states = seed_states(seeds)
     hash_ms = (time.perf_counter() - t0) * 1e3

@@ -305,6 +305,21 @@ int hops_noise_filter(const double* alpha_dev, const float* z_dev, int32_t n_lop
 /* Doubles of device work area hops_noise_filter needs (work_dev). */
 size_t hops_noise_filter_work_doubles(int32_t n_lop, int32_t n_t);
 
+/* hops_noise_filter for rows that share correlation functions (the
+ * trajectories of an ensemble: the same system, their own noise): z_dev and
+ * the outputs have n_rows rows, alpha_dev n_alpha rows, and row r is filtered
+ * with alpha row r % n_alpha (n_rows a multiple of n_alpha).  The result
+ * equals hops_noise_filter on alpha tiled to n_rows rows, without the tiled
+ * copy.  The work area of hops_noise_filter_work_doubles(n_rows, n_t)
+ * suffices.  Both filter entry points take their cuFFT plan from a pool of
+ * at most 8 idle plans (per device, length and batch; each holds cuFFT's work
+ * area) and return it when the call has synchronised (n_negative_host set),
+ * so repeated set-ups of one shape skip the plan construction.  Same replaced
+ * interface as hops_noise_filter. */
+int hops_noise_filter_shared(const double* alpha_dev, int32_t n_alpha, const float* z_dev,
+                             int32_t n_rows, int32_t n_t, double* work_dev, double* out_dev,
+                             float* out64_dev, int64_t* n_negative_host, void* stream);
+
 /* Effective noise of EFFECTIVE_NOISE_INTEGRATION: replaces the window means of
  * integrator/integrator_rk.py:115-128 (np.mean over complex64 samples).
  * noise_dev: complex64 [rows][n_t]; out_dev: complex64 [rows][n_out] with

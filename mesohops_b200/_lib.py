@@ -115,6 +115,8 @@ def lib():
     L.hops_resident_scalar_doubles.restype = _i
     L.hops_resident_scalar_doubles.argtypes = [_i, _i, _i]
     L.hops_noise_filter.argtypes = [_p, _p, _i, _i, _p, _p, _p, C.POINTER(C.c_int64), _p]
+    L.hops_noise_filter_shared.argtypes = [_p, _i, _p, _i, _i, _p, _p, _p,
+                                           C.POINTER(C.c_int64), _p]
     L.hops_noise_filter_work_doubles.restype = C.c_size_t
     L.hops_noise_filter_work_doubles.argtypes = [_i, _i]
     L.hops_noise_window_mean.argtypes = [_p, C.c_int64, _i, _i, _i, _i, _i, _p, _p]
@@ -173,7 +175,8 @@ def exported_symbols():
     return ["hops_last_error", "hops_version", "hops_device_query",
             "hops_scalar_workspace_doubles", "hops_batch_reset", "hops_dsystem_dt",
             "hops_rk4_propagate", "hops_resident_propagate", "hops_resident_scalar_doubles",
-            "hops_noise_filter", "hops_noise_filter_work_doubles", "hops_kernel_timing",
+            "hops_noise_filter", "hops_noise_filter_shared", "hops_noise_filter_work_doubles",
+            "hops_kernel_timing",
             "hops_kernel_timing_read", "hops_noalloc_scratch_bytes",
             "hops_rk4_propagate_noalloc", "hops_stage_tuning", "hops_step_fusion",
             "hops_grid_barrier_test",

@@ -6,6 +6,8 @@
 #include <cufft.h>
 #include <stdio.h>
 #include <stdarg.h>
+#include <mutex>
+#include <vector>
 #include "hops_common.cuh"
 
 using namespace hops;
@@ -44,14 +46,16 @@ __device__ __forceinline__ double2 rot(double nu, long k) {
   return mk(cs, sn);
 }
 
-// emb[l][k], k < N = 2(n_t-1): rotated correlation function and its Hermitian mirror.
-__global__ void k_embed(const double* alpha, int n_lop, int n_t, double2* emb) {
+// emb[r][k], k < N = 2(n_t-1): rotated correlation function of alpha row
+// l = r % n_alpha and its Hermitian mirror.
+__global__ void k_embed(const double* alpha, int n_alpha, int n_rows, int n_t, double2* emb) {
   const long N = 2L * (n_t - 1);
-  const long total = (long)n_lop * N;
+  const long total = (long)n_rows * N;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
        i += (long)gridDim.x * blockDim.x) {
-    const int l = (int)(i / N);
-    const long k = i - (long)l * N;
+    const long r = i / N;
+    const long k = i - r * N;
+    const int l = (int)(r % n_alpha);
     const double nu = rot_nu(alpha, l, n_t);
     double2 v;
     if (k < n_t) {
@@ -86,9 +90,10 @@ __global__ void k_filter(const double2* spec, long total, double2* zw, unsigned 
   if (cnt) atomicAdd(nneg, cnt);
 }
 
-// out[l][k] = ifft(...)[k] / N * conj(rot(k)), k < n_t.
-__global__ void k_unrotate(const double* alpha, const double2* y, int n_lop, int n_t,
-                           double2* out, float2* out64) {
+// out[l][k] = ifft(...)[k] / N * conj(rot(k)), k < n_t; row l unrotated with
+// alpha row l % n_alpha.
+__global__ void k_unrotate(const double* alpha, int n_alpha, const double2* y, int n_lop,
+                           int n_t, double2* out, float2* out64) {
   const long N = 2L * (n_t - 1);
   const long total = (long)n_lop * n_t;
   const double invN = 1.0 / (double)N;
@@ -96,7 +101,7 @@ __global__ void k_unrotate(const double* alpha, const double2* y, int n_lop, int
        i += (long)gridDim.x * blockDim.x) {
     const int l = (int)(i / n_t);
     const long k = i - (long)l * n_t;
-    const double nu = rot_nu(alpha, l, n_t);
+    const double nu = rot_nu(alpha, l % n_alpha, n_t);
     double2 v = cscale(y[(long)l * N + k], invN);
     v = cmul(v, cconj(rot(nu, k)));
     if (out) out[i] = v;
@@ -115,28 +120,81 @@ extern "C" size_t hops_noise_filter_work_doubles(int32_t n_lop, int32_t n_t) {
   return (size_t)4 * n_lop * 2 * (size_t)(n_t - 1) + 2;
 }
 
-extern "C" int hops_noise_filter(const double* alpha_dev, const float* z_dev, int32_t n_lop,
-                                 int32_t n_t, double* work_dev, double* out_dev, float* out64_dev,
-                                 int64_t* n_negative_host, void* stream) {
-  if (!alpha_dev || !z_dev || !work_dev || n_lop <= 0 || n_t < 3)
-    return nerr(HOPS_EINVAL, "hops_noise_filter: bad arguments (n_lop=%d n_t=%d)", n_lop, n_t);
+// Batched Z2Z plans kept for reuse: making a plan costs milliseconds (tens of
+// milliseconds for lengths with large prime factors), and an ensemble, the
+// trajectories of an adaptive worker or repeated set-ups ask for the same
+// (device, length, batch) again.  A plan is lent to one call at a time and
+// taken back only after that call has synchronised its stream, so two calls
+// never share a plan's work area; at most kPlanKeep idle plans are kept.
+namespace {
+struct PlanKey {
+  int dev, n, batch;
+};
+struct IdlePlan {
+  PlanKey key;
+  cufftHandle plan;
+};
+std::mutex g_plan_mu;
+std::vector<IdlePlan> g_plans;
+constexpr size_t kPlanKeep = 8;
+
+bool plan_take(int n, int batch, cufftHandle* out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    for (size_t i = 0; i < g_plans.size(); ++i)
+      if (g_plans[i].key.dev == dev && g_plans[i].key.n == n && g_plans[i].key.batch == batch) {
+        *out = g_plans[i].plan;
+        g_plans.erase(g_plans.begin() + (long)i);
+        return true;
+      }
+  }
+  return cufftPlan1d(out, n, CUFFT_Z2Z, batch) == CUFFT_SUCCESS;
+}
+
+// `synced`: the call's work on the plan has completed.
+void plan_give(int n, int batch, cufftHandle plan, bool synced) {
+  int dev = 0;
+  if (synced && cudaGetDevice(&dev) == cudaSuccess) {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    g_plans.push_back({{dev, n, batch}, plan});
+    if (g_plans.size() <= kPlanKeep) return;
+    plan = g_plans.front().plan;  // the oldest idle plan goes
+    g_plans.erase(g_plans.begin());
+  }
+  cufftDestroy(plan);
+}
+}  // namespace
+
+extern "C" int hops_noise_filter_shared(const double* alpha_dev, int32_t n_alpha,
+                                        const float* z_dev, int32_t n_rows, int32_t n_t,
+                                        double* work_dev, double* out_dev, float* out64_dev,
+                                        int64_t* n_negative_host, void* stream) {
+  if (!alpha_dev || !z_dev || !work_dev || n_alpha <= 0 || n_rows <= 0 || n_rows % n_alpha ||
+      n_t < 3)
+    return nerr(HOPS_EINVAL, "hops_noise_filter: bad arguments (n_alpha=%d n_rows=%d n_t=%d)",
+                n_alpha, n_rows, n_t);
   cudaStream_t s = (cudaStream_t)stream;
   const int N = 2 * (n_t - 1);
-  const long total = (long)n_lop * N;
+  const long total = (long)n_rows * N;
   double2* emb = reinterpret_cast<double2*>(work_dev);
   double2* zw = emb + total;
   unsigned long long* nneg = reinterpret_cast<unsigned long long*>(zw + total);
   cufftHandle plan;
-  if (cufftPlan1d(&plan, N, CUFFT_Z2Z, n_lop) != CUFFT_SUCCESS)
-    return nerr(HOPS_ECUDA, "cufftPlan1d(%d, batch %d) failed", N, n_lop);
+  if (!plan_take(N, n_rows, &plan))
+    return nerr(HOPS_ECUDA, "cufftPlan1d(%d, batch %d) failed", N, n_rows);
   int rc = HOPS_OK;
+  bool synced = false;
   do {
     if (cufftSetStream(plan, s) != CUFFT_SUCCESS) { rc = nerr(HOPS_ECUDA, "cufftSetStream failed"); break; }
     if (cudaMemsetAsync(nneg, 0, sizeof(unsigned long long), s) != cudaSuccess) {
       rc = nerr(HOPS_ECUDA, "memset failed");
       break;
     }
-    k_embed<<<grid_for(total), 256, 0, s>>>(alpha_dev, n_lop, n_t, emb);
+    // every row's embedding from its alpha row: one batched plan serves all
+    // three transforms
+    k_embed<<<grid_for(total), 256, 0, s>>>(alpha_dev, n_alpha, n_rows, n_t, emb);
     if (cufftExecZ2Z(plan, (cufftDoubleComplex*)emb, (cufftDoubleComplex*)emb, CUFFT_FORWARD) != CUFFT_SUCCESS) {
       rc = nerr(HOPS_ECUDA, "cufftExecZ2Z (embedding) failed");
       break;
@@ -151,9 +209,9 @@ extern "C" int hops_noise_filter(const double* alpha_dev, const float* z_dev, in
       rc = nerr(HOPS_ECUDA, "cufftExecZ2Z (inverse) failed");
       break;
     }
-    k_unrotate<<<grid_for((long)n_lop * n_t), 256, 0, s>>>(alpha_dev, zw, n_lop, n_t,
-                                                           reinterpret_cast<double2*>(out_dev),
-                                                           reinterpret_cast<float2*>(out64_dev));
+    k_unrotate<<<grid_for((long)n_rows * n_t), 256, 0, s>>>(alpha_dev, n_alpha, zw, n_rows, n_t,
+                                                            reinterpret_cast<double2*>(out_dev),
+                                                            reinterpret_cast<float2*>(out64_dev));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
       rc = nerr(HOPS_ECUDA, "noise filter launch: %s", cudaGetErrorString(e));
@@ -166,11 +224,19 @@ extern "C" int hops_noise_filter(const double* alpha_dev, const float* z_dev, in
         rc = nerr(HOPS_ECUDA, "reading the clip count failed");
         break;
       }
+      synced = true;
       *n_negative_host = (int64_t)h;
     }
   } while (0);
-  cufftDestroy(plan);
+  plan_give(N, n_rows, plan, synced);
   return rc;
+}
+
+extern "C" int hops_noise_filter(const double* alpha_dev, const float* z_dev, int32_t n_lop,
+                                 int32_t n_t, double* work_dev, double* out_dev, float* out64_dev,
+                                 int64_t* n_negative_host, void* stream) {
+  return hops_noise_filter_shared(alpha_dev, n_lop, z_dev, n_lop, n_t, work_dev, out_dev,
+                                  out64_dev, n_negative_host, stream);
 }
 
 // ------------------------------------------------ effective-noise windows ----

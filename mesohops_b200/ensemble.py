@@ -85,7 +85,7 @@ class HopsEnsemble:
             alpha = proto._corr()
             raw = raw_white_noise(seeds, range(L), n_t, self.noise_param["RAND_MODEL"],
                                   self.device)
-            out, _ = filter_on_device(np.tile(alpha, (self.B, 1)), raw, self.device,
+            out, _ = filter_on_device(alpha, raw, self.device,
                                       complex128=bool(self.noise_param["INTERPOLATE"]))
             self.noise = out.reshape(self.B, L, n_t)
         else:

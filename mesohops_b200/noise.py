@@ -89,26 +89,30 @@ def draw_from_states(states, lops, ntaus, rand_model):
 def filter_on_device(alpha, z_raw, device, complex128=False):
     """FP64 circulant-embedding filter on the GPU.
 
-    alpha: complex128 [R, n_t] correlation functions; z_raw: complex64
-    [R, 2(n_t-1)], a host array or a device tensor.  Returns (complex64 device tensor [R, n_t] -- complex128 if
-    complex128 -- and the number of clipped negative spectral values).
+    alpha: complex128 [A, n_t] correlation functions; z_raw: complex64
+    [R, 2(n_t-1)], a host array or a device tensor, R a multiple of A; row r
+    is filtered with alpha row r % A (the trajectories of an ensemble share
+    one system's correlation functions).  Returns (complex64 device tensor
+    [R, n_t] -- complex128 if complex128 -- and the number of clipped
+    negative spectral values over the R rows).
     """
     L = _lib.lib()
-    R, n_t = alpha.shape
+    A, n_t = alpha.shape
     dev = torch.device(device)
     a = torch.from_numpy(np.ascontiguousarray(alpha, dtype=np.complex128)).to(dev)
     if isinstance(z_raw, torch.Tensor):
         z = z_raw.to(device=dev, dtype=torch.complex64).contiguous()
     else:
         z = torch.from_numpy(np.ascontiguousarray(z_raw, dtype=np.complex64)).to(dev)
+    R = int(z.shape[0])
     work = torch.empty(int(L.hops_noise_filter_work_doubles(R, n_t)), dtype=torch.float64, device=dev)
     out = torch.empty((R, n_t), dtype=torch.complex128 if complex128 else torch.complex64,
                       device=dev)
     nneg = C.c_int64(0)
     stream = torch.cuda.current_stream(dev).cuda_stream
-    rc = L.hops_noise_filter(a.data_ptr(), z.data_ptr(), R, n_t, work.data_ptr(),
-                             out.data_ptr() if complex128 else None,
-                             None if complex128 else out.data_ptr(), C.byref(nneg), stream)
+    rc = L.hops_noise_filter_shared(a.data_ptr(), A, z.data_ptr(), R, n_t, work.data_ptr(),
+                                    out.data_ptr() if complex128 else None,
+                                    None if complex128 else out.data_ptr(), C.byref(nneg), stream)
     _lib.check(rc, "hops_noise_filter")
     return out, int(nneg.value)
 

@@ -67,3 +67,36 @@ def test_fft_filter_trajectory_noise(cuda_device):
     assert np.max(np.abs(n - ref)) <= 1e-6 * np.max(np.abs(ref))
     hops.propagate(40.0, 4.0)
     assert np.all(np.isfinite(hops.phi))
+
+
+def test_shared_alpha_filter_equals_tiled(cuda_device):
+    """Rows that share correlation functions (an ensemble's trajectories) give
+    bit for bit what the filter gives on alpha tiled to every row, and the same
+    clip count."""
+    import ctypes as C
+    import torch
+    from mesohops_b200 import _lib
+    from mesohops_b200.noise import filter_on_device
+    f = load_golden("noise_dimer")
+    t = O.noise_t_axis(float(f["tlen"]), float(f["tau"]))
+    gw = [[g, w] for g, w in zip(f["G"], f["W"])]
+    alpha = O.alpha_by_lop(t, gw, [0, 1], 2)
+    n_t = alpha.shape[1]
+    rng = np.random.default_rng(11)
+    B = 5
+    raw = (rng.normal(size=(2 * B, 2 * (n_t - 1)))
+           + 1j * rng.normal(size=(2 * B, 2 * (n_t - 1)))).astype(np.complex64)
+    shared, n_shared = filter_on_device(alpha, raw, cuda_device)
+    L = _lib.lib()
+    dev = torch.device(cuda_device)
+    a = torch.from_numpy(np.ascontiguousarray(np.tile(alpha, (B, 1)))).to(dev)
+    z = torch.from_numpy(raw).to(dev)
+    work = torch.empty(int(L.hops_noise_filter_work_doubles(2 * B, n_t)), dtype=torch.float64,
+                       device=dev)
+    out = torch.empty((2 * B, n_t), dtype=torch.complex64, device=dev)
+    nneg = C.c_int64(0)
+    rc = L.hops_noise_filter(a.data_ptr(), z.data_ptr(), 2 * B, n_t, work.data_ptr(), None,
+                             out.data_ptr(), C.byref(nneg), torch.cuda.current_stream(dev).cuda_stream)
+    assert rc == 0
+    assert torch.equal(shared, out)
+    assert n_shared == nneg.value
