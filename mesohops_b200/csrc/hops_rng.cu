@@ -36,6 +36,7 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include "../../include/hops_b200.h"
 #include "hops_ziggurat_table.h"
 
 void hops_set_error_text(const char* msg);  // defined in hops_rk4.cu
@@ -251,16 +252,16 @@ extern "C" int hops_noise_draw(const uint64_t* seed_states_dev, int32_t n_traj,
                                int32_t model, float* z_dev, void* stream) {
   if (!seed_states_dev || !lops_dev || !z_dev || n_traj <= 0 || n_lop <= 0 || n_t < 2 ||
       (model != 0 && model != 1))
-    return rerr(1, "hops_noise_draw: bad arguments (n_traj=%d n_lop=%d n_t=%d model=%d)", n_traj,
-                n_lop, n_t, model);
+    return rerr(HOPS_EINVAL, "hops_noise_draw: bad arguments (n_traj=%d n_lop=%d n_t=%d model=%d)",
+                n_traj, n_lop, n_t, model);
   const long rows = (long)n_traj * n_lop;
   const int threads = 256;  // 8 rows (warps) per CTA
   const long blocks = (rows * 32 + threads - 1) / threads;
-  if (blocks > 0x7fffffffL) return rerr(1, "hops_noise_draw: %ld rows", rows);
+  if (blocks > 0x7fffffffL) return rerr(HOPS_EINVAL, "hops_noise_draw: %ld rows", rows);
   k_raw_draws<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
       reinterpret_cast<const unsigned long long*>(seed_states_dev), lops_dev, n_traj, n_lop, n_t,
       model, z_dev);
   const cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return rerr(2, "hops_noise_draw: %s", cudaGetErrorString(e));
+  if (e != cudaSuccess) return rerr(HOPS_ECUDA, "hops_noise_draw: %s", cudaGetErrorString(e));
   return 0;
 }

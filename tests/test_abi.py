@@ -44,3 +44,17 @@ def test_host_only_calls():
     rc = L.hops_resident_propagate(None, 0, 0, 0, 0, 1, None)
     assert rc == _lib.HOPS_EINVAL
     assert b"bad resident" in L.hops_last_error()
+
+
+def test_noise_entry_points_validate_before_any_cuda_call():
+    from mesohops_b200 import _lib
+    L = _lib.lib()
+    # no seed states, no rows, unknown sampler
+    assert L.hops_noise_draw(None, 1, None, 1, 10, 0, None, None) == _lib.HOPS_EINVAL
+    assert b"hops_noise_draw" in L.hops_last_error()
+    assert L.hops_noise_draw(8, 1, 8, 1, 10, 7, 8, None) == _lib.HOPS_EINVAL
+    assert L.hops_noise_draw(8, 1, 8, 1, 1, 0, 8, None) == _lib.HOPS_EINVAL
+    # rows that are not a multiple of the shared correlation functions
+    rc = L.hops_noise_filter_shared(8, 3, 8, 10, 20, 8, None, 8, None, None)
+    assert rc == _lib.HOPS_EINVAL
+    assert b"n_alpha=3 n_rows=10" in L.hops_last_error()
