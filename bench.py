@@ -427,24 +427,27 @@ def extras(args, wl, sysp, ens, dev, value, K):
 
 
 def noise_setup_leg(ens, dev, reps=3, host_sample=8):
-    """Set-up of the batch's FFT_FILTER noise: the seed hashing on the host
-    (numpy's PCG64(SEED).state per trajectory), the raw draws on the device
+    """Set-up of the batch's FFT_FILTER noise: the SEEDs hashed into PCG64
+    states on the device (wall clock, with their upload), the raw draws on the device
     (hops_noise_draw) and the FP64 filter, CUDA events over `reps` runs each,
     beside numpy's host draws of the same rows (the reference's generator, a
     sample of `host_sample` trajectories scaled to the batch); the sample's
     device rows are checked equal to numpy's bit for bit."""
     import torch
-    from mesohops_b200.noise import HopsNoise, draw_from_states, filter_on_device, seed_states
+    from mesohops_b200.noise import HopsNoise, draw_from_states, filter_on_device, \
+        seed_states_on_device
     from oracle import hops_oracle as O
     B, L, n_t = ens.B, ens.system.n_lop, ens.n_t
     seeds = list(range(B))
     model = ens.noise_param["RAND_MODEL"]
     alpha = HopsNoise({k: v for k, v in ens.noise_param.items() if k != "T_AXIS"},
                       ens.system)._corr()
+    seed_states_on_device(seeds, dev)
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
-    states = seed_states(seeds)
+    st = seed_states_on_device(seeds, dev)
+    torch.cuda.synchronize()
     hash_ms = (time.perf_counter() - t0) * 1e3
-    st = torch.from_numpy(states.view(np.int64)).to(dev)
     lp = torch.arange(L, dtype=torch.int32, device=dev)
     draw_from_states(st, lp, n_t, model)
     torch.cuda.synchronize()
@@ -463,7 +466,7 @@ def noise_setup_leg(ens, dev, reps=3, host_sample=8):
     host_s = (time.perf_counter() - t0) * B / nb
     same = bool(np.array_equal(z[:nb * L].cpu().numpy(), host))
     return {"rows": B * L, "samples_per_row": 2 * (n_t - 1), "rand_model": model,
-            "host_seed_states_ms": round(hash_ms, 3),
+            "seed_states_ms": round(hash_ms, 3),
             "device_draws_ms": round(e[0].elapsed_time(e[1]) / reps, 4),
             "device_filter_ms": round(e[1].elapsed_time(e[2]) / reps, 3),
             "host_numpy_draws_ms": round(host_s * 1e3, 1),

@@ -353,6 +353,15 @@ int hops_noise_window_mean(const float* noise_dev, int64_t rows, int32_t n_t, in
 int hops_noise_draw(const uint64_t* seed_states_dev, int32_t n_traj, const int32_t* lops_dev,
                     int32_t n_lop, int32_t n_t, int32_t model, float* z_dev, void* stream);
 
+/* The seed_states_dev input of hops_noise_draw from integer SEEDs, on the
+ * device: numpy's SeedSequence(SEED) hashing and PCG64 seeding (the
+ * reference's np.random.PCG64(seed=SEED), hops_noise.py:584).  SEED b is given
+ * as its 32-bit words, least significant first, in seed_words_dev[
+ * seed_ptr_dev[b] .. seed_ptr_dev[b+1]) (SEED 0: one word 0; SEEDs >= 0);
+ * seed_states_dev: uint64 [n_traj][4] out, as hops_noise_draw reads it. */
+int hops_noise_seed_states(const uint32_t* seed_words_dev, const int32_t* seed_ptr_dev,
+                           int32_t n_traj, uint64_t* seed_states_dev, void* stream);
+
 /*
  * Shape of the batched stage kernel (batches of >= 32 trajectories): 32*nb
  * trajectories per warp task and the

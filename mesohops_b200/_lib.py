@@ -121,6 +121,7 @@ def lib():
     L.hops_noise_filter_work_doubles.argtypes = [_i, _i]
     L.hops_noise_window_mean.argtypes = [_p, C.c_int64, _i, _i, _i, _i, _i, _p, _p]
     L.hops_noise_draw.argtypes = [_p, _i, _p, _i, _i, _i, _p, _p]
+    L.hops_noise_seed_states.argtypes = [_p, _p, _i, _p, _p]
     L.hops_noalloc_scratch_bytes.restype = C.c_size_t
     L.hops_noalloc_scratch_bytes.argtypes = [C.POINTER(HopsStructure), _i, _i]
     L.hops_rk4_propagate_noalloc.argtypes = [C.POINTER(HopsStructure), _i, _i, _i, _p, _p, _p,
@@ -182,7 +183,8 @@ def exported_symbols():
             "hops_grid_barrier_test",
             "hops_flux_errors",
             "hops_flux_errors_smem_doubles", "hops_tri_max_depth", "hops_tri_pass1",
-            "hops_tri_pass2", "hops_noise_window_mean", "hops_noise_draw", "hops_batch_settle",
+            "hops_tri_pass2", "hops_noise_window_mean", "hops_noise_draw", "hops_noise_seed_states",
+            "hops_batch_settle",
             "hops_structure_upload", "hops_structure_host_view", "hops_structure_device_view",
             "hops_structure_destroy", "hops_batch_create", "hops_batch_destroy",
             "hops_batch_set_state_host", "hops_batch_set_noise_host",

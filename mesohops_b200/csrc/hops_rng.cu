@@ -234,6 +234,55 @@ __global__ void __launch_bounds__(256) k_raw_draws(const unsigned long long* __r
   }
 }
 
+// numpy's SeedSequence(SEED) for an integer SEED (O'Neill's seed_seq_fe
+// hashing: a pool of four 32-bit words filled from the SEED's 32-bit words,
+// least significant first, by a multiplicative hash; every pool word mixed
+// into every other; the remaining SEED words mixed in; then generate_state(4,
+// uint64) read from the pool with a second hash), followed by PCG64's seeding
+// from those four words: increment = (w2:w3 << 1) | 1, state = step(step(0) +
+// w0:w1).  One thread per trajectory; words[ptr[b] .. ptr[b+1]) is SEED b.
+__global__ void k_seed_states(const uint32_t* __restrict__ words, const int32_t* __restrict__ ptr,
+                              int n_traj, unsigned long long* __restrict__ states) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n_traj) return;
+  const int w0 = ptr[b], nw = ptr[b + 1] - ptr[b];
+  uint32_t hc = 0x43b0d7e5u;
+  auto hashmix = [&](uint32_t v) {
+    v ^= hc;
+    hc *= 0x931e8875u;
+    v *= hc;
+    return v ^ (v >> 16);
+  };
+  auto mix = [](uint32_t x, uint32_t y) {
+    uint32_t r = 0xca01f9ddu * x - 0x4973f715u * y;
+    return r ^ (r >> 16);
+  };
+  uint32_t pool[4];
+  for (int i = 0; i < 4; ++i) pool[i] = hashmix(i < nw ? words[w0 + i] : 0u);
+  for (int src = 0; src < 4; ++src)
+    for (int dst = 0; dst < 4; ++dst)
+      if (src != dst) pool[dst] = mix(pool[dst], hashmix(pool[src]));
+  for (int src = 4; src < nw; ++src)
+    for (int dst = 0; dst < 4; ++dst) pool[dst] = mix(pool[dst], hashmix(words[w0 + src]));
+  uint32_t hb = 0x8b51f9ddu, out[8];
+  for (int i = 0; i < 8; ++i) {
+    uint32_t v = pool[i & 3] ^ hb;
+    hb *= 0x58f38dedu;
+    v *= hb;
+    out[i] = v ^ (v >> 16);
+  }
+  uint64_t v64[4];
+  for (int i = 0; i < 4; ++i) v64[i] = (uint64_t)out[2 * i] | ((uint64_t)out[2 * i + 1] << 32);
+  const u128 inc = ((((u128)v64[2] << 64) | v64[3]) << 1) | 1;
+  u128 st = inc;                                   // step from state 0
+  st += ((u128)v64[0] << 64) | v64[1];
+  st = st * kPcgMult + inc;
+  states[4 * b + 0] = (unsigned long long)(st >> 64);
+  states[4 * b + 1] = (unsigned long long)st;
+  states[4 * b + 2] = (unsigned long long)(inc >> 64);
+  states[4 * b + 3] = (unsigned long long)inc;
+}
+
 thread_local char g_rerr[512];
 
 int rerr(int code, const char* fmt, ...) {
@@ -263,5 +312,16 @@ extern "C" int hops_noise_draw(const uint64_t* seed_states_dev, int32_t n_traj,
       model, z_dev);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return rerr(HOPS_ECUDA, "hops_noise_draw: %s", cudaGetErrorString(e));
+  return 0;
+}
+
+extern "C" int hops_noise_seed_states(const uint32_t* seed_words_dev, const int32_t* seed_ptr_dev,
+                                      int32_t n_traj, uint64_t* seed_states_dev, void* stream) {
+  if (!seed_words_dev || !seed_ptr_dev || !seed_states_dev || n_traj <= 0)
+    return rerr(HOPS_EINVAL, "hops_noise_seed_states: bad arguments (n_traj=%d)", n_traj);
+  k_seed_states<<<(n_traj + 127) / 128, 128, 0, (cudaStream_t)stream>>>(
+      seed_words_dev, seed_ptr_dev, n_traj, reinterpret_cast<unsigned long long*>(seed_states_dev));
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return rerr(HOPS_ECUDA, "hops_noise_seed_states: %s", cudaGetErrorString(e));
   return 0;
 }

@@ -4,8 +4,8 @@ Models: FFT_FILTER (correlated complex Gaussian noise), PRE_CALCULATED (a
 given correlated trajectory) and ZERO.  The raw white noise is drawn on the
 GPU (``hops_noise_draw``) from the reference's PCG64(SEED).jumped(lop) streams
 with numpy's normal (or uniform, for BOX_MULLER) sampler restated, so a SEED
-gives the reference's raw draws (hops_noise.py:558-628); only the seed hashing
-(numpy's PCG64(SEED).state, one per trajectory) stays on the host.  The
+gives the reference's raw draws (hops_noise.py:558-628); the SEEDs are hashed
+into PCG64 states on the GPU as well (numpy's SeedSequence restated).  The
 circulant-embedding filter (hops_noise.py:630-716) runs in FP64 on the GPU
 through ``hops_noise_filter``.  The correlated noise is stored as complex64
 (hops_noise.py:247), one row per unique L-operator.
@@ -44,14 +44,44 @@ RAND_MODELS = {"SUM_GAUSSIAN": 0, "BOX_MULLER": 1}
 
 def seed_states(seeds):
     """uint64 [len(seeds)][4]: each trajectory's un-jumped PCG64 generator as
-    numpy seeds it (state high, state low, increment high, increment low).
-    SEED None takes fresh entropy, as the reference's PCG64(seed=None) does."""
+    numpy seeds it (state high, state low, increment high, increment low),
+    computed by numpy on the host.  SEED None takes fresh entropy, as the
+    reference's PCG64(seed=None) does.  ``seed_states_on_device`` computes the
+    same on the GPU."""
     out = np.empty((len(seeds), 4), dtype=np.uint64)
     m = (1 << 64) - 1
     for i, seed in enumerate(seeds):
         st = np.random.PCG64(seed=seed).state["state"]
         out[i] = (st["state"] >> 64, st["state"] & m, st["inc"] >> 64, st["inc"] & m)
     return out
+
+
+def seed_states_on_device(seeds, device):
+    """int64 device tensor [len(seeds), 4], the ``seed_states`` of the SEEDs
+    hashed on the GPU (``hops_noise_seed_states``); the host only splits each
+    SEED into 32-bit words.  SEED None draws fresh entropy on the host (numpy's
+    SeedSequence()), which is then hashed like an integer SEED."""
+    words, ptr = [], [0]
+    for seed in seeds:
+        v = int(np.random.SeedSequence().entropy) if seed is None else int(seed)
+        if v < 0:
+            raise ValueError(f"expected non-negative integer SEED, got {seed}")
+        w = []
+        while True:
+            w.append(v & 0xFFFFFFFF)
+            v >>= 32
+            if not v:
+                break
+        words.extend(w)
+        ptr.append(len(words))
+    dev = torch.device(device)
+    wd = torch.from_numpy(np.array(words, dtype=np.uint32).view(np.int32)).to(dev)
+    pd = torch.from_numpy(np.array(ptr, dtype=np.int32)).to(dev)
+    st = torch.empty((len(seeds), 4), dtype=torch.int64, device=dev)
+    rc = _lib.lib().hops_noise_seed_states(wd.data_ptr(), pd.data_ptr(), len(seeds), st.data_ptr(),
+                                           torch.cuda.current_stream(dev).cuda_stream)
+    _lib.check(rc, "hops_noise_seed_states")
+    return st
 
 
 def raw_white_noise(seeds, lops, ntaus, rand_model, device):
@@ -67,7 +97,7 @@ def raw_white_noise(seeds, lops, ntaus, rand_model, device):
     if not seeds or not lops:
         return torch.empty((len(seeds) * len(lops), 2 * (ntaus - 1)), dtype=torch.complex64,
                            device=dev)
-    st = torch.from_numpy(seed_states(seeds).view(np.int64)).to(dev)
+    st = seed_states_on_device(seeds, dev)
     lp = torch.tensor(lops, dtype=torch.int32, device=dev)
     return draw_from_states(st, lp, ntaus, rand_model)
 

@@ -155,3 +155,63 @@ def test_device_draws_unseeded_and_empty(cuda_device):
     assert abs(np.mean(z)) < 0.05
     e = raw_white_noise([1, 2], [], 50, "SUM_GAUSSIAN", cuda_device)
     assert tuple(e.shape) == (0, 98)
+
+
+SEEDS = [0, 1, 7, 12345, 2**32 - 1, 2**32 + 5, 2**63 + 11, 2**64 + 9, 2**100 + 3, 2**160 + 17]
+
+
+def restated_seed_state(seed):
+    """numpy's SeedSequence(seed) + PCG64 seeding, the steps k_seed_states takes."""
+    m32 = 0xFFFFFFFF
+    ent = []
+    v = seed
+    while True:
+        ent.append(v & m32)
+        v >>= 32
+        if not v:
+            break
+    hc = [0x43B0D7E5]
+
+    def hashmix(x):
+        x = (x ^ hc[0]) & m32
+        hc[0] = (hc[0] * 0x931E8875) & m32
+        x = (x * hc[0]) & m32
+        return x ^ (x >> 16)
+
+    def mix(x, y):
+        r = (0xCA01F9DD * x - 0x4973F715 * y) & m32
+        return r ^ (r >> 16)
+
+    pool = [hashmix(ent[i] if i < len(ent) else 0) for i in range(4)]
+    for s in range(4):
+        for d in range(4):
+            if s != d:
+                pool[d] = mix(pool[d], hashmix(pool[s]))
+    for s in range(4, len(ent)):
+        for d in range(4):
+            pool[d] = mix(pool[d], hashmix(ent[s]))
+    hb, out = 0x8B51F9DD, []
+    for i in range(8):
+        x = (pool[i % 4] ^ hb) & m32
+        hb = (hb * 0x58F38DED) & m32
+        x = (x * hb) & m32
+        out.append(x ^ (x >> 16))
+    w = [out[2 * i] | (out[2 * i + 1] << 32) for i in range(4)]
+    inc = ((((w[2] << 64) | w[3]) << 1) | 1) & M128
+    st = (((inc + ((w[0] << 64) | w[1])) & M128) * MULT + inc) & M128
+    return st, inc
+
+
+def test_seed_hashing_restated():
+    for seed in SEEDS:
+        st = np.random.PCG64(seed).state["state"]
+        assert restated_seed_state(seed) == (st["state"], st["inc"])
+
+
+@pytest.mark.gpu
+def test_device_seed_states_equal_numpy(cuda_device):
+    from mesohops_b200.noise import seed_states, seed_states_on_device
+    dev = seed_states_on_device(SEEDS, cuda_device).cpu().numpy().view(np.uint64)
+    assert np.array_equal(dev, seed_states(SEEDS))
+    with pytest.raises(ValueError):
+        seed_states_on_device([3, -1], cuda_device)
