@@ -17,8 +17,8 @@
 //     multiplier 0x2360ed051fc65da44385df649fccf645, XSL-RR output taken after
 //     the step; jumped(l) advances the state by l * 0x9e3779b97f4a7c15f39cc0605cedc835
 //     steps (mod 2^128) with Brown's logarithmic-time LCG skip.  The caller
-//     passes the un-jumped state and increment (numpy's PCG64(SEED).state), so
-//     the seed hashing stays on the host.
+//     passes the un-jumped state and increment (numpy's PCG64(SEED).state),
+//     which k_seed_states computes from integer SEEDs on the device.
 //   * Uniform doubles are (raw >> 11) * 2^-53.
 //   * Normals come from the 256-layer Marsaglia-Tsang ziggurat over a 52-bit
 //     field (table and its derivation in hops_ziggurat_table.h and
